@@ -1,0 +1,205 @@
+/*
+ * vca.h -- C ABI of the B200 lava-CA and Potts-MC library (libvca.so).
+ *
+ * The reference engine has no plugin layer: its hot paths are the C++ classes LavaCA<Storage>
+ * (engine/src/ca/LavaCA.hpp) and PottsMC (engine/src/mc/PottsMC.hpp), called directly by
+ * Simulation::runWith and McStage::run.  This header is the boundary that replaces those two
+ * classes: each entry point names the member function it stands in for.  Everything here is
+ * plain C (pointers, sizes, enums); no C++ or CUDA types cross it.
+ *
+ * Ownership: device buffers belong to the handle; host arrays passed in or out belong to the
+ * caller and are only read or written during the call.
+ * Threading: a handle is used by one host thread at a time; each handle owns one CUDA stream.
+ * Errors: every call returns a vca_status; vca_last_error() gives the message of the last failure
+ * on the calling thread.  No exception crosses the boundary.
+ * Layout of host planes: unframed, globalIndex order x + nx*(y + ny*z)
+ * (engine/src/core/Types.hpp:95-100), as in ca_result.bin.
+ */
+#ifndef VCA_H
+#define VCA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VCA_ABI_VERSION 1
+
+typedef enum {
+    VCA_OK = 0,
+    VCA_ERR_ARG = 1,      /* invalid argument (maps to the reference's ConfigError, exit code 1) */
+    VCA_ERR_STATE = 2,    /* call out of order, e.g. sweep before initialize */
+    VCA_ERR_CUDA = 3,     /* CUDA runtime failure or no usable sm_100 device */
+    VCA_ERR_NOMEM = 4,    /* device allocation failed */
+    VCA_ERR_TIMEOUT = 5   /* a bounded device wait ran out (the context stays usable) */
+} vca_status;
+
+/* NeighborhoodKind (engine/src/core/Types.hpp:22) */
+enum { VCA_NB_VON_NEUMANN = 0, VCA_NB_MOORE = 1, VCA_NB_PENTAGONAL = 2, VCA_NB_HEXAGONAL = 3 };
+/* BoundaryKind (engine/src/core/Types.hpp:25) */
+enum { VCA_BC_ABSORBING = 0, VCA_BC_PERIODIC = 1 };
+/* CaMode (engine/src/core/Types.hpp:28) */
+enum { VCA_MODE_LAVA = 0, VCA_MODE_CLASSIC = 1 };
+/* Step schedule.  Both give bit-identical results (grids, histories, stop step), like the
+ * reference's ca.sweep = front / full (engine/src/ca/LavaCA.hpp:13-29):
+ *   ACTIVE -- tiles with no lava within one cell, and unchanged since the last step, are skipped;
+ *   DENSE  -- every cell of the grid is read and written every step. */
+enum { VCA_SWEEP_ACTIVE = 0, VCA_SWEEP_DENSE = 1 };
+/* StopReason (engine/src/ca/CaRules.hpp:108) */
+enum { VCA_STOP_RUNNING = 0, VCA_STOP_NO_LAVA = 1, VCA_STOP_NO_AIR = 2, VCA_STOP_NO_CHANGE = 3,
+       VCA_STOP_MAX_STEPS = 4 };
+/* CellType (engine/src/core/Types.hpp:13-19) */
+enum { VCA_AIR = 0, VCA_ROCK = 1, VCA_LAVA = 2, VCA_BASALT = 3, VCA_VOID = 255 };
+
+typedef struct vca_ca vca_ca;
+typedef struct vca_mc vca_mc;
+
+/* ------------------------------------------------------------------------------------------
+ * Lava cellular automaton -- replaces LavaCA<Storage> (engine/src/ca/LavaCA.hpp:80-271)
+ * ---------------------------------------------------------------------------------------- */
+
+/* Dims + CaParams (engine/src/ca/CaRules.hpp:93-105) + Neighborhood kind + Boundary kind.
+ * Temperatures are the float values the reference casts from the config
+ * (Simulation::caParams, engine/src/app/Simulation.cpp:122-136). */
+typedef struct {
+    int nx, ny, nz;
+    int neighborhood;          /* VCA_NB_* */
+    int boundary;              /* VCA_BC_* */
+    int mode;                  /* VCA_MODE_* */
+    uint64_t seed;             /* rngSeed */
+    int max_steps;             /* ca.maxSteps, 0..65535 */
+    int eruption_steps;        /* vents.eruptionSteps */
+    float erupt_temp;          /* vents.eruptTemp */
+    float solidus_temp;        /* ca.solidusTemp */
+    float cooling_ambient;     /* ca.coolingAmbient */
+    float cooling_lateral;     /* ca.coolingLateral */
+    float cooling_fall;        /* ca.coolingFall */
+    int ponding;               /* ca.ponding */
+    int sweep;                 /* VCA_SWEEP_* */
+    int device;                /* CUDA device ordinal */
+} vca_ca_desc;
+
+/* Vent (engine/src/terrain/VentPlacer.hpp:26-31). */
+typedef struct {
+    int x, y, z;
+    int32_t flow_id;
+} vca_vent;
+
+typedef struct {
+    int steps;                 /* LavaCA::steps() */
+    int stop_reason;           /* LavaCA::stopReason(), VCA_STOP_* */
+    uint64_t lava_cells;       /* LAVA cells now (classic: grains) */
+    uint64_t air_cells;        /* AIR cells now */
+    uint64_t tiles_total;      /* tiles of the grid */
+    uint64_t tiles_processed;  /* tile visits summed over all steps (DENSE: steps x tiles) */
+    uint64_t cells_per_tile;   /* cells one tile covers */
+} vca_ca_info;
+
+/* LavaCA ctor (LavaCA.hpp:84-144): all cells AIR, buffers on the device. */
+vca_status vca_ca_create(const vca_ca_desc* desc, vca_ca** out);
+/* LavaCA::applyTerrain (LavaCA.hpp:185-211): ROCK for z < h(x,y); spill levels by priority flood
+ * (TerrainGenerator::fillDepressions, engine/src/terrain/TerrainGenerator.cpp:86-161).
+ * heights: nx*ny values, x fastest.  Lava mode only. */
+vca_status vca_ca_apply_terrain(vca_ca* ca, const int32_t* heights);
+/* LavaCA::placeSeeds (LavaCA.hpp:215-227): vents become LAVA {flowId, eruptTemp (lava) or 0
+ * (classic)}; sets the initial stop state (countInitialState, LavaCA.hpp:1252-1280). */
+vca_status vca_ca_place_seeds(vca_ca* ca, const vca_vent* vents, int count);
+/* LavaCA::step (LavaCA.hpp:230-247); *running = !finished() afterwards. */
+vca_status vca_ca_step(vca_ca* ca, int* running);
+/* LavaCA::run (LavaCA.hpp:253-256): steps until the stop rule holds. */
+vca_status vca_ca_run(vca_ca* ca);
+/* steps(), stopReason() and counters (LavaCA.hpp:258-265). */
+vca_status vca_ca_get_info(vca_ca* ca, vca_ca_info* out);
+/* activeHistory() / changedHistory() (LavaCA.hpp:263-265): copies min(capacity, steps) entries;
+ * either pointer may be NULL. */
+vca_status vca_ca_history(vca_ca* ca, uint64_t* active, uint64_t* changed, int capacity, int* count);
+/* LavaCA::result() (LavaCA.hpp:271): current planes to host, unframed globalIndex order;
+ * any pointer may be NULL to skip that plane. */
+vca_status vca_ca_download(vca_ca* ca, uint8_t* type, int32_t* flow_id, float* temp, uint16_t* solid_step,
+                           uint16_t* arrival_step);
+/* Replace the whole state (test and resume hook; the reference reaches the same state through
+ * applyTerrain + placeSeeds + steps).  spill may be NULL (no terrain); vents give the isVent table
+ * (LavaCA.hpp:335-341) and are not written into the grid; steps_done is the step counter t. */
+vca_status vca_ca_set_state(vca_ca* ca, const uint8_t* type, const int32_t* flow_id, const float* temp,
+                            const uint16_t* solid_step, const uint16_t* arrival_step, const int32_t* spill,
+                            const vca_vent* vents, int vent_count, int steps_done);
+/* Spill levels in use (nx*ny, x fastest); returns VCA_ERR_STATE when there is no terrain. */
+vca_status vca_ca_get_spill(vca_ca* ca, int32_t* spill);
+/* Device time of the CA steps so far [ms] (CUDA events around the step launches) and the average
+ * duration of one launch of the rules kernel [ms] over the last vca_ca_run / vca_ca_step calls. */
+vca_status vca_ca_timing(vca_ca* ca, double* total_ms, double* rules_kernel_ms, uint64_t* rules_launches);
+void vca_ca_destroy(vca_ca* ca);
+
+/* ------------------------------------------------------------------------------------------
+ * Potts Monte Carlo, checkerboard update -- replaces PottsMC (engine/src/mc/PottsMC.hpp:52-152)
+ * with mc.update = "checkerboard".  mc.update = "random" is sequential by definition
+ * (engine/src/mc/McRules.hpp:30-32) and is not offered.
+ * ---------------------------------------------------------------------------------------- */
+
+/* PottsMC ctor arguments (PottsMC.cpp:14-46): Dims, McParams (engine/src/mc/McRules.hpp:80-85),
+ * Neighborhood kind and Boundary.  domain_full selects the boundary mode: 0 = basalt (lava
+ * boundary: z never periodic), 1 = full (classic boundary: all axes periodic when periodic)
+ * (McStage::run, engine/src/app/McStage.cpp:104-106). */
+typedef struct {
+    int nx, ny, nz;
+    int neighborhood;
+    int boundary;
+    int domain_full;
+    uint64_t seed;
+    int Q;
+    double J;
+    double kT;
+    int device;
+} vca_mc_desc;
+
+typedef struct {
+    int sweeps;                /* sweepsDone() */
+    int colors;                /* colorCount() */
+    uint64_t domain_cells;     /* domainCells() */
+    uint64_t attempts;         /* attempts() -- trials not skipped by mobility */
+    uint64_t accepted;         /* accepted() */
+    uint64_t uphill;           /* acceptedUphill() */
+} vca_mc_info;
+
+vca_status vca_mc_create(const vca_mc_desc* desc, vca_mc** out);
+/* setDomain / setDomainAll (PottsMC.cpp:61-83): in_domain is N bytes, or NULL for all cells. */
+vca_status vca_mc_set_domain(vca_mc* mc, const uint8_t* in_domain);
+/* setMobility (PottsMC.cpp:85-102): N floats, or NULL to switch mobility off. */
+vca_status vca_mc_set_mobility(vca_mc* mc, const float* mobility);
+/* CoolingMobility::basaltDomain (engine/src/mc/CoolingMobility.cpp:8-14) of the CA handle's
+ * current state, computed on the device without a host round trip. */
+vca_status vca_mc_set_domain_from_ca(vca_mc* mc, vca_ca* ca);
+/* CoolingMobility::fromCooling (CoolingMobility.cpp:16-83) of the CA handle's state, on the device.
+ * If use_in_dynamics is 0 the values are kept only for vca_mc_mobility() (the reference computes
+ * them for statistics even when mc.mobilityFromCooling is false). */
+vca_status vca_mc_set_mobility_from_ca(vca_mc* mc, vca_ca* ca, double mobility_min, int use_in_dynamics);
+/* Current mobility values (N floats, 0 outside the domain); VCA_ERR_STATE if none were set. */
+vca_status vca_mc_mobility(vca_mc* mc, float* out);
+/* PottsMC::initialize with setCheckerboard(true) (PottsMC.cpp:104-224). */
+vca_status vca_mc_initialize(vca_mc* mc);
+/* count x PottsMC::sweep (PottsMC.cpp:516-533); accepted (may be NULL) gets the accepted
+ * changes of these sweeps. */
+vca_status vca_mc_sweep(vca_mc* mc, int count, uint64_t* accepted);
+vca_status vca_mc_get_info(vca_mc* mc, vca_mc_info* out);
+/* PottsMC::totalEnergy (PottsMC.cpp:590-664). */
+vca_status vca_mc_energy(vca_mc* mc, double* energy);
+/* PottsMC::crystals (PottsMC.cpp:666-697): N int32, 0 outside the domain. */
+vca_status vca_mc_crystals(vca_mc* mc, int32_t* out);
+/* Overwrite all orientations (setOrientation for every cell, PottsMC.cpp:566-576); values
+ * outside the domain must be 0 and inside 1..Q. */
+vca_status vca_mc_set_spins(vca_mc* mc, const int32_t* spins);
+/* Device time of the sweeps so far [ms] and of one colour-pass launch on average [ms]. */
+vca_status vca_mc_timing(vca_mc* mc, double* total_ms, double* color_kernel_ms, uint64_t* color_launches);
+void vca_mc_destroy(vca_mc* mc);
+
+/* ------------------------------------------------------------------------------------------ */
+const char* vca_last_error(void);
+/* ABI version and build string ("vca <abi> sm_100a ..."). */
+const char* vca_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -218,3 +218,41 @@ def mc_energy(p: McParams, t: int, spin: np.ndarray) -> float:
 
 def mc_colors(p: McParams) -> int:
     return int(lib().vo_mc_colors(ctypes.byref(p)))
+
+
+def basalt_domain(s: CaState) -> np.ndarray:
+    """CoolingMobility::basaltDomain (engine/src/mc/CoolingMobility.cpp:8-14)."""
+    return ((s.type == BASALT) | (s.type == LAVA)).astype(np.uint8)
+
+
+def mobility_from_cooling(s: CaState, domain: np.ndarray, mobility_min: float) -> np.ndarray:
+    """CoolingMobility::fromCooling (engine/src/mc/CoolingMobility.cpp:16-83), float64 steps rounded
+    one by one as in the reference, then to float32."""
+    dom = domain.astype(bool)
+    mob = np.zeros(len(domain), np.float32)
+    if not dom.any():
+        return mob
+    end = int(np.maximum(s.solid[dom], s.arrival[dom]).max())
+    solid = np.where(s.type == BASALT, s.solid.astype(np.int64), end)
+    tm = np.where(dom, np.maximum(solid - s.arrival.astype(np.int64), 0), 0)
+    tmin, tmax = int(tm[dom].min()), int(tm[dom].max())
+    if tmax == tmin:
+        mob[dom] = 1.0
+        return mob
+    norm = (tm[dom] - tmin).astype(np.float64) / float(tmax - tmin)
+    mob[dom] = (mobility_min + (1.0 - mobility_min) * norm).astype(np.float32)
+    return mob
+
+
+def mc_params(nx, ny, nz, neighborhood: str, boundary: str, domain_full: bool, seed: int, Q: int, J: float,
+              kT: float) -> McParams:
+    """PottsMC periodicity from the boundary and the domain mode (PottsMC.cpp:18, McStage.cpp:104-106)."""
+    per = boundary == "periodic"
+    return McParams(nx, ny, nz, NB[neighborhood], (int(per and nx > 1), int(per and ny > 1),
+                                                   int(per and domain_full and nz > 1)), seed, Q, J, kT)
+
+
+def ca_stop_after(p: CaParams, steps_done: int, counts: np.ndarray) -> int:
+    """Stop reason after a step (LavaCA::finishStep, LavaCA.hpp:1206-1229)."""
+    c = np.ascontiguousarray(counts, np.uint64)
+    return int(lib().vo_ca_stop_after(ctypes.byref(p), steps_done, _ptr(c)))

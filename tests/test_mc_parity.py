@@ -1,0 +1,119 @@
+"""CUDA Potts checkerboard MC (libvca.so through the C ABI) against the CPU oracle, bit for bit:
+orientations after every sweep, attempts / accepted / uphill counters and the energy
+(PottsMC::sweep / totalEnergy, engine/src/mc/PottsMC.cpp:516-664)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import cases as C
+from volcano_ca_mc_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def _ca_result(nx, ny, nz, nb, bc, seed, steps=80):
+    """A basalt field from an oracle CA run (the MC domain of McStage::run)."""
+    p = capi.CaParams(nx, ny, nz, neighborhood=nb, boundary=bc, seed=seed, max_steps=steps, eruption_steps=steps // 3,
+                      cooling_ambient=3.0, cooling_lateral=4.0, cooling_fall=2.0)
+    heights = C.terrain(nx, ny, nz, seed)
+    vents = C.pick_vents(heights, nx, ny, nz, 2, seed)
+    per = bc == "periodic"
+    spill = O.fill_depressions(heights, nx, ny, per and nx > 1, per and ny > 1)
+    s0 = C.initial_state(nx, ny, nz, heights, vents, p.erupt_temp)
+    s, *_ = O.ca_run(C.oracle_params(p), s0, spill, O.vent_table(vents))
+    return p, heights, vents, s
+
+
+MC_CASES = [
+    # nx, ny, nz, nb, bc, Q, kT, mobility
+    (80, 1, 48, "moore", "absorbing", 50, 0.0, True),
+    (63, 1, 40, "hexagonal", "periodic", 32, 0.6, True),
+    (70, 1, 40, "von_neumann", "periodic", 64, 0.5, False),
+    (28, 22, 18, "moore", "absorbing", 128, 0.6, True),
+    (33, 17, 15, "pentagonal", "periodic", 64, 0.5, True),
+    (30, 30, 16, "von_neumann", "absorbing", 40, 0.0, False),
+]
+
+
+@pytest.mark.parametrize("case", MC_CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}-{c[3]}-{c[4]}-kT{c[6]}")
+def test_basalt_sweeps_match_oracle(case):
+    nx, ny, nz, nb, bc, Q, kT, use_mob = case
+    seed = 300 + nx + ny
+    _, _, _, s = _ca_result(nx, ny, nz, nb, bc, seed)
+    domain = O.basalt_domain(s)
+    assert domain.sum() > 20
+    mob = O.mobility_from_cooling(s, domain, 0.05)
+    mp = O.mc_params(nx, ny, nz, nb, bc, False, seed, Q, 1.0, kT)
+    spin = O.mc_init(mp, domain)
+
+    mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood=nb, boundary=bc, seed=seed, Q=Q, J=1.0, kT=kT))
+    mc.set_domain(domain)
+    if use_mob:
+        mc.set_mobility(mob)
+    mc.initialize()
+    info = mc.info()
+    assert info.colors == O.mc_colors(mp)
+    assert info.domain_cells == int(domain.sum())
+    assert np.array_equal(mc.crystals(), spin)
+    assert mc.energy() == O.mc_energy(mp, 0, spin)
+    tot = np.zeros(3, np.uint64)
+    for t in range(12):
+        tot += O.mc_sweep(mp, t, domain, mob if use_mob else None, spin)
+        acc = mc.sweep(1)
+        got = mc.crystals()
+        assert np.array_equal(got, spin), f"sweep {t + 1}: {(got != spin).sum()} cells differ"
+    info = mc.info()
+    assert (info.attempts, info.accepted, info.uphill) == tuple(int(v) for v in tot)
+    assert info.sweeps == 12
+    assert mc.energy() == O.mc_energy(mp, 12, spin)
+    mc.close()
+
+
+@pytest.mark.parametrize("nb,bc,dims", [("moore", "periodic", (25, 1, 31)), ("von_neumann", "periodic", (24, 20, 1)),
+                                        ("pentagonal", "periodic", (15, 13, 11)), ("von_neumann", "periodic", (9, 10, 7))])
+def test_full_domain_sweeps_match_oracle(nb, bc, dims):
+    """mc.domain = full: all axes periodic, odd periodic axes give 3 classes (PottsMC.cpp:145-193)."""
+    nx, ny, nz = dims
+    seed = 11 + nx
+    mp = O.mc_params(nx, ny, nz, nb, bc, True, seed, 20, 1.0, 0.4)
+    domain = np.ones(nx * ny * nz, np.uint8)
+    spin = O.mc_init(mp, domain)
+    mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood=nb, boundary=bc, domain_full=True, seed=seed, Q=20,
+                                    kT=0.4))
+    mc.set_domain(None)
+    mc.initialize()
+    assert mc.info().colors == O.mc_colors(mp)
+    tot = np.zeros(3, np.uint64)
+    for t in range(8):
+        tot += O.mc_sweep(mp, t, domain, None, spin)
+        mc.sweep(1)
+        assert np.array_equal(mc.crystals(), spin), f"sweep {t + 1}"
+    info = mc.info()
+    assert (info.attempts, info.accepted, info.uphill) == tuple(int(v) for v in tot)
+    assert mc.energy() == O.mc_energy(mp, 8, spin)
+    mc.close()
+
+
+def test_domain_and_mobility_from_ca_on_device():
+    """vca_mc_set_domain_from_ca / set_mobility_from_ca equal CoolingMobility on the host."""
+    nx, ny, nz = 40, 18, 20
+    p, heights, vents, s = _ca_result(nx, ny, nz, "moore", "absorbing", 21, steps=5000)
+    ca = capi.LavaCA(p)
+    ca.set_state(s.type, s.flow, s.temp, s.solid, s.arrival, None, vents, steps_done=0)
+    domain = O.basalt_domain(s)
+    mob = O.mobility_from_cooling(s, domain, 0.05)
+    mc = capi.PottsMC(capi.McParams(nx, ny, nz, seed=21, Q=64, kT=0.6))
+    mc.set_domain_from_ca(ca)
+    mc.set_mobility_from_ca(ca, 0.05, True)
+    got = mc.mobility()
+    assert np.array_equal(got.view(np.uint32), mob.view(np.uint32))
+    mc.initialize()
+    assert mc.info().domain_cells == int(domain.sum())
+    mp = O.mc_params(nx, ny, nz, "moore", "absorbing", False, 21, 64, 1.0, 0.6)
+    spin = O.mc_init(mp, domain)
+    for t in range(5):
+        O.mc_sweep(mp, t, domain, mob, spin)
+    mc.sweep(5)
+    assert np.array_equal(mc.crystals(), spin)
+    mc.close()
+    ca.close()

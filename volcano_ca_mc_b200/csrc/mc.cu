@@ -1,0 +1,835 @@
+// mc.cu -- Potts Monte Carlo crystallisation with the checkerboard update on sm_100a, and the
+// vca_mc_* half of the C ABI.
+//
+// One MCS (PottsMC::sweep -> sweepColors, engine/src/mc/PottsMC.cpp:451-533) is one launch per
+// colour.  The domain cells of a colour are a compact list of global indices (built once, in
+// globalIndex order, by a device stream compaction), so a colour pass touches only domain cells:
+// per trial it reads the list entry, the cell's mobility and spin, and its neighbours' spins
+// (shared with the neighbouring trials through L1/L2), and writes the spin when accepted.
+// Cells of one colour are never neighbours in any variant (PottsMC.cpp:160-165), so the trials
+// of a colour are independent and the order inside the pass does not matter.
+//
+// Acceptance is decided in integers: the reference accepts an uphill move when
+// toUniform(r) < exp(-dE/kT), i.e. (r >> 11) * 2^-53 < p.  Scaling by 2^53 is exact, so this is
+// (r >> 11) < ceil(p * 2^53); the thresholds are built on the host with the host's exp(), once
+// per (unlikeBefore, unlikeAfter) pair, and the device compares 64-bit integers.
+#include <cuda_runtime.h>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vca.h"
+#include "vca_device.cuh"
+#include "vca_internal.h"
+
+namespace vca {
+
+bool build_nb(int kind, int nx, int ny, int nz, NbTable& t);
+struct CaView {
+    const uint8_t* type;
+    const uint16_t* solid;
+    const uint16_t* arrival;
+    int nx, ny, nz, P;
+    cudaStream_t stream;
+    int device;
+};
+vca_status ca_view(vca_ca* h, CaView* v);
+
+constexpr int kMcThreads = 256;
+constexpr int kTableSide = 27;  // unlike counts 0..26
+
+// Exact 32-bit division by a runtime divisor (n < 2^32): q = (c * n) >> 64 with c = ceil(2^64 / d).
+struct FastDiv {
+    uint32_t d;
+    uint64_t c;
+};
+inline FastDiv make_fastdiv(uint32_t d) { return FastDiv{d, d <= 1 ? 0 : ~0ULL / d + 1}; }
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, FastDiv f) { return f.d <= 1 ? n : (uint32_t)__umul64hi(f.c, (uint64_t)n); }
+
+struct McCtrl {
+    uint32_t sweeps;
+    uint32_t ticket;
+    unsigned long long attempts;
+    unsigned long long accepted;
+    unsigned long long uphill;
+    unsigned long long energy_acc;
+    unsigned long long sweep_accepted;  // accepted in the running sweep
+};
+
+struct McArgs {
+    int nx, ny, nz;
+    int per[3];
+    FastDiv div_nx, div_ny;
+    int parity_colors;
+    int classes[3];
+    uint64_t seed;
+    FastMod q_mod;       // % Q (initial orientation)
+    FastMod qm1_mod;     // % (Q - 1) (proposal)
+    FastMod var_mod;     // % variants
+    int variants;
+    int32_t* spin;
+    const uint32_t* list;
+    const float* list_mob;
+    const unsigned long long* table;  // 27 x 27 acceptance thresholds
+    const NbTable* nb;
+    McCtrl* ctrl;
+};
+
+__device__ __forceinline__ bool mc_wrap(int& v, int n, int periodic) {
+    if (v >= 0 && v < n) return true;
+    if (!periodic || n == 1) return false;
+    v = v < 0 ? v + n : v - n;
+    return true;
+}
+// Spin of a neighbour through the frame: periodic copy or 0 (PottsMC::fillFrame, PottsMC.cpp:226-277).
+__device__ __forceinline__ int32_t spin_at(const McArgs& a, int x, int y, int z) {
+    if (!mc_wrap(x, a.nx, a.per[0]) || !mc_wrap(y, a.ny, a.per[1]) || !mc_wrap(z, a.nz, a.per[2])) return 0;
+    return a.spin[(uint64_t)x + (uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z)];
+}
+
+// PottsMC::axisClass / colorOf (PottsMC.cpp:145-158), colour numbering of buildColors (173-193).
+__host__ __device__ inline int axis_class(int c, int n, int periodic) {
+    if (periodic && (n % 2) == 1 && c == n - 1) return 2;
+    return c & 1;
+}
+__host__ __device__ inline int color_of(const McArgs& a, int x, int y, int z) {
+    if (a.parity_colors) return (x + y + z) & 1;
+    const int cx = axis_class(x, a.nx, a.per[0]), cy = axis_class(y, a.ny, a.per[1]), cz = axis_class(z, a.nz, a.per[2]);
+    return cx + a.classes[0] * (cy + a.classes[1] * cz);
+}
+
+__device__ __forceinline__ void decode(const McArgs& a, uint32_t g, int& x, int& y, int& z) {
+    const uint32_t r = fdiv(g, a.div_nx);
+    x = (int)(g - r * (uint32_t)a.nx);
+    const uint32_t zz = fdiv(r, a.div_ny);
+    y = (int)(r - zz * (uint32_t)a.ny);
+    z = (int)zz;
+}
+
+// PottsMC::initialize (PottsMC.cpp:104-143): 1 + hashRand(seed, 0, g, McInit) % Q in the domain.
+__global__ void mc_init_kernel(McArgs a, const uint8_t* domain, uint64_t n) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
+        int32_t s = 0;
+        if (domain[g]) s = 1 + (int32_t)fast_mod(hash_salt(hash_index(hash_prefix(a.seed, 0), g), kSaltMcInit), a.q_mod);
+        a.spin[g] = s;
+    }
+}
+
+struct ColorPred {
+    McArgs a;
+    const uint8_t* domain;
+    int color;
+    __device__ bool operator()(uint32_t g) const {
+        if (!domain[g]) return false;
+        int x, y, z;
+        decode(a, g, x, y, z);
+        return color_of(a, x, y, z) == color;
+    }
+};
+
+__global__ void mc_gather_mob_kernel(const uint32_t* list, const float* mob, float* out, uint64_t n) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+        out[j] = mob[list[j]];
+}
+
+// One colour of one MCS: colorTrials (PottsMC.cpp:394-448) for the list entries [0, count).
+template <bool kMobility, bool kRandomNb>
+__global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const uint32_t* list, const float* list_mob,
+                                                              uint64_t count, int last_color) {
+    __shared__ unsigned long long s_table[kTableSide * kTableSide];
+    __shared__ unsigned long long s_red[3][kMcThreads / 32];
+    __shared__ bool s_last;
+    for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
+    __syncthreads();
+    McCtrl* ctrl = a.ctrl;
+    const uint32_t t = ctrl->sweeps;
+    const uint64_t prefix = hash_prefix(a.seed, t);
+    const NbTable& nb = *a.nb;
+    unsigned my_att = 0, my_acc = 0, my_up = 0;
+    for (uint64_t j = blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < count; j += (uint64_t)gridDim.x * kMcThreads) {
+        const uint32_t g = list[j];
+        const uint64_t h = hash_index(prefix, g);
+        if (kMobility) {
+            const uint64_t r = hash_salt(h, kSaltMcMobility);
+            if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)list_mob[j]) continue;
+        }
+        ++my_att;
+        int var = 0;
+        if (kRandomNb) var = (int)fast_mod(hash_salt(h, kSaltNeighborhood), a.var_mod);
+        int x, y, z;
+        decode(a, g, x, y, z);
+        const int32_t cur = a.spin[g];
+        int32_t prop = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
+        if (prop >= cur) ++prop;
+        int in_dom = 0, same_a = 0, same_b = 0;
+        const int cnt = nb.count[var];
+        for (int k = 0; k < cnt; ++k) {
+            const int32_t sj = spin_at(a, x + nb.off[var][k][0], y + nb.off[var][k][1], z + nb.off[var][k][2]);
+            in_dom += sj != 0;
+            same_a += sj == cur;
+            same_b += sj == prop;
+        }
+        const int before = in_dom - same_a, after = in_dom - same_b;
+        const unsigned long long e = s_table[before * kTableSide + after];
+        bool accept;
+        if (e >> 63) {
+            accept = true;
+        } else {
+            accept = e != 0 && (hash_salt(h, kSaltMcAccept) >> 11) < e;
+            my_up += accept ? 1u : 0u;
+        }
+        if (accept) {
+            a.spin[g] = prop;
+            ++my_acc;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned ra = __reduce_add_sync(0xFFFFFFFFu, my_att);
+    const unsigned rc = __reduce_add_sync(0xFFFFFFFFu, my_acc);
+    const unsigned ru = __reduce_add_sync(0xFFFFFFFFu, my_up);
+    if (lane == 0) {
+        s_red[0][warp] = ra;
+        s_red[1][warp] = rc;
+        s_red[2][warp] = ru;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long sa = 0, sc = 0, su = 0;
+        for (int w = 0; w < kMcThreads / 32; ++w) {
+            sa += s_red[0][w];
+            sc += s_red[1][w];
+            su += s_red[2][w];
+        }
+        if (sa) atomicAdd(&ctrl->attempts, sa);
+        if (sc) {
+            atomicAdd(&ctrl->accepted, sc);
+            atomicAdd(&ctrl->sweep_accepted, sc);
+        }
+        if (su) atomicAdd(&ctrl->uphill, su);
+        s_last = false;
+        if (last_color) {
+            __threadfence();
+            s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
+        }
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        ctrl->ticket = 0;
+        ctrl->sweeps = t + 1;   // ++sweeps_ (PottsMC.cpp:531)
+        __threadfence();
+    }
+}
+
+// PottsMC::totalEnergy (PottsMC.cpp:590-664): unlike pairs.  Deterministic neighbourhoods count
+// each pair once through the forward offsets; random ones sum E_i over the cells with the
+// variant of MCS t (the caller halves it).
+__global__ __launch_bounds__(kMcThreads) void mc_energy_kernel(McArgs a, const uint32_t* list, uint64_t count, int forward) {
+    __shared__ unsigned long long s_sum;
+    if (threadIdx.x == 0) s_sum = 0;
+    __syncthreads();
+    const NbTable& nb = *a.nb;
+    const uint64_t prefix = hash_prefix(a.seed, a.ctrl->sweeps);
+    unsigned long long mine = 0;
+    for (uint64_t j = blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < count; j += (uint64_t)gridDim.x * kMcThreads) {
+        const uint32_t g = list[j];
+        int x, y, z;
+        decode(a, g, x, y, z);
+        const int32_t s = a.spin[g];
+        int var = 0;
+        if (!forward && a.variants > 1) var = (int)fast_mod(hash_salt(hash_index(prefix, g), kSaltNeighborhood), a.var_mod);
+        int in_dom = 0, same = 0;
+        for (int k = 0; k < nb.count[var]; ++k) {
+            const int dx = nb.off[var][k][0], dy = nb.off[var][k][1], dz = nb.off[var][k][2];
+            if (forward && !(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
+            const int32_t sj = spin_at(a, x + dx, y + dy, z + dz);
+            in_dom += sj != 0;
+            same += sj == s;
+        }
+        mine += (unsigned long long)(in_dom - same);
+    }
+    for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_sum, mine);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum) atomicAdd(&a.ctrl->energy_acc, s_sum);
+}
+
+// CoolingMobility (engine/src/mc/CoolingMobility.cpp) on the device.
+__global__ void mc_domain_from_ca_kernel(const uint8_t* type, int nx, int P, uint64_t rows, uint8_t* domain) {
+    const uint64_t n = (uint64_t)nx * rows;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = g / nx;
+        const int x = (int)(g - r * nx);
+        const uint8_t t = type[r * P + x];
+        domain[g] = (t == kBasalt || t == kLava) ? 1 : 0;  // basaltDomain (CoolingMobility.cpp:8-14)
+    }
+}
+
+// endStep: largest solidStep / arrivalStep in the domain (CoolingMobility.cpp:16-25).
+__global__ void mc_end_step_kernel(const uint16_t* solid, const uint16_t* arrival, const uint8_t* domain, int nx, int P,
+                                   uint64_t rows, unsigned int* end_step) {
+    unsigned m = 0;
+    const uint64_t n = (uint64_t)nx * rows;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
+        if (!domain[g]) continue;
+        const uint64_t r = g / nx;
+        const uint64_t p = r * P + (g - r * nx);
+        m = max(m, (unsigned)max(solid[p], arrival[p]));
+    }
+    m = __reduce_max_sync(0xFFFFFFFFu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(end_step, m);
+}
+
+// liquidTime (CoolingMobility.cpp:32-45) and its range (timeRange, 47-56): mm[0] = min, mm[1] = max.
+__global__ void mc_time_range_kernel(const uint8_t* type, const uint16_t* solid, const uint16_t* arrival,
+                                     const uint8_t* domain, int nx, int P, uint64_t rows, const unsigned int* end_step,
+                                     unsigned int* time, unsigned int* mm) {
+    unsigned lo = 0xFFFFFFFFu, hi = 0;
+    const unsigned end = *end_step;
+    const uint64_t n = (uint64_t)nx * rows;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
+        unsigned tm = 0;
+        if (domain[g]) {
+            const uint64_t r = g / nx;
+            const uint64_t p = r * P + (g - r * nx);
+            const unsigned s = type[p] == kBasalt ? solid[p] : end;
+            const unsigned ar = arrival[p];
+            tm = s > ar ? s - ar : 0;
+            lo = min(lo, tm);
+            hi = max(hi, tm);
+        }
+        time[g] = tm;
+    }
+    lo = __reduce_min_sync(0xFFFFFFFFu, lo);
+    hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], lo);
+        atomicMax(&mm[1], hi);
+    }
+}
+
+// normalize (CoolingMobility.cpp:58-74): mobilityMin + (1 - mobilityMin) * (t - tMin) / (tMax - tMin)
+// in double, each operation rounded once (no contraction), then to float.
+__global__ void mc_normalize_kernel(const unsigned int* time, const uint8_t* domain, const unsigned int* mm,
+                                    double mobility_min, uint64_t n, float* mobility) {
+    const unsigned lo = mm[0], hi = mm[1];
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
+        float m = 0.0f;
+        if (domain[g]) {
+            if (hi == lo) {
+                m = 1.0f;
+            } else {
+                const double norm = __ddiv_rn((double)(time[g] - lo), (double)(hi - lo));
+                m = __double2float_rn(__dadd_rn(mobility_min, __dmul_rn(__dsub_rn(1.0, mobility_min), norm)));
+            }
+        }
+        mobility[g] = m;
+    }
+}
+
+}  // namespace vca
+
+using namespace vca;
+
+struct vca_mc {
+    vca_mc_desc desc;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    NbTable nb_host;
+    NbTable* nb = nullptr;
+    int per[3] = {0, 0, 0};
+    int colors = 0;
+    int parity_colors = 0;
+    int classes[3] = {1, 1, 1};
+    uint64_t n = 0;
+    int32_t* spin = nullptr;
+    uint8_t* domain = nullptr;
+    float* mobility = nullptr;     // N floats when set
+    bool mobility_set = false;
+    bool mobility_on = false;
+    uint32_t* list = nullptr;      // domain cells by colour
+    float* list_mob = nullptr;
+    std::vector<uint64_t> color_off;
+    unsigned long long* table = nullptr;
+    McCtrl* ctrl = nullptr;
+    McCtrl* ctrl_host = nullptr;
+    bool domain_set = false;
+    bool initialized = false;
+    int sms = 148;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    double total_ms = 0.0;
+    double color_ms = 0.0;
+    uint64_t color_launches = 0;
+    int profile_kernels = 0;
+    std::vector<cudaEvent_t> prof_events;
+};
+
+namespace {
+
+vca_status mc_check(const vca_mc* h) {
+    if (!h) {
+        set_error("null vca_mc handle");
+        return VCA_ERR_ARG;
+    }
+    return VCA_OK;
+}
+
+McArgs mc_args(const vca_mc* h) {
+    McArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.nx = h->desc.nx;
+    a.ny = h->desc.ny;
+    a.nz = h->desc.nz;
+    for (int i = 0; i < 3; ++i) {
+        a.per[i] = h->per[i];
+        a.classes[i] = h->classes[i];
+    }
+    a.div_nx = make_fastdiv((uint32_t)a.nx);
+    a.div_ny = make_fastdiv((uint32_t)a.ny);
+    a.parity_colors = h->parity_colors;
+    a.seed = h->desc.seed;
+    a.q_mod = make_fastmod((uint64_t)h->desc.Q);
+    a.qm1_mod = make_fastmod((uint64_t)(h->desc.Q - 1));
+    a.var_mod = make_fastmod((uint64_t)h->nb_host.variants);
+    a.variants = h->nb_host.variants;
+    a.spin = h->spin;
+    a.list = h->list;
+    a.list_mob = h->list_mob;
+    a.table = h->table;
+    a.nb = h->nb;
+    a.ctrl = h->ctrl;
+    return a;
+}
+
+vca_status mc_sync(vca_mc* h) {
+    VCA_CUDA(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(McCtrl), cudaMemcpyDeviceToHost, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    return VCA_OK;
+}
+
+int grid_for(uint64_t work, int sms) {
+    const uint64_t b = (work + kMcThreads - 1) / kMcThreads;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms * 16));
+}
+
+void mc_free(vca_mc* h) {
+    cudaSetDevice(h->device);
+    cudaFree(h->nb);
+    cudaFree(h->spin);
+    cudaFree(h->domain);
+    cudaFree(h->mobility);
+    cudaFree(h->list);
+    cudaFree(h->list_mob);
+    cudaFree(h->table);
+    cudaFree(h->ctrl);
+    if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
+    if (h->ev_a) cudaEventDestroy(h->ev_a);
+    if (h->ev_b) cudaEventDestroy(h->ev_b);
+    for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+vca_status vca_mc_create(const vca_mc_desc* d, vca_mc** out) {
+    if (!d || !out) {
+        set_error("vca_mc_create: null argument");
+        return VCA_ERR_ARG;
+    }
+    *out = nullptr;
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1 || (d->nx > 1) + (d->ny > 1) + (d->nz > 1) < 2) {
+        set_error("vca_mc_create: the space must be 2D or 3D");
+        return VCA_ERR_ARG;
+    }
+    const uint64_t n = (uint64_t)d->nx * d->ny * d->nz;
+    if (n > 2000000000ULL) {
+        set_error("vca_mc_create: more than 2 000 000 000 cells");
+        return VCA_ERR_ARG;
+    }
+    if (d->Q < 2) {
+        set_error("vca_mc_create: Q must be at least 2 (PottsMC needs two orientations)");
+        return VCA_ERR_ARG;
+    }
+    if (!(d->J > 0.0) || !(d->kT >= 0.0)) {
+        set_error("vca_mc_create: J must be > 0 and kT >= 0");
+        return VCA_ERR_ARG;
+    }
+    vca_mc* h = new vca_mc();
+    h->desc = *d;
+    h->device = d->device;
+    h->n = n;
+    if (!build_nb(d->neighborhood, d->nx, d->ny, d->nz, h->nb_host)) {
+        delete h;
+        set_error("vca_mc_create: the hexagonal neighbourhood is defined in 2D only");
+        return VCA_ERR_ARG;
+    }
+    auto fail = [&](vca_status s) {
+        mc_free(h);
+        delete h;
+        return s;
+    };
+    cudaError_t e = cudaSetDevice(d->device);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, d->device)) != cudaSuccess) return fail(cuda_fail(e, "cudaGetDeviceProperties"));
+    if (prop.major < 10) {
+        set_error("vca_mc_create: needs an sm_100 (Blackwell) device");
+        return fail(VCA_ERR_CUDA);
+    }
+    h->sms = prop.multiProcessorCount;
+    // Periodic axes: PottsMC ctor (PottsMC.cpp:18) with the Boundary of McStage::run (McStage.cpp:106).
+    const bool periodic = d->boundary == VCA_BC_PERIODIC;
+    h->per[0] = periodic && d->nx > 1;
+    h->per[1] = periodic && d->ny > 1;
+    h->per[2] = periodic && d->domain_full && d->nz > 1;
+    // Colours (PottsMC::buildColors, PottsMC.cpp:160-193).
+    const int dims[3] = {d->nx, d->ny, d->nz};
+    bool odd = false;
+    for (int a = 0; a < 3; ++a) odd = odd || (h->per[a] && dims[a] % 2 == 1);
+    h->parity_colors = d->neighborhood == VCA_NB_VON_NEUMANN && !odd;
+    if (h->parity_colors) {
+        h->colors = 2;
+    } else {
+        h->colors = 1;
+        for (int a = 0; a < 3; ++a) {
+            h->classes[a] = dims[a] == 1 ? 1 : (h->per[a] && dims[a] % 2 == 1 ? 3 : 2);
+            h->colors *= h->classes[a];
+        }
+    }
+    // Acceptance thresholds for every (unlikeBefore, unlikeAfter): dE = J*after - J*before
+    // (PottsMC.cpp:431); dE <= 0 always (bit 63), else ceil(exp(-dE/kT) * 2^53), or 0 when kT = 0.
+    std::vector<unsigned long long> table(kTableSide * kTableSide, 0);
+    for (int b = 0; b < kTableSide; ++b)
+        for (int a = 0; a < kTableSide; ++a) {
+            const double dE = d->J * a - d->J * b;
+            unsigned long long v = 0;
+            if (dE <= 0.0) {
+                v = 1ULL << 63;
+            } else if (d->kT > 0.0) {
+                const double p = std::exp(-dE / d->kT);
+                v = (unsigned long long)std::ceil(p * 9007199254740992.0);
+            }
+            table[b * kTableSide + a] = v;
+        }
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
+    if ((e = cudaMalloc(&h->nb, sizeof(NbTable))) != cudaSuccess || (e = cudaMalloc(&h->spin, 4 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->domain, n)) != cudaSuccess || (e = cudaMalloc(&h->table, 8 * table.size())) != cudaSuccess ||
+        (e = cudaMalloc(&h->ctrl, sizeof(McCtrl))) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaMalloc"));
+    if ((e = cudaMallocHost(&h->ctrl_host, sizeof(McCtrl))) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaMemcpyAsync(h->nb, &h->nb_host, sizeof(NbTable), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->table, table.data(), 8 * table.size(), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->spin, 0, 4 * n, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->domain, 0, n, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream)) != cudaSuccess)
+        return fail(cuda_fail(e, "upload"));
+    if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaEventCreate"));
+    const char* prof = std::getenv("VCA_PROFILE_KERNELS");
+    h->profile_kernels = prof != nullptr && prof[0] == '1';
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return fail(cuda_fail(e, "cudaStreamSynchronize"));
+    *out = h;
+    return VCA_OK;
+}
+
+vca_status vca_mc_set_domain(vca_mc* h, const uint8_t* in_domain) {
+    if (vca_status s = mc_check(h)) return s;
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (in_domain) {
+        std::vector<uint8_t> d(in_domain, in_domain + h->n);
+        for (auto& v : d) v = v ? 1 : 0;
+        VCA_CUDA(cudaMemcpyAsync(h->domain, d.data(), h->n, cudaMemcpyHostToDevice, h->stream));
+        VCA_CUDA(cudaStreamSynchronize(h->stream));
+    } else {
+        VCA_CUDA(cudaMemsetAsync(h->domain, 1, h->n, h->stream));
+    }
+    h->domain_set = true;
+    h->initialized = false;
+    return VCA_OK;
+}
+
+vca_status vca_mc_set_mobility(vca_mc* h, const float* mobility) {
+    if (vca_status s = mc_check(h)) return s;
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (!mobility) {
+        h->mobility_on = false;
+        return VCA_OK;
+    }
+    if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->n));
+    VCA_CUDA(cudaMemcpyAsync(h->mobility, mobility, 4 * h->n, cudaMemcpyHostToDevice, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    h->mobility_set = true;
+    h->mobility_on = true;
+    h->initialized = false;
+    return VCA_OK;
+}
+
+vca_status vca_mc_set_domain_from_ca(vca_mc* h, vca_ca* ca) {
+    if (vca_status s = mc_check(h)) return s;
+    CaView v;
+    if (vca_status s = ca_view(ca, &v)) return s;
+    if (v.nx != h->desc.nx || v.ny != h->desc.ny || v.nz != h->desc.nz) {
+        set_error("vca_mc_set_domain_from_ca: CA and MC dimensions differ");
+        return VCA_ERR_ARG;
+    }
+    if (v.device != h->device) {
+        set_error("vca_mc_set_domain_from_ca: CA and MC handles live on different devices");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    VCA_CUDA(cudaStreamSynchronize(v.stream));
+    mc_domain_from_ca_kernel<<<h->sms * 8, 256, 0, h->stream>>>(v.type, v.nx, v.P, (uint64_t)v.ny * v.nz, h->domain);
+    VCA_CUDA(cudaGetLastError());
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    h->domain_set = true;
+    h->initialized = false;
+    return VCA_OK;
+}
+
+vca_status vca_mc_set_mobility_from_ca(vca_mc* h, vca_ca* ca, double mobility_min, int use_in_dynamics) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!h->domain_set) {
+        set_error("vca_mc_set_mobility_from_ca: set the domain first");
+        return VCA_ERR_STATE;
+    }
+    CaView v;
+    if (vca_status s = ca_view(ca, &v)) return s;
+    if (v.nx != h->desc.nx || v.ny != h->desc.ny || v.nz != h->desc.nz || v.device != h->device) {
+        set_error("vca_mc_set_mobility_from_ca: CA and MC handles do not match");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    VCA_CUDA(cudaStreamSynchronize(v.stream));
+    if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->n));
+    unsigned int* scratch = nullptr;  // [end, min, max] + time[n]
+    VCA_CUDA(cudaMalloc(&scratch, 4 * (3 + h->n)));
+    const unsigned int init[3] = {0u, 0xFFFFFFFFu, 0u};
+    VCA_CUDA(cudaMemcpyAsync(scratch, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+    const uint64_t rows = (uint64_t)v.ny * v.nz;
+    const int blocks = h->sms * 8;
+    mc_end_step_kernel<<<blocks, 256, 0, h->stream>>>(v.solid, v.arrival, h->domain, v.nx, v.P, rows, scratch);
+    mc_time_range_kernel<<<blocks, 256, 0, h->stream>>>(v.type, v.solid, v.arrival, h->domain, v.nx, v.P, rows, scratch,
+                                                        scratch + 3, scratch + 1);
+    mc_normalize_kernel<<<blocks, 256, 0, h->stream>>>(scratch + 3, h->domain, scratch + 1, mobility_min, h->n, h->mobility);
+    cudaError_t e = cudaGetLastError();
+    cudaError_t e2 = cudaStreamSynchronize(h->stream);
+    cudaFree(scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "mobility kernels");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "mobility kernels");
+    h->mobility_set = true;
+    h->mobility_on = use_in_dynamics != 0;
+    h->initialized = false;
+    return VCA_OK;
+}
+
+vca_status vca_mc_mobility(vca_mc* h, float* out) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!h->mobility_set) {
+        set_error("vca_mc_mobility: no mobility was set");
+        return VCA_ERR_STATE;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    VCA_CUDA(cudaMemcpyAsync(out, h->mobility, 4 * h->n, cudaMemcpyDeviceToHost, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    return VCA_OK;
+}
+
+vca_status vca_mc_initialize(vca_mc* h) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!h->domain_set) {
+        set_error("vca_mc_initialize: set the domain first");
+        return VCA_ERR_STATE;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    McArgs a = mc_args(h);
+    mc_init_kernel<<<h->sms * 8, 256, 0, h->stream>>>(a, h->domain, h->n);
+    VCA_CUDA(cudaGetLastError());
+    // Colour lists, colour by colour, globalIndex ascending inside a colour (PottsMC.cpp:194-223).
+    cudaFree(h->list);
+    h->list = nullptr;
+    cudaFree(h->list_mob);
+    h->list_mob = nullptr;
+    unsigned long long* d_count = nullptr;
+    VCA_CUDA(cudaMalloc(&d_count, 8 * (size_t)h->colors));
+    VCA_CUDA(cudaMemsetAsync(d_count, 0, 8 * (size_t)h->colors, h->stream));
+    size_t temp_bytes = 0;
+    ColorPred pred{a, h->domain, 0};
+    thrust::counting_iterator<uint32_t> it(0);
+    // A domain bound for the list: count of domain cells.
+    std::vector<uint8_t> dummy;
+    uint32_t* all = nullptr;
+    VCA_CUDA(cudaMalloc(&all, 4 * h->n));
+    VCA_CUDA(cub::DeviceSelect::If(nullptr, temp_bytes, it, all, d_count, (int64_t)h->n, pred, h->stream));
+    void* temp = nullptr;
+    VCA_CUDA(cudaMalloc(&temp, temp_bytes));
+    std::vector<unsigned long long> counts((size_t)h->colors, 0);
+    h->color_off.assign((size_t)h->colors + 1, 0);
+    uint64_t total = 0;
+    for (int c = 0; c < h->colors; ++c) {
+        pred.color = c;
+        VCA_CUDA(cub::DeviceSelect::If(temp, temp_bytes, it, all + total, d_count + c, (int64_t)h->n, pred, h->stream));
+        VCA_CUDA(cudaMemcpyAsync(&counts[c], d_count + c, 8, cudaMemcpyDeviceToHost, h->stream));
+        VCA_CUDA(cudaStreamSynchronize(h->stream));
+        h->color_off[c] = total;
+        total += counts[c];
+    }
+    h->color_off[h->colors] = total;
+    cudaFree(temp);
+    cudaFree(d_count);
+    VCA_CUDA(cudaMalloc(&h->list, 4 * std::max<uint64_t>(total, 1)));
+    if (total) VCA_CUDA(cudaMemcpyAsync(h->list, all, 4 * total, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->mobility_on) {
+        VCA_CUDA(cudaMalloc(&h->list_mob, 4 * std::max<uint64_t>(total, 1)));
+        if (total) mc_gather_mob_kernel<<<grid_for(total, h->sms), 256, 0, h->stream>>>(h->list, h->mobility, h->list_mob, total);
+        VCA_CUDA(cudaGetLastError());
+    }
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    cudaFree(all);
+    VCA_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    h->initialized = true;
+    return VCA_OK;
+}
+
+vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!h->initialized) {
+        set_error("vca_mc_sweep: initialize first");
+        return VCA_ERR_STATE;
+    }
+    if (count < 0) {
+        set_error("vca_mc_sweep: negative count");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    McArgs a = mc_args(h);
+    VCA_CUDA(cudaMemsetAsync(&h->ctrl->sweep_accepted, 0, 8, h->stream));
+    VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
+    const bool random_nb = h->nb_host.variants > 1;
+    size_t ev_used = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
+    for (int s = 0; s < count; ++s) {
+        for (int c = 0; c < h->colors; ++c) {
+            const uint64_t b = h->color_off[c], e = h->color_off[c + 1];
+            const uint64_t cnt = e - b;
+            const int grid = grid_for(cnt, h->sms);
+            const uint32_t* list = h->list + b;
+            const float* mob = h->mobility_on ? h->list_mob + b : nullptr;
+            const int last = c == h->colors - 1;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (h->profile_kernels) {
+                while (h->prof_events.size() < ev_used + 2) {
+                    cudaEvent_t ev;
+                    VCA_CUDA(cudaEventCreate(&ev));
+                    h->prof_events.push_back(ev);
+                }
+                e0 = h->prof_events[ev_used];
+                e1 = h->prof_events[ev_used + 1];
+                ev_used += 2;
+                VCA_CUDA(cudaEventRecord(e0, h->stream));
+            }
+            if (h->mobility_on) {
+                if (random_nb) mc_color_kernel<true, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+                else mc_color_kernel<true, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+            } else {
+                if (random_nb) mc_color_kernel<false, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+                else mc_color_kernel<false, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+            }
+            if (h->profile_kernels) {
+                VCA_CUDA(cudaEventRecord(e1, h->stream));
+                prof.push_back({e0, e1});
+            }
+        }
+        if (h->profile_kernels && prof.size() > 2048) break;  // bounded event pool per call
+    }
+    VCA_CUDA(cudaGetLastError());
+    VCA_CUDA(cudaEventRecord(h->ev_b, h->stream));
+    VCA_CUDA(cudaEventSynchronize(h->ev_b));
+    float ms = 0.f;
+    VCA_CUDA(cudaEventElapsedTime(&ms, h->ev_a, h->ev_b));
+    h->total_ms += ms;
+    for (auto& pr : prof) {
+        float m = 0.f;
+        VCA_CUDA(cudaEventElapsedTime(&m, pr.first, pr.second));
+        h->color_ms += m;
+        ++h->color_launches;
+    }
+    if (vca_status s_ = mc_sync(h)) return s_;
+    if (accepted) *accepted = h->ctrl_host->sweep_accepted;
+    return VCA_OK;
+}
+
+vca_status vca_mc_get_info(vca_mc* h, vca_mc_info* out) {
+    if (vca_status s = mc_check(h)) return s;
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (vca_status s_ = mc_sync(h)) return s_;
+    out->sweeps = (int)h->ctrl_host->sweeps;
+    out->colors = h->colors;
+    out->domain_cells = h->initialized ? h->color_off.back() : 0;
+    out->attempts = h->ctrl_host->attempts;
+    out->accepted = h->ctrl_host->accepted;
+    out->uphill = h->ctrl_host->uphill;
+    return VCA_OK;
+}
+
+vca_status vca_mc_energy(vca_mc* h, double* energy) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!h->initialized) {
+        set_error("vca_mc_energy: initialize first");
+        return VCA_ERR_STATE;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    VCA_CUDA(cudaMemsetAsync(&h->ctrl->energy_acc, 0, 8, h->stream));
+    const uint64_t total = h->color_off.back();
+    const bool forward = h->nb_host.variants == 1;
+    if (total) mc_energy_kernel<<<grid_for(total, h->sms), kMcThreads, 0, h->stream>>>(mc_args(h), h->list, total, forward);
+    VCA_CUDA(cudaGetLastError());
+    if (vca_status s_ = mc_sync(h)) return s_;
+    const double unlike = (double)h->ctrl_host->energy_acc;
+    *energy = forward ? h->desc.J * unlike : 0.5 * h->desc.J * unlike;
+    return VCA_OK;
+}
+
+vca_status vca_mc_crystals(vca_mc* h, int32_t* out) {
+    if (vca_status s = mc_check(h)) return s;
+    VCA_CUDA(cudaSetDevice(h->device));
+    VCA_CUDA(cudaMemcpyAsync(out, h->spin, 4 * h->n, cudaMemcpyDeviceToHost, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    return VCA_OK;
+}
+
+vca_status vca_mc_set_spins(vca_mc* h, const int32_t* spins) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!spins) {
+        set_error("vca_mc_set_spins: null spins");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    VCA_CUDA(cudaMemcpyAsync(h->spin, spins, 4 * h->n, cudaMemcpyHostToDevice, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    return VCA_OK;
+}
+
+vca_status vca_mc_timing(vca_mc* h, double* total_ms, double* color_kernel_ms, uint64_t* color_launches) {
+    if (vca_status s = mc_check(h)) return s;
+    if (total_ms) *total_ms = h->total_ms;
+    if (color_kernel_ms) *color_kernel_ms = h->color_launches ? h->color_ms / (double)h->color_launches : 0.0;
+    if (color_launches) *color_launches = h->color_launches;
+    return VCA_OK;
+}
+
+void vca_mc_destroy(vca_mc* h) {
+    if (!h) return;
+    mc_free(h);
+    delete h;
+}
+
+}  // extern "C"

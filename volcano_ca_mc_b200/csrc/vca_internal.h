@@ -1,0 +1,131 @@
+// vca_internal.h -- handle layouts and helpers shared by the CA and MC halves of libvca.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "vca.h"
+#include "vca_device.cuh"
+
+namespace vca {
+
+// Error channel of the C ABI: the message of the last failure on this host thread.
+void set_error(const std::string& msg);
+vca_status cuda_fail(cudaError_t e, const char* what);
+
+#define VCA_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t e__ = (call);                                   \
+        if (e__ != cudaSuccess) return ::vca::cuda_fail(e__, #call); \
+    } while (0)
+
+// Device-side control block of a CA handle: step counter, stop state, per-step accumulators and
+// the active-tile list lengths.  Written by the last block of each rules launch.
+struct CaCtrl {
+    uint32_t steps;           // steps done (t of the next step)
+    int32_t stop;             // VCA_STOP_*
+    uint64_t lava;            // LAVA cells after the last step (classic: grains)
+    uint64_t air;             // AIR cells after the last step
+    unsigned long long acc_active;   // accumulators of the running step
+    unsigned long long acc_changed;
+    unsigned long long acc_born;
+    unsigned long long acc_tiles;
+    unsigned int ticket;      // blocks finished in the running rules launch
+    unsigned int list_count[2];
+    unsigned int pad;
+    unsigned long long tiles_processed;  // tiles visited over all steps
+    int32_t max_steps;
+    int32_t random_nb;
+    int32_t classic;
+    int32_t pad2;
+};
+
+// Geometry of the pitched device planes.  Each (y, z) row holds P >= nx cells, P a multiple of 64,
+// so that every row starts 64-byte aligned in every plane; cells x >= nx are VOID padding.
+struct CaGeom {
+    int nx, ny, nz;
+    int P;                    // row pitch in cells
+    int per[3];               // periodic axes (Boundary, engine/src/core/Boundary.cpp:5-11)
+    int TY, TZ;               // tile rows: TY * TZ = 16, tile = 64 x TY x TZ cells
+    int tiles_x, tiles_y, tiles_z;
+};
+
+struct CaTables {
+    NbTable nb;
+    int nside;
+    int8_t side[8][3];        // union of the dz == 0 offsets of all variants (LavaCA.hpp:104-112)
+};
+
+struct CaKernelArgs {
+    CaGeom g;
+    int classic;
+    int ponding;
+    int diag_falls;           // LavaCA::diagonalFalls_ (LavaCA.hpp:108-110)
+    int dense;
+    uint64_t seed;
+    int max_steps;
+    int eruption_steps;
+    float erupt_temp, solidus, cool_ambient, cool_lateral, cool_fall;
+    FastMod var_mod;          // % variant count
+    uint8_t* type[2];
+    int32_t* flow[2];
+    float* temp[2];
+    uint16_t* solid[2];
+    uint16_t* arrival[2];
+    int8_t* desc;
+    const int32_t* spill;     // nx*ny or nullptr
+    const int4* vents;        // (x, y, z, -) per flowId
+    int vent_slots;
+    const CaTables* tables;
+    CaCtrl* ctrl;
+    uint32_t* tile_flags[2];  // bit 0: LAVA in tile after the step, bit 1: a cell changed
+    uint32_t* tile_list[2];
+    unsigned long long* hist_active;
+    unsigned long long* hist_changed;
+    uint64_t ntiles;
+};
+
+}  // namespace vca
+
+struct vca_ca {
+    vca_ca_desc desc;
+    vca::CaGeom geom;
+    vca::CaTables tables_host;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int grid_blocks = 0;      // persistent grid of the tile kernels
+    uint64_t ntiles = 0;
+    size_t plane_cells = 0;   // P * ny * nz
+    // device memory
+    uint8_t* type[2] = {nullptr, nullptr};
+    int32_t* flow[2] = {nullptr, nullptr};
+    float* temp[2] = {nullptr, nullptr};
+    uint16_t* solid[2] = {nullptr, nullptr};
+    uint16_t* arrival[2] = {nullptr, nullptr};
+    int8_t* desc_plane = nullptr;
+    int32_t* spill = nullptr;
+    int4* vents = nullptr;
+    int vent_slots = 0;
+    vca::CaTables* tables = nullptr;
+    vca::CaCtrl* ctrl = nullptr;
+    vca::CaCtrl* ctrl_host = nullptr;   // pinned mirror
+    uint32_t* tile_flags[2] = {nullptr, nullptr};
+    uint32_t* tile_list[2] = {nullptr, nullptr};
+    unsigned long long* hist_active = nullptr;
+    unsigned long long* hist_changed = nullptr;
+    bool has_terrain = false;
+    bool seeded = false;
+    // host mirror of the control state after the last sync
+    int steps = 0;
+    int stop = VCA_STOP_RUNNING;
+    // timing
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    double total_ms = 0.0;
+    double rules_ms = 0.0;
+    uint64_t rules_launches = 0;
+    int profile_kernels = 0;  // bracket each rules launch with events (set by VCA_PROFILE_KERNELS=1)
+    std::vector<cudaEvent_t> prof_events;
+};
