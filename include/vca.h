@@ -95,6 +95,7 @@ typedef struct {
     uint64_t tiles_total;      /* tiles of the grid */
     uint64_t tiles_processed;  /* tile visits summed over all steps (DENSE: steps x tiles) */
     uint64_t cells_per_tile;   /* cells one tile covers */
+    uint64_t kernel_launches;  /* CUDA kernel launches issued by this handle so far */
 } vca_ca_info;
 
 /* LavaCA ctor (LavaCA.hpp:84-144): all cells AIR, buffers on the device. */
@@ -161,6 +162,7 @@ typedef struct {
     uint64_t attempts;         /* attempts() -- trials not skipped by mobility */
     uint64_t accepted;         /* accepted() */
     uint64_t uphill;           /* acceptedUphill() */
+    uint64_t kernel_launches;  /* CUDA kernel launches issued by this handle so far */
 } vca_mc_info;
 
 vca_status vca_mc_create(const vca_mc_desc* desc, vca_mc** out);

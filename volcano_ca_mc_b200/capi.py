@@ -55,7 +55,8 @@ class Vent(ctypes.Structure):
 class CaInfo(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int), ("stop_reason", ctypes.c_int), ("lava_cells", ctypes.c_uint64),
                 ("air_cells", ctypes.c_uint64), ("tiles_total", ctypes.c_uint64),
-                ("tiles_processed", ctypes.c_uint64), ("cells_per_tile", ctypes.c_uint64)]
+                ("tiles_processed", ctypes.c_uint64), ("cells_per_tile", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64)]
 
 
 class McDesc(ctypes.Structure):
@@ -67,7 +68,8 @@ class McDesc(ctypes.Structure):
 
 class McInfo(ctypes.Structure):
     _fields_ = [("sweeps", ctypes.c_int), ("colors", ctypes.c_int), ("domain_cells", ctypes.c_uint64),
-                ("attempts", ctypes.c_uint64), ("accepted", ctypes.c_uint64), ("uphill", ctypes.c_uint64)]
+                ("attempts", ctypes.c_uint64), ("accepted", ctypes.c_uint64), ("uphill", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64)]
 
 
 _lib = None

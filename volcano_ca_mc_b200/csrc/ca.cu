@@ -2,22 +2,33 @@
 //
 // One CA step (LavaCA::step, engine/src/ca/LavaCA.hpp:230-247) is three launches on the handle's
 // stream:
-//   ca_schedule_kernel  (ACTIVE sweep only) -- which 64 x TY x TZ tiles can change this step;
-//   ca_descent_kernel   -- D(n) of every supported LAVA cell (computeDescent, LavaCA.hpp:551-566);
-//   ca_rules_kernel     -- the rules cur -> next for every cell of the scheduled tiles
-//                          (updateLava / updateClassic, LavaCA.hpp:1109-1201), the step counters,
-//                          and, in its last block, finishStep (LavaCA.hpp:1206-1229).
-// The state is double-buffered SoA planes (type u8, flowId i32, temp f32, solidStep u16,
-// arrivalStep u16) in pitched rows; which buffer is current is the parity of the device-side
-// step counter, so a run of steps needs no host round trip until the stop test.
+//   ca_drop_kernel  -- brings the drop-depth plane (dropDepth of every AIR cell, LavaCA.hpp:404-414)
+//                      up to date by rescanning the column segments above last step's type changes;
+//   ca_rules_kernel -- a persistent streaming loop over 64 x TY x TZ tiles (TY * TZ = 16): every
+//                      cell of the tile is read and written to the next buffer, LAVA cools
+//                      (updateLava, LavaCA.hpp:1135-1151), AIR cells with LAVA within one cell are
+//                      listed as candidates, the tiles of the next step are scheduled;
+//   ca_cand_kernel  -- the candidates: gatherLavaCandidates, vote and solidus test (LavaCA.hpp:
+//                      443-519, 1121-1134) with D(n) of each lava source evaluated from the
+//                      drop-depth plane (descent / computeDescent, LavaCA.hpp:421-429, 551-566);
+//                      in its last block, finishStep (LavaCA.hpp:1206-1229).
+// State: double-buffered SoA planes (type u8, flowId i32, temp f32, solidStep u16, arrivalStep u16)
+// in pitched rows; the current buffer is the parity of the device-side step counter, so a run of
+// steps needs no host round trip until the stop test.
+//
+// ACTIVE schedule: only LAVA cells and AIR cells with LAVA within one cell can change in a step
+// (the front set of LavaCA::frontCandidatesLayer, LavaCA.hpp:907-940).  A tile is processed in step
+// t+1 when a tile within one tile of it holds LAVA after step t, or when it changed in step t (its
+// two buffers then differ).  Every other tile keeps both buffers equal and is skipped; the result is
+// bit-identical to the DENSE schedule, which processes every tile every step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <queue>
 #include <string>
 #include <utility>
 #include <vector>
@@ -28,15 +39,15 @@
 
 namespace vca {
 
-constexpr int kThreads = 256;   // threads of a tile block: 16 per 64-cell row, 16 rows
+constexpr int kThreads = 256;       // threads of a tile block: 16 per 64-cell row, 16 rows
 constexpr int kTileX = 64;
-constexpr int kMaxDrop = 16;    // LavaCA::kMaxDrop (LavaCA.hpp:1293)
-constexpr int kSmemRowBytes = 72;  // 4 pad + 64 cells + 4 pad
-constexpr int kMaxHaloRows = 36;   // (TY + 2) * (TZ + 2) for TY = TZ = 4
+constexpr int kMaxDrop = 16;        // LavaCA::kMaxDrop (LavaCA.hpp:1293)
+constexpr int kSmemRowBytes = 72;   // 4 pad + 64 cells + 4 pad
+constexpr int kMaxHaloRows = 36;    // (TY + 2) * (TZ + 2) for TY = TZ = 4; 18 for the 2D tiles
 
 // ------------------------------------------------------------------------------------------
-// Addressing with the reference's frame semantics: a coordinate one step outside the interior
-// is the opposite layer on a periodic axis, else the VOID frame (Boundary::applyWith,
+// Addressing with the reference's frame semantics: a coordinate one step outside the interior is
+// the opposite layer on a periodic axis, else the VOID frame (Boundary::applyWith,
 // engine/src/core/Boundary.hpp:75-131).
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ int64_t pidx(const CaGeom& g, int x, int y, int z) {
@@ -51,45 +62,13 @@ __device__ __forceinline__ bool wrap_axis(int& v, int n, int periodic) {
 __device__ __forceinline__ bool resolve(const CaGeom& g, int& x, int& y, int& z) {
     return wrap_axis(x, g.nx, g.per[0]) && wrap_axis(y, g.ny, g.per[1]) && wrap_axis(z, g.nz, g.per[2]);
 }
-__device__ __forceinline__ int type_at(const CaGeom& g, const uint8_t* T, int x, int y, int z) {
-    if (!resolve(g, x, y, z)) return kVoid;
-    return __ldg(T + pidx(g, x, y, z));
-}
-// LavaCA::spillAt (LavaCA.hpp:383): the column wraps.
-__device__ __forceinline__ int spill_at(const CaKernelArgs& k, int x, int y) {
-    const int nx = k.g.nx, ny = k.g.ny;
-    x = x < 0 ? x + nx : (x >= nx ? x - nx : x);
-    y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-    return __ldg(k.spill + x + (int64_t)nx * y);
+// A halo coordinate of a tile: up to one cell outside [0, n) maps through the frame; further out
+// (past a partial last tile) is outside the grid.
+__device__ __forceinline__ bool halo_axis(int& v, int n, int periodic) {
+    if (v > n) return false;
+    return wrap_axis(v, n, periodic);
 }
 __device__ __forceinline__ bool solid_ground(int t) { return t == kRock || t == kBasalt; }
-
-// LavaCA::hasSupport (LavaCA.hpp:390-399).
-__device__ bool has_support(const CaKernelArgs& k, const uint8_t* T, int x, int y, int z) {
-    if (z == 0) return true;
-    const int below = type_at(k.g, T, x, y, z - 1);
-    if (solid_ground(below)) return true;
-    return below == kLava && k.spill != nullptr && z - 1 < spill_at(k, x, y);
-}
-// LavaCA::dropDepth (LavaCA.hpp:404-414).
-__device__ int drop_depth(const CaKernelArgs& k, const uint8_t* T, int x, int y, int z) {
-    for (int d = 0; d <= kMaxDrop && z - d >= 0; ++d) {
-        if (d > 0 && type_at(k.g, T, x, y, z - d) != kAir) return -1;
-        if (has_support(k, T, x, y, z - d)) return d;
-    }
-    return kMaxDrop;
-}
-// LavaCA::descent (LavaCA.hpp:421-429).
-__device__ int descent(const CaKernelArgs& k, const uint8_t* T, int x, int y, int z) {
-    int best = 0;
-    const CaTables* tb = k.tables;
-    const int nside = tb->nside;
-    for (int s = 0; s < nside; ++s) {
-        const int ax = x + tb->side[s][0], ay = y + tb->side[s][1];
-        if (type_at(k.g, T, ax, ay, z) == kAir) best = max(best, drop_depth(k, T, ax, ay, z));
-    }
-    return best;
-}
 
 // CandidateVote (engine/src/ca/CaRules.hpp:127-183).
 struct Vote {
@@ -133,53 +112,188 @@ struct Vote {
     }
 };
 
-__device__ __forceinline__ int variant_of(const CaKernelArgs& k, uint64_t prefix, uint64_t gidx) {
-    if (k.tables->nb.variants == 1) return 0;
-    return (int)fast_mod(hash_salt(hash_index(prefix, gidx), kSaltNeighborhood), k.var_mod);
+__device__ __forceinline__ void tile_origin(const CaGeom& g, uint32_t tile, int& x0, int& y0, int& z0) {
+    const int tx = (int)(tile % (uint32_t)g.tiles_x);
+    const uint32_t r = tile / (uint32_t)g.tiles_x;
+    x0 = tx * kTileX;
+    y0 = (int)(r % (uint32_t)g.tiles_y) * g.TY;
+    z0 = (int)(r / (uint32_t)g.tiles_y) * g.TZ;
 }
 
-// LavaCA::tryPonding (LavaCA.hpp:443-461).
-__device__ void try_ponding(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, const float* Te, int x, int y,
-                            int z, Vote& v) {
-    if (k.spill == nullptr || z > __ldg(k.spill + x + (int64_t)k.g.nx * y)) return;
-    const int bz = z - 1;
-    if (type_at(k.g, T, x, y, bz) != kLava) return;
-    if (!has_support(k, T, x, y, bz)) return;
-    const int nh = k.g.ny > 1 ? 4 : 2;
-    const int hx[4] = {-1, 1, 0, 0}, hy[4] = {0, 0, -1, 1};
-    for (int h = 0; h < nh; ++h) {
-        const int n = type_at(k.g, T, x + hx[h], y + hy[h], bz);
-        if (n == kAir || n == kVoid) return;
+// ------------------------------------------------------------------------------------------
+// Drop depth (LavaCA::dropDepth, LavaCA.hpp:404-414), kept current for every AIR cell.
+//
+// dropDepth of an AIR cell z only looks down its own column.  With k the number of AIR cells
+// directly below z (the run of AIR from its bottom cell w = z - k up to z), the loop can only find
+// support at w, so
+//     dropDepth(z) = 16 if k > 16;  k if hasSupport(w);  16 if k == 16;  -1 otherwise
+// (when w has no support the cell under w exists and is not AIR).  An upward scan of a column
+// segment [lo, hi) from lo - 17 yields it for every cell of the segment: a run that reaches below
+// the scan start is longer than 16 either way.  dropDepth(z) depends only on the types in
+// [z - 17, z], so after a step only the 18 cells above each cell whose type changed need a
+// rescan; the rules kernel lists those cells.  Non-AIR cells hold -1.
+// ------------------------------------------------------------------------------------------
+__device__ void drop_scan(const CaKernelArgs& k, const uint8_t* T, int x, int y, int lo, int hi) {
+    const CaGeom& g = k.g;
+    const bool has_spill = k.spill != nullptr;
+    const int sp = has_spill ? __ldg(k.spill + x + (int64_t)g.nx * y) : 0;
+    const int zb = max(0, lo - (kMaxDrop + 1));
+    int prev = zb > 0 ? T[pidx(g, x, y, zb - 1)] : kVoid;
+    int run_start = 0;
+    bool in_run = false, run_sup = false;
+#pragma unroll 4
+    for (int z = zb; z < hi; ++z) {
+        const int tz = T[pidx(g, x, y, z)];
+        // hasSupport(z) (LavaCA.hpp:390-399)
+        const bool hs = z == 0 || solid_ground(prev) || (prev == kLava && has_spill && z - 1 < sp);
+        int dd = -1;
+        if (tz == kAir) {
+            if (!in_run) {
+                in_run = true;
+                if (z == zb && prev == kAir) {
+                    run_start = z - 4 * kMaxDrop;  // the run goes on below the scan: longer than 16
+                    run_sup = false;
+                } else {
+                    run_start = z;
+                    run_sup = hs;
+                }
+            }
+            const int kk = z - run_start;
+            dd = kk > kMaxDrop ? kMaxDrop : (run_sup ? kk : (kk == kMaxDrop ? kMaxDrop : -1));
+        } else {
+            in_run = false;
+        }
+        if (z >= lo) k.drop[pidx(g, x, y, z)] = (int8_t)dd;
+        prev = tz;
     }
-    const int64_t b = pidx(k.g, x, y, bz);
-    v.add(__ldg(F + b), __fsub_rn(__ldg(Te + b), k.cool_lateral));
 }
 
-// LavaCA::gatherLavaCandidates (LavaCA.hpp:465-519).
-__device__ void gather_lava(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, const float* Te, int x, int y,
-                            int z, uint64_t prefix, uint64_t gidx, Vote& v) {
-    v.n = 0;
+// Rescans the columns above last step's type changes (or every column when forced or when the
+// change list overflowed), and clears the change list this step's rules will fill.
+__global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force_full) {
+    CaCtrl* ctrl = k.ctrl;
+    if (!force_full && ctrl->stop) return;
+    const uint32_t t = ctrl->steps;
+    const int cur = t & 1, nxt = cur ^ 1;
+    if (!force_full && blockIdx.x == 0 && threadIdx.x == 0) {
+        ctrl->chg_count[nxt] = 0;   // filled by this step's rules
+        ctrl->list_count[nxt] = 0;  // tiles of the next step, scheduled by this step's rules
+    }
+    if (k.classic) return;
+    const CaGeom& g = k.g;
+    const uint8_t* T = k.type[cur];
+    const unsigned n = force_full ? 0u : ctrl->chg_count[cur];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (force_full || n > k.chg_cap) {
+        const uint64_t cols = (uint64_t)g.nx * g.ny;
+        for (uint64_t c = gtid; c < cols; c += stride) drop_scan(k, T, (int)(c % g.nx), (int)(c / g.nx), 0, g.nz);
+        return;
+    }
+    for (uint64_t j = gtid; j < n; j += stride) {
+        const uint32_t gi = k.chg_list[cur][j];
+        const uint32_t r = gi / (uint32_t)g.nx;
+        const int x = (int)(gi - r * (uint32_t)g.nx);
+        const int y = (int)(r % (uint32_t)g.ny);
+        const int z = (int)(r / (uint32_t)g.ny);
+        drop_scan(k, T, x, y, z, min(g.nz, z + kMaxDrop + 2));
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Rules, candidate pass: an AIR cell with LAVA within one cell (listed by the streaming pass).
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int type_at(const CaGeom& g, const uint8_t* T, int x, int y, int z) {
+    if (!resolve(g, x, y, z)) return kVoid;
+    return __ldg(T + pidx(g, x, y, z));
+}
+
+// D(n) of a LAVA cell n (descent + computeDescent, LavaCA.hpp:421-429, 551-566): -1 without support,
+// else the largest drop depth among its AIR side neighbours (at least 0).
+__device__ __forceinline__ int descent_of(const CaKernelArgs& k, const uint8_t* T, int sx, int sy, int sz) {
+    const CaGeom& g = k.g;
+    if (sz > 0) {
+        const int below = __ldg(T + pidx(g, sx, sy, sz - 1));
+        const bool sup = solid_ground(below) ||
+                         (below == kLava && k.spill != nullptr && sz - 1 < __ldg(k.spill + sx + (int64_t)g.nx * sy));
+        if (!sup) return -1;
+    }
+    const CaTables* tb = k.tables;
+    const int nside = tb->nside;
+    int best = 0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        if (s >= nside) break;
+        int ax = sx + tb->side[s][0], ay = sy + tb->side[s][1];
+        if (!wrap_axis(ax, g.nx, g.per[0]) || !wrap_axis(ay, g.ny, g.per[1])) continue;
+        const int64_t q = pidx(g, ax, ay, sz);
+        const int tq = __ldg(T + q);
+        const int dq = k.drop[q];
+        if (tq == kAir) best = max(best, dq);
+    }
+    return best;
+}
+
+// gatherLavaCandidates + tryPonding (LavaCA.hpp:443-519) or updateClassic's vote (1176-1182), the
+// winner (CaRules.hpp:152-173) and the solidus test.  Returns true when the cell becomes LAVA.
+__device__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, const float* Te, int x, int y,
+                               int z, uint64_t prefix, uint64_t gidx, int32_t* out_flow, float* out_temp) {
+    const CaGeom& g = k.g;
     const NbTable& nb = k.tables->nb;
-    const int var = variant_of(k, prefix, gidx);
+    const int var = nb.variants == 1 ? 0 : (int)fast_mod(hash_salt(hash_index(prefix, gidx), kSaltNeighborhood), k.var_mod);
     const int cnt = nb.count[var];
+    Vote v;
+    v.n = 0;
+    if (k.classic) {
+        for (int i = 0; i < cnt; ++i) {
+            int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
+            if (!resolve(g, sx, sy, sz)) continue;
+            const int64_t s = pidx(g, sx, sy, sz);
+            if (__ldg(T + s) == kLava) v.add(__ldg(F + s), 0.0f);
+        }
+        if (v.n == 0) return false;
+        const int w = v.winner(prefix, gidx);
+        *out_flow = v.ids[w];
+        *out_temp = 0.0f;
+        return true;
+    }
     int c_drop = -100;
     for (int i = 0; i < cnt; ++i) {
         const int dx = nb.off[var][i][0], dy = nb.off[var][i][1], dz = nb.off[var][i][2];
         if (dz < 0) {
-            if (k.ponding && dx == 0 && dy == 0) try_ponding(k, T, F, Te, x, y, z, v);
+            if (!(k.ponding && dx == 0 && dy == 0)) continue;
+            // tryPonding (LavaCA.hpp:443-461)
+            if (k.spill == nullptr || z > __ldg(k.spill + x + (int64_t)g.nx * y)) continue;
+            const int bz = z - 1;
+            if (type_at(g, T, x, y, bz) != kLava) continue;
+            if (bz > 0) {  // hasSupport(x, y, bz)
+                const int below = __ldg(T + pidx(g, x, y, bz - 1));
+                const bool sup = solid_ground(below) || (below == kLava && bz - 1 < __ldg(k.spill + x + (int64_t)g.nx * y));
+                if (!sup) continue;
+            }
+            const int nh = g.ny > 1 ? 4 : 2;
+            const int hx[4] = {-1, 1, 0, 0}, hy[4] = {0, 0, -1, 1};
+            bool open_side = false;
+            for (int h = 0; h < nh; ++h) {
+                const int n = type_at(g, T, x + hx[h], y + hy[h], bz);
+                open_side = open_side || n == kAir || n == kVoid;
+            }
+            if (open_side) continue;
+            const int64_t b = pidx(g, x, y, bz);
+            v.add(__ldg(F + b), __fsub_rn(__ldg(Te + b), k.cool_lateral));
             continue;
         }
         int sx = x + dx, sy = y + dy, sz = z + dz;
-        if (!resolve(k.g, sx, sy, sz)) continue;
-        const int64_t s = pidx(k.g, sx, sy, sz);
+        if (!resolve(g, sx, sy, sz)) continue;  // the VOID frame is never lava
+        const int64_t s = pidx(g, sx, sy, sz);
         if (__ldg(T + s) != kLava) continue;
         float cooling;
         if (dz > 0 && dx == 0 && dy == 0) {
             cooling = k.cool_fall;
         } else {
-            const int d = k.desc[s];
+            const int d = descent_of(k, T, sx, sy, sz);
             if (d < 0) continue;
-            if (c_drop == -100) c_drop = drop_depth(k, T, x, y, z);
+            if (c_drop == -100) c_drop = k.drop[pidx(g, x, y, z)];
             if (dz > 0) {
                 if (c_drop != 0 || d != 1) continue;
                 cooling = k.cool_fall;
@@ -190,137 +304,73 @@ __device__ void gather_lava(const CaKernelArgs& k, const uint8_t* T, const int32
         }
         v.add(__ldg(F + s), __fsub_rn(__ldg(Te + s), cooling));
     }
+    if (v.n == 0) return false;
+    const int w = v.winner(prefix, gidx);
+    const float wt = v.max_temp[w];
+    if (!(wt >= k.solidus)) return false;
+    *out_flow = v.ids[w];
+    *out_temp = wt;
+    return true;
 }
 
-// updateClassic's vote (LavaCA.hpp:1176-1182).
-__device__ void gather_classic(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, int x, int y, int z,
-                               uint64_t prefix, uint64_t gidx, Vote& v) {
-    v.n = 0;
-    const NbTable& nb = k.tables->nb;
-    const int var = variant_of(k, prefix, gidx);
-    for (int i = 0; i < nb.count[var]; ++i) {
-        int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
-        if (!resolve(k.g, sx, sy, sz)) continue;
-        const int64_t s = pidx(k.g, sx, sy, sz);
-        if (__ldg(T + s) == kLava) v.add(__ldg(F + s), 0.0f);
-    }
-}
-
-// ------------------------------------------------------------------------------------------
-// Tile decoding.  Tile id = tx + tiles_x * (ty + tiles_y * tz).
-// ------------------------------------------------------------------------------------------
-__device__ __forceinline__ void tile_origin(const CaGeom& g, uint32_t tile, int& x0, int& y0, int& z0) {
-    const int tx = (int)(tile % (uint32_t)g.tiles_x);
-    const uint32_t r = tile / (uint32_t)g.tiles_x;
-    const int ty = (int)(r % (uint32_t)g.tiles_y);
-    const int tz = (int)(r / (uint32_t)g.tiles_y);
-    x0 = tx * kTileX;
-    y0 = ty * g.TY;
-    z0 = tz * g.TZ;
-}
-
-// ------------------------------------------------------------------------------------------
-// Schedule (ACTIVE sweep): tile t is processed in step s when a tile within one tile of it held
-// LAVA after step s-1 (only cells within one cell of LAVA, and LAVA itself, can change: the
-// front set of LavaCA::frontCandidates, LavaCA.hpp:907-940), or when t changed in step s-1
-// (its two buffers differ and next must be refreshed).  Other tiles keep both buffers equal.
-// ------------------------------------------------------------------------------------------
-__global__ void ca_schedule_kernel(CaKernelArgs k) {
-    const CaCtrl* ctrl = k.ctrl;
-    if (ctrl->stop) return;
-    const uint32_t t = ctrl->steps;
-    const int cur = t & 1, nxt = cur ^ 1;
+// Schedule the tiles within one tile of `tile` for step t + 1 (ACTIVE); lanes 0..26 of a warp
+// each try one target, `want` says which lanes take part.
+__device__ __forceinline__ void schedule_around(const CaKernelArgs& k, uint32_t tile, uint32_t t, int nxt, int lane,
+                                                bool want) {
     const CaGeom& g = k.g;
-    if (blockIdx.x == 0 && threadIdx.x == 0) k.ctrl->list_count[nxt] = 0;
-    const uint32_t* fin = k.tile_flags[cur];
-    uint32_t* fout = k.tile_flags[nxt];
-    // Warp-uniform loop: every lane of a warp runs the same iterations, so the ballot below sees all 32.
-    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < k.ntiles; base += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t tile = base + threadIdx.x;
-        bool process = false;
-        if (tile < k.ntiles) {
-            const int tx = (int)(tile % g.tiles_x);
-            const uint64_t r = tile / g.tiles_x;
-            const int ty = (int)(r % g.tiles_y);
-            const int tz = (int)(r / g.tiles_y);
-            process = (fin[tile] & 2u) != 0;
-            for (int dz = -1; dz <= 1 && !process; ++dz) {
-                int zz = tz + dz;
-                if (!wrap_axis(zz, g.tiles_z, g.per[2])) continue;
-                for (int dy = -1; dy <= 1 && !process; ++dy) {
-                    int yy = ty + dy;
-                    if (!wrap_axis(yy, g.tiles_y, g.per[1])) continue;
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        int xx = tx + dx;
-                        if (!wrap_axis(xx, g.tiles_x, g.per[0])) continue;
-                        if (fin[xx + (uint64_t)g.tiles_x * (yy + (uint64_t)g.tiles_y * zz)] & 1u) {
-                            process = true;
-                            break;
-                        }
-                    }
-                }
-            }
-            fout[tile] = 0;
-        }
-        // Warp-aggregated append keeps neighbouring tiles next to each other in the list.
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, process);
-        const unsigned lane = threadIdx.x & 31;
-        unsigned slot = 0;
-        if (lane == 0 && ballot) slot = atomicAdd(&k.ctrl->list_count[cur], (unsigned)__popc(ballot));
-        slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-        if (process) k.tile_list[cur][slot + __popc(ballot & ((1u << lane) - 1u))] = (uint32_t)tile;
-    }
-}
-
-// ------------------------------------------------------------------------------------------
-// D(n) of the LAVA cells of the scheduled tiles (computeDescent / frontDescent,
-// LavaCA.hpp:551-566, 877-888).  Only cells that are LAVA now are read back by the rules.
-// ------------------------------------------------------------------------------------------
-__global__ __launch_bounds__(kThreads) void ca_descent_kernel(CaKernelArgs k) {
-    const CaCtrl* ctrl = k.ctrl;
-    if (ctrl->stop) return;
-    if (k.classic) return;
-    const uint32_t t = ctrl->steps;
-    const int cur = t & 1;
-    const CaGeom& g = k.g;
-    const uint8_t* T = k.type[cur];
-    const uint64_t count = k.dense ? k.ntiles : ctrl->list_count[cur];
-    const int xq = threadIdx.x & 15, row = threadIdx.x >> 4;
-    const int ly = row % g.TY, lz = row / g.TY;
-    for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const uint32_t tile = k.dense ? (uint32_t)i : k.tile_list[cur][i];
-        int x0, y0, z0;
-        tile_origin(g, tile, x0, y0, z0);
-        const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
-        if (y >= g.ny || z >= g.nz) continue;
-        const int64_t p = pidx(g, x, y, z);
-        const uint32_t w = *reinterpret_cast<const uint32_t*>(T + p);
-        uint32_t lava = __vcmpeq4(w, 0x02020202u);
-        while (lava) {
-            const int j = (__ffs(lava) - 1) >> 3;
-            lava &= ~(0xFFu << (8 * j));
-            const int xx = x + j;
-            int8_t d = -1;
-            if (has_support(k, T, xx, y, z)) d = (int8_t)descent(k, T, xx, y, z);
-            k.desc[p + j] = d;
+    bool first = false;
+    uint32_t target = 0;
+    if (want && lane < 27) {
+        const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+        int tx = (int)(tile % (uint32_t)g.tiles_x) + dx;
+        const uint32_t r = tile / (uint32_t)g.tiles_x;
+        int ty = (int)(r % (uint32_t)g.tiles_y) + dy;
+        int tz = (int)(r / (uint32_t)g.tiles_y) + dz;
+        if (wrap_axis(tx, g.tiles_x, g.per[0]) && wrap_axis(ty, g.tiles_y, g.per[1]) && wrap_axis(tz, g.tiles_z, g.per[2])) {
+            target = (uint32_t)tx + (uint32_t)g.tiles_x * ((uint32_t)ty + (uint32_t)g.tiles_y * tz);
+            first = atomicMax(&k.tile_mark[target], t + 2) < t + 2;
         }
     }
+    const unsigned ballot = __ballot_sync(0xFFFFFFFFu, first);
+    unsigned slot = 0;
+    if (lane == 0 && ballot) slot = atomicAdd(&k.ctrl->list_count[nxt], (unsigned)__popc(ballot));
+    slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+    const unsigned pos = slot + __popc(ballot & ((1u << lane) - 1u));
+    if (first && pos < k.ntiles) k.tile_list[nxt][pos] = target;  // a tile is listed once per step
+}
+
+// Warp-aggregated append of n entries (values v[0..n-1], n <= 4) per lane to list/count.
+__device__ __forceinline__ void warp_append(uint32_t* list, unsigned int* count, uint32_t cap, int lane, unsigned n,
+                                            const uint32_t* v) {
+    unsigned incl = n;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned u = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+        if (lane >= off) incl += u;
+    }
+    unsigned base = 0;
+    if (lane == 31 && incl) base = atomicAdd(count, incl);
+    base = __shfl_sync(0xFFFFFFFFu, base, 31) + incl - n;
+    for (unsigned j = 0; j < n; ++j)
+        if (base + j < cap) list[base + j] = v[j];
 }
 
 // ------------------------------------------------------------------------------------------
-// Rules.  A block handles one 64 x TY x TZ tile at a time (persistent loop over the schedule):
-//   1. stage the tile's cell types with a one-cell halo in shared memory (frame semantics at the
-//      grid edges), and mark per cell whether LAVA lies within one cell (3x3x3): only such AIR
-//      cells can gain lava (CaRules.hpp:69-79);
-//   2. each thread updates 4 consecutive cells of a row: 128-bit loads and stores of the flowId
-//      and temp planes, 64-bit of the two step planes, 32-bit of the type plane;
-//   3. AIR cells next to lava run the exact candidate gathering and vote from global memory.
+// Rules, streaming pass.  A persistent block takes one tile at a time:
+//   1. its threads load their 4 cells' state (128-bit flowId and temp, 64-bit steps, 32-bit types),
+//      then stage the tile's types with a one-cell halo in shared memory (frame semantics at the
+//      grid edges), so that the two memory latencies overlap;
+//   2. LAVA cells cool (updateLava's LAVA branch, LavaCA.hpp:1135-1151); every cell is written to
+//      the next buffer unchanged otherwise; AIR cells with LAVA within one cell (3x3x3) are listed
+//      for the candidate pass, which may overwrite them;
+//   3. cells whose type changed are listed for the drop-depth rescan;
+//   4. (ACTIVE) a tile with LAVA schedules itself and its neighbours for the next step, a tile that
+//      only changed schedules itself.
 // ------------------------------------------------------------------------------------------
-__global__ __launch_bounds__(kThreads) void ca_rules_kernel(CaKernelArgs k) {
+__global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaKernelArgs k) {
     __shared__ __align__(16) uint8_t s_type[kMaxHaloRows * kSmemRowBytes];
-    __shared__ uint32_t s_dil[kMaxHaloRows * 16];
-    __shared__ unsigned long long s_red[4][kThreads / 32];
-    __shared__ bool s_last;
+    __shared__ unsigned s_flags[2];
+    __shared__ unsigned long long s_red[2][kThreads / 32];
 
     CaCtrl* ctrl = k.ctrl;
     if (ctrl->stop) return;
@@ -328,39 +378,47 @@ __global__ __launch_bounds__(kThreads) void ca_rules_kernel(CaKernelArgs k) {
     const int cur = t & 1, nxt = cur ^ 1;
     const CaGeom& g = k.g;
     const uint8_t* T = k.type[cur];
-    const int32_t* F = k.flow[cur];
-    const float* Te = k.temp[cur];
     const uint64_t count = k.dense ? k.ntiles : ctrl->list_count[cur];
 
-    // StepCtx (LavaCA.hpp:542-546)
-    const bool erupting = (int64_t)t < (int64_t)k.eruption_steps;
-    const uint16_t stamp = (uint16_t)min(t, 65535u);
-    uint64_t prefix = 0;
-    bool have_prefix = false;
-
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int xq = tid & 15, row = tid >> 4;
     const int ly = row % g.TY, lz = row / g.TY;
     const int hy_on = g.ny > 1 ? 1 : 0, hz_on = g.nz > 1 ? 1 : 0;
     const int HY = hy_on ? g.TY + 2 : 1, HZ = hz_on ? g.TZ + 2 : 1;
     const int halo_rows = HY * HZ;
+    const bool erupting = (int64_t)t < (int64_t)k.eruption_steps;
+    const uint32_t stamp = min(t, 65535u);
+    if (tid == 0) s_flags[0] = s_flags[1] = 0;
 
-    unsigned int my_active = 0, my_changed = 0, my_born = 0;
-    unsigned int tiles_done = 0;
+    unsigned int my_active = 0, my_changed = 0, tiles_done = 0;
+    int it = 0;
 
-    for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
+    for (uint64_t i = blockIdx.x; i < count; i += gridDim.x, ++it) {
         const uint32_t tile = k.dense ? (uint32_t)i : k.tile_list[cur][i];
         int x0, y0, z0;
         tile_origin(g, tile, x0, y0, z0);
         ++tiles_done;
+        const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
+        const bool valid = y < g.ny && z < g.nz;
+        const int64_t p = pidx(g, valid ? x : 0, valid ? y : 0, valid ? z : 0);
 
-        // 1. stage types with halo
-        for (int w = tid; w < halo_rows * 16; w += kThreads) {
-            const int r = w >> 4, word = w & 15;
+        uint32_t w = 0xFFFFFFFFu;
+        int4 f4 = make_int4(0, 0, 0, 0);
+        float4 t4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint2 s2 = make_uint2(0, 0), a2 = make_uint2(0, 0);
+        if (valid) {
+            w = *reinterpret_cast<const uint32_t*>(T + p);
+            f4 = *reinterpret_cast<const int4*>(k.flow[cur] + p);
+            t4 = *reinterpret_cast<const float4*>(k.temp[cur] + p);
+            s2 = *reinterpret_cast<const uint2*>(k.solid[cur] + p);
+            a2 = *reinterpret_cast<const uint2*>(k.arrival[cur] + p);
+        }
+        for (int wi = tid; wi < halo_rows * 16; wi += kThreads) {
+            const int r = wi >> 4, word = wi & 15;
             int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
             uint32_t v = 0xFFFFFFFFu;
-            int xw = x0 + 4 * word;
-            if (wrap_axis(yy, g.ny, g.per[1]) && wrap_axis(zz, g.nz, g.per[2])) {
+            const int xw = x0 + 4 * word;
+            if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2])) {
                 v = *reinterpret_cast<const uint32_t*>(T + pidx(g, xw, yy, zz));
                 // Periodic x with padded rows: the frame cell x = nx inside this word is the copy of x = 0.
                 if (g.per[0] && g.nx < g.P && xw <= g.nx && g.nx < xw + 4) {
@@ -376,164 +434,199 @@ __global__ __launch_bounds__(kThreads) void ca_rules_kernel(CaKernelArgs k) {
             int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
             int xx = right ? x0 + kTileX : x0 - 1;
             uint8_t v = kVoid;
-            if (right && xx > g.nx) {
-                v = kVoid;  // beyond the frame: only padding cells see it
-            } else if (wrap_axis(xx, g.nx, g.per[0]) && wrap_axis(yy, g.ny, g.per[1]) && wrap_axis(zz, g.nz, g.per[2])) {
+            if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
                 v = T[pidx(g, xx, yy, zz)];
-            }
             s_type[r * kSmemRowBytes + (right ? 4 + kTileX : 3)] = v;
         }
         __syncthreads();
-        for (int w = tid; w < halo_rows * 16; w += kThreads) {
-            const int r = w >> 4, word = w & 15;
-            const uint8_t* rowp = s_type + r * kSmemRowBytes + 4 + 4 * word;
-            const uint32_t m = __vcmpeq4(*reinterpret_cast<const uint32_t*>(rowp), 0x02020202u);
-            const uint32_t left = rowp[-1] == kLava ? 0xFFu : 0u;
-            const uint32_t rightb = rowp[4] == kLava ? 0xFF000000u : 0u;
-            s_dil[w] = m | (m << 8) | (m >> 8) | left | rightb;
-        }
-        __syncthreads();
 
-        const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
         bool any_lava = false, any_changed = false;
-        if (y < g.ny && z < g.nz) {
+        unsigned nbas = 0, ncand = 0;
+        uint32_t bas[4], cand[4];
+        const uint32_t g0 = (uint32_t)(x + g.nx * (y + g.ny * z));
+        const uint32_t lava_m = __vcmpeq4(w, 0x02020202u);
+        uint32_t cand_m = __vcmpeq4(w, 0u);
+        if (cand_m) {
             const int hr = (ly + hy_on) + HY * (lz + hz_on);
-            uint32_t w = *reinterpret_cast<const uint32_t*>(s_type + hr * kSmemRowBytes + 4 + 4 * xq);
-            // Padding cells (x >= nx) are VOID: the staged copy may hold the periodic image of x = 0 there.
-            if (x + 4 > g.nx) {
-                const int keep = max(0, g.nx - x);
-                w |= 0xFFFFFFFFu << (8 * keep);
-            }
             uint32_t near = 0;
             for (int dz = -hz_on; dz <= hz_on; ++dz)
-                for (int dy = -hy_on; dy <= hy_on; ++dy) near |= s_dil[(hr + dy + HY * dz) * 16 + xq];
-
-            const int64_t p = pidx(g, x, y, z);
-            int4 f4 = *reinterpret_cast<const int4*>(F + p);
-            float4 t4 = *reinterpret_cast<const float4*>(Te + p);
-            uint2 s2 = *reinterpret_cast<const uint2*>(k.solid[cur] + p);
-            uint2 a2 = *reinterpret_cast<const uint2*>(k.arrival[cur] + p);
-            int32_t fl[4] = {f4.x, f4.y, f4.z, f4.w};
-            float te[4] = {t4.x, t4.y, t4.z, t4.w};
-            uint16_t so[4] = {(uint16_t)(s2.x & 0xFFFF), (uint16_t)(s2.x >> 16), (uint16_t)(s2.y & 0xFFFF),
-                              (uint16_t)(s2.y >> 16)};
-            uint16_t ar[4] = {(uint16_t)(a2.x & 0xFFFF), (uint16_t)(a2.x >> 16), (uint16_t)(a2.y & 0xFFFF),
-                              (uint16_t)(a2.y >> 16)};
-            uint32_t wout = w;
+                for (int dy = -hy_on; dy <= hy_on; ++dy) {
+                    const uint8_t* rp = s_type + (hr + dy + HY * dz) * kSmemRowBytes + 4 + 4 * xq;
+                    const uint32_t m = __vcmpeq4(*reinterpret_cast<const uint32_t*>(rp), 0x02020202u);
+                    near |= m | (m << 8) | (m >> 8) | (rp[-1] == kLava ? 0xFFu : 0u) | (rp[4] == kLava ? 0xFF000000u : 0u);
+                }
+            cand_m &= near;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint8_t ty = (w >> (8 * j)) & 0xFF;
-                if (ty == kAir) {
-                    if ((near >> (8 * j)) & 0xFF) {
-                        const int xx = x + j;
-                        const uint64_t gi = (uint64_t)xx + (uint64_t)g.nx * ((uint64_t)y + (uint64_t)g.ny * z);
-                        if (!have_prefix) {
-                            prefix = hash_prefix(k.seed, t);
-                            have_prefix = true;
-                        }
-                        Vote v;
-                        if (!k.classic) {
-                            gather_lava(k, T, F, Te, xx, y, z, prefix, gi, v);
-                        } else {
-                            gather_classic(k, T, F, xx, y, z, prefix, gi, v);
-                        }
-                        if (v.n > 0) {
-                            const int wi = v.winner(prefix, gi);
-                            const float wt = k.classic ? 0.0f : v.max_temp[wi];
-                            if (k.classic || wt >= k.solidus) {
-                                wout = (wout & ~(0xFFu << (8 * j))) | ((uint32_t)kLava << (8 * j));
-                                fl[j] = v.ids[wi];
-                                te[j] = wt;
-                                so[j] = 0;
-                                ar[j] = stamp;
-                                ++my_active;
-                                ++my_changed;
-                                ++my_born;
-                                any_changed = true;
-                                any_lava = true;
-                            }
-                        }
+            for (int j = 0; j < 4; ++j)
+                if ((cand_m >> (8 * j)) & 0xFF) cand[ncand++] = g0 + j;
+        }
+        uint32_t wout = w;
+        if (lava_m) {
+            if (k.classic) {
+                const unsigned nl = __popc(lava_m) >> 3;
+                my_active += nl;
+                any_lava = true;
+            } else {
+                float te[4] = {t4.x, t4.y, t4.z, t4.w};
+                const int32_t fl[4] = {f4.x, f4.y, f4.z, f4.w};
+                uint32_t so[2] = {s2.x, s2.y};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (!((lava_m >> (8 * j)) & 0xFF)) continue;
+                    const float before = te[j];
+                    bool vent = false;
+                    if (erupting && fl[j] > 0 && fl[j] < k.vent_slots) {
+                        const int4 vc = __ldg(k.vents + fl[j]);
+                        vent = vc.x == x + j && vc.y == y && vc.z == z;
                     }
-                } else if (ty == kLava) {
-                    if (!k.classic) {
-                        const float before = te[j];
-                        float nt;
-                        bool vent = false;
-                        const int32_t f = fl[j];
-                        if (erupting && f > 0 && f < k.vent_slots) {
-                            const int4 vc = __ldg(k.vents + f);
-                            vent = vc.x == x + j && vc.y == y && vc.z == z;
-                        }
-                        nt = vent ? k.erupt_temp : __fsub_rn(before, k.cool_ambient);
-                        if (nt < k.solidus) {
-                            wout = (wout & ~(0xFFu << (8 * j))) | ((uint32_t)kBasalt << (8 * j));
-                            so[j] = stamp;
-                            te[j] = nt;
-                            ++my_changed;
-                            any_changed = true;
-                        } else {
-                            te[j] = nt;
-                            ++my_active;
-                            any_lava = true;
-                            if (nt != before) {
-                                ++my_changed;
-                                any_changed = true;
-                            }
-                        }
+                    const float nt = vent ? k.erupt_temp : __fsub_rn(before, k.cool_ambient);
+                    te[j] = nt;
+                    if (nt < k.solidus) {
+                        const uint32_t half = (j & 1) * 16;
+                        wout = (wout & ~(0xFFu << (8 * j))) | ((uint32_t)kBasalt << (8 * j));
+                        so[j >> 1] = (so[j >> 1] & ~(0xFFFFu << half)) | (stamp << half);
+                        ++my_changed;
+                        bas[nbas++] = g0 + j;
+                        any_changed = true;
                     } else {
                         ++my_active;
                         any_lava = true;
+                        if (nt != before) {
+                            ++my_changed;
+                            any_changed = true;
+                        }
                     }
                 }
+                t4 = make_float4(te[0], te[1], te[2], te[3]);
+                s2 = make_uint2(so[0], so[1]);
             }
-            *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = wout;
-            *reinterpret_cast<int4*>(k.flow[nxt] + p) = make_int4(fl[0], fl[1], fl[2], fl[3]);
-            *reinterpret_cast<float4*>(k.temp[nxt] + p) = make_float4(te[0], te[1], te[2], te[3]);
-            *reinterpret_cast<uint2*>(k.solid[nxt] + p) =
-                make_uint2((uint32_t)so[0] | ((uint32_t)so[1] << 16), (uint32_t)so[2] | ((uint32_t)so[3] << 16));
-            *reinterpret_cast<uint2*>(k.arrival[nxt] + p) =
-                make_uint2((uint32_t)ar[0] | ((uint32_t)ar[1] << 16), (uint32_t)ar[2] | ((uint32_t)ar[3] << 16));
         }
-        const int tl = __syncthreads_or(any_lava);
-        const int tc = __syncthreads_or(any_changed);
-        if (tid == 0 && !k.dense) k.tile_flags[nxt][tile] = (tl ? 1u : 0u) | (tc ? 2u : 0u);
-    }
+        if (valid) {
+            *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = wout;
+            *reinterpret_cast<int4*>(k.flow[nxt] + p) = f4;
+            *reinterpret_cast<float4*>(k.temp[nxt] + p) = t4;
+            *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
+            *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
+        }
+        if (__any_sync(0xFFFFFFFFu, ncand != 0))
+            warp_append(k.cand_list, &ctrl->cand_count, k.cand_cap, lane, ncand, cand);
+        if (__any_sync(0xFFFFFFFFu, nbas != 0))
+            warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, nbas, bas);
 
-    // Block sums of the step counters, then finishStep in the last block (LavaCA.hpp:1206-1229).
-    const unsigned lane = tid & 31, warp = tid >> 5;
-    unsigned a = __reduce_add_sync(0xFFFFFFFFu, my_active);
-    unsigned c = __reduce_add_sync(0xFFFFFFFFu, my_changed);
-    unsigned b = __reduce_add_sync(0xFFFFFFFFu, my_born);
+        unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
+        bits = __reduce_or_sync(0xFFFFFFFFu, bits);
+        if (lane == 0 && bits) atomicOr(&s_flags[it & 1], bits);
+        __syncthreads();
+        const unsigned tf = s_flags[it & 1];
+        if (tid == 32) s_flags[(it + 1) & 1] = 0;
+        if (!k.dense && tid < 32) schedule_around(k, tile, t, nxt, lane, (tf & 1u) || ((tf & 2u) && lane == 13));
+    }
+    const unsigned warp = tid >> 5;
+    const unsigned a = __reduce_add_sync(0xFFFFFFFFu, my_active);
+    const unsigned c = __reduce_add_sync(0xFFFFFFFFu, my_changed);
     if (lane == 0) {
         s_red[0][warp] = a;
         s_red[1][warp] = c;
-        s_red[2][warp] = b;
     }
     __syncthreads();
     if (tid == 0) {
-        unsigned long long sa = 0, sc = 0, sb = 0;
-        for (int w = 0; w < kThreads / 32; ++w) {
-            sa += s_red[0][w];
-            sc += s_red[1][w];
-            sb += s_red[2][w];
+        unsigned long long sa = 0, sc = 0;
+        for (int wv = 0; wv < kThreads / 32; ++wv) {
+            sa += s_red[0][wv];
+            sc += s_red[1][wv];
         }
         if (sa) atomicAdd(&ctrl->acc_active, sa);
         if (sc) atomicAdd(&ctrl->acc_changed, sc);
-        if (sb) atomicAdd(&ctrl->acc_born, sb);
         if (tiles_done) atomicAdd(&ctrl->acc_tiles, (unsigned long long)tiles_done);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Rules, candidate pass: resolves the listed AIR cells (gatherLavaCandidates / vote / solidus,
+// updateLava's AIR branch, LavaCA.hpp:1121-1134), writes the ones that gain LAVA into the next
+// buffer, lists their type change, schedules their tiles' neighbourhoods, and finishes the step in
+// its last block (finishStep, LavaCA.hpp:1206-1229).
+// ------------------------------------------------------------------------------------------
+__global__ __launch_bounds__(kThreads) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
+    __shared__ unsigned long long s_red[kThreads / 32];
+    __shared__ bool s_last;
+    CaCtrl* ctrl = k.ctrl;
+    if (ctrl->stop) return;
+    const uint32_t t = ctrl->steps;
+    const int cur = t & 1, nxt = cur ^ 1;
+    const CaGeom& g = k.g;
+    const uint8_t* T = k.type[cur];
+    const int32_t* F = k.flow[cur];
+    const float* Te = k.temp[cur];
+    const uint32_t stamp = min(t, 65535u);
+    const uint64_t prefix = hash_prefix(k.seed, t);
+    const unsigned n = ctrl->cand_count;
+    const int lane = threadIdx.x & 31;
+    unsigned born = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    // warp-uniform loop (the appends below use full-warp collectives)
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += stride) {
+        const uint64_t j = base + threadIdx.x;
+        bool gained = false;
+        uint32_t gi = 0, tile = 0;
+        if (j < n) {
+            gi = k.cand_list[j];
+            const uint32_t r = gi / (uint32_t)g.nx;
+            const int x = (int)(gi - r * (uint32_t)g.nx);
+            const int y = (int)(r % (uint32_t)g.ny);
+            const int z = (int)(r / (uint32_t)g.ny);
+            int32_t nf;
+            float nt;
+            if (air_gains_lava(k, T, F, Te, x, y, z, prefix, gi, &nf, &nt)) {
+                const int64_t p = pidx(g, x, y, z);
+                k.type[nxt][p] = kLava;
+                k.flow[nxt][p] = nf;
+                k.temp[nxt][p] = nt;
+                k.solid[nxt][p] = 0;
+                k.arrival[nxt][p] = (uint16_t)stamp;
+                gained = true;
+                ++born;
+                tile = (uint32_t)(x / kTileX) +
+                       (uint32_t)g.tiles_x * ((uint32_t)(y / g.TY) + (uint32_t)g.tiles_y * (uint32_t)(z / g.TZ));
+            }
+        }
+        if (!k.classic && __any_sync(0xFFFFFFFFu, gained))
+            warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, gained ? 1u : 0u, &gi);
+        if (!k.dense) {
+            // each lane that gained lava has its tile's neighbourhood scheduled by the whole warp
+            unsigned todo = __ballot_sync(0xFFFFFFFFu, gained);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t tl = __shfl_sync(0xFFFFFFFFu, tile, src);
+                schedule_around(k, tl, t, nxt, lane, true);
+            }
+        }
+    }
+    const unsigned b = __reduce_add_sync(0xFFFFFFFFu, born);
+    if (lane == 0) s_red[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long sb = 0;
+        for (int wv = 0; wv < kThreads / 32; ++wv) sb += s_red[wv];
+        if (sb) {
+            atomicAdd(&ctrl->acc_active, sb);
+            atomicAdd(&ctrl->acc_changed, sb);
+            atomicAdd(&ctrl->acc_born, sb);
+        }
         __threadfence();
-        const unsigned ticket = atomicAdd(&ctrl->ticket, 1u);
-        s_last = ticket == gridDim.x - 1;
+        s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (s_last && tid == 0) {
+    if (s_last && threadIdx.x == 0) {
         __threadfence();
         const unsigned long long active = atomicExch(&ctrl->acc_active, 0ull);
         const unsigned long long changed = atomicExch(&ctrl->acc_changed, 0ull);
-        const unsigned long long born = atomicExch(&ctrl->acc_born, 0ull);
+        const unsigned long long nborn = atomicExch(&ctrl->acc_born, 0ull);
         const unsigned long long tiles = atomicExch(&ctrl->acc_tiles, 0ull);
         ctrl->ticket = 0;
-        const uint64_t air = ctrl->air - born;
+        ctrl->cand_count = 0;
+        const uint64_t air = ctrl->air - nborn;
         ctrl->air = air;
         ctrl->lava = active;
         ctrl->tiles_processed += tiles;
@@ -555,8 +648,8 @@ __global__ __launch_bounds__(kThreads) void ca_rules_kernel(CaKernelArgs k) {
 // Set-up kernels.
 // ------------------------------------------------------------------------------------------
 // Per-tile LAVA flag of the current state and the LAVA / AIR totals (countInitialState,
-// LavaCA.hpp:1252-1280).  One block per tile.
-__global__ __launch_bounds__(kThreads) void ca_tile_init_kernel(CaKernelArgs k, int cur) {
+// LavaCA.hpp:1252-1280), accumulated into ctrl->acc_active / acc_born.
+__global__ __launch_bounds__(kThreads) void ca_tile_init_kernel(const __grid_constant__ CaKernelArgs k, int cur) {
     const CaGeom& g = k.g;
     const int xq = threadIdx.x & 15, row = threadIdx.x >> 4;
     const int ly = row % g.TY, lz = row / g.TY;
@@ -571,14 +664,10 @@ __global__ __launch_bounds__(kThreads) void ca_tile_init_kernel(CaKernelArgs k, 
         if (y < g.ny && z < g.nz) {
             const uint32_t w = *reinterpret_cast<const uint32_t*>(k.type[cur] + pidx(g, x, y, z));
             lava = __popc(__vcmpeq4(w, 0x02020202u)) >> 3;
-            air = __popc(__vcmpeq4(w, 0u)) >> 3;
-            // padding cells are VOID, so they count as neither
+            air = __popc(__vcmpeq4(w, 0u)) >> 3;  // padding cells are VOID, so they count as neither
         }
         const int any = __syncthreads_or(lava > 0);
-        if (threadIdx.x == 0) {
-            k.tile_flags[cur][tile] = any ? 1u : 0u;
-            k.tile_flags[cur ^ 1][tile] = 0u;
-        }
+        if (threadIdx.x == 0) k.tile_flags[tile] = any ? 1u : 0u;
         const unsigned la = __reduce_add_sync(0xFFFFFFFFu, lava);
         const unsigned ai = __reduce_add_sync(0xFFFFFFFFu, air);
         if ((threadIdx.x & 31) == 0) {
@@ -591,6 +680,37 @@ __global__ __launch_bounds__(kThreads) void ca_tile_init_kernel(CaKernelArgs k, 
     if (threadIdx.x == 0) {
         atomicAdd(&k.ctrl->acc_active, s_cnt[0]);
         atomicAdd(&k.ctrl->acc_born, s_cnt[1]);
+    }
+}
+
+// The tile list of the first step: every tile within one tile of a tile holding LAVA.
+__global__ void ca_init_schedule_kernel(const __grid_constant__ CaKernelArgs k, uint32_t t0) {
+    const CaGeom& g = k.g;
+    const int cur = t0 & 1;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < k.ntiles; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t tile = base + threadIdx.x;
+        bool process = false;
+        if (tile < k.ntiles) {
+            const int tx = (int)(tile % g.tiles_x);
+            const uint64_t r = tile / g.tiles_x;
+            const int ty = (int)(r % g.tiles_y), tz = (int)(r / g.tiles_y);
+            for (int dz = -1; dz <= 1 && !process; ++dz)
+                for (int dy = -1; dy <= 1 && !process; ++dy)
+                    for (int dx = -1; dx <= 1 && !process; ++dx) {
+                        int xx = tx + dx, yy = ty + dy, zz = tz + dz;
+                        if (!wrap_axis(xx, g.tiles_x, g.per[0]) || !wrap_axis(yy, g.tiles_y, g.per[1]) ||
+                            !wrap_axis(zz, g.tiles_z, g.per[2]))
+                            continue;
+                        process = (k.tile_flags[xx + (uint64_t)g.tiles_x * (yy + (uint64_t)g.tiles_y * zz)] & 1u) != 0;
+                    }
+            if (process) k.tile_mark[tile] = t0 + 1;
+        }
+        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, process);
+        const unsigned lane = threadIdx.x & 31;
+        unsigned slot = 0;
+        if (lane == 0 && ballot) slot = atomicAdd(&k.ctrl->list_count[cur], (unsigned)__popc(ballot));
+        slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+        if (process) k.tile_list[cur][slot + __popc(ballot & ((1u << lane) - 1u))] = (uint32_t)tile;
     }
 }
 
@@ -618,137 +738,25 @@ __global__ void ca_terrain_kernel(uint8_t* type, const int32_t* heights, int nx,
     }
 }
 
+// Vents / seeds: CellState{Lava, flowId, temp, 0, 0} (LavaCA::placeSeeds, LavaCA.hpp:215-220).
+__global__ void ca_seed_kernel(const __grid_constant__ CaKernelArgs k, const int4* seeds, int count, int cur, float temp) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int4 s = seeds[i];
+        const int64_t p = pidx(k.g, s.x, s.y, s.z);
+        k.type[cur][p] = kLava;
+        k.flow[cur][p] = s.w;
+        k.temp[cur][p] = temp;
+        k.solid[cur][p] = 0;
+        k.arrival[cur][p] = 0;
+    }
+}
+
 }  // namespace vca
 
 // ============================================================================================
 // Host side
 // ============================================================================================
 using namespace vca;
-
-namespace vca {
-
-static thread_local std::string g_last_error;
-
-void set_error(const std::string& msg) { g_last_error = msg; }
-
-vca_status cuda_fail(cudaError_t e, const char* what) {
-    set_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
-    return e == cudaErrorMemoryAllocation ? VCA_ERR_NOMEM : VCA_ERR_CUDA;
-}
-
-// TerrainGenerator::fillDepressions (engine/src/terrain/TerrainGenerator.cpp:86-161): priority
-// flood from the outlets (non-periodic edges; on a fully wrapped map, the lowest columns).
-std::vector<int32_t> fill_depressions(const std::vector<int32_t>& h, int nx, int ny, bool px, bool py) {
-    const size_t n = h.size();
-    std::vector<int32_t> filled = h;
-    std::vector<char> closed(n, 0);
-    using Item = std::pair<int32_t, size_t>;
-    std::priority_queue<Item, std::vector<Item>, std::greater<Item>> open;
-    auto seed = [&](size_t i) {
-        if (!closed[i]) {
-            closed[i] = 1;
-            open.push({h[i], i});
-        }
-    };
-    for (int y = 0; y < ny; ++y)
-        for (int x = 0; x < nx; ++x) {
-            const bool ex = !px && nx > 1 && (x == 0 || x == nx - 1);
-            const bool ey = !py && ny > 1 && (y == 0 || y == ny - 1);
-            if (ex || ey) seed((size_t)x + (size_t)nx * y);
-        }
-    if (open.empty() && n > 0) {
-        const int32_t lowest = *std::min_element(h.begin(), h.end());
-        for (size_t i = 0; i < n; ++i)
-            if (h[i] == lowest) seed(i);
-    }
-    const int dx[4] = {-1, 1, 0, 0}, dy[4] = {0, 0, -1, 1};
-    while (!open.empty()) {
-        const Item it = open.top();
-        open.pop();
-        const int x = (int)(it.second % (size_t)nx), y = (int)(it.second / (size_t)nx);
-        for (int d = 0; d < 4; ++d) {
-            int sx = x + dx[d], sy = y + dy[d];
-            if (sx < 0 || sx >= nx) {
-                if (!px || nx == 1) continue;
-                sx = (sx + nx) % nx;
-            }
-            if (sy < 0 || sy >= ny) {
-                if (!py || ny == 1) continue;
-                sy = (sy + ny) % ny;
-            }
-            const size_t j = (size_t)sx + (size_t)nx * sy;
-            if (closed[j]) continue;
-            closed[j] = 1;
-            filled[j] = std::max(h[j], it.first);
-            open.push({filled[j], j});
-        }
-    }
-    return filled;
-}
-
-// Neighbourhood tables (engine/src/core/Neighborhood.cpp:18-119): 2D in the plane of the two
-// axes of size > 1 (v outer, u inner), 3D in dz, dy, dx order.
-bool build_nb(int kind, int nx, int ny, int nz, NbTable& t) {
-    std::memset(&t, 0, sizeof(t));
-    const int sizes[3] = {nx, ny, nz};
-    int plane[3] = {0, 0, 0}, axes = 0;
-    for (int a = 0; a < 3; ++a)
-        if (sizes[a] > 1) plane[axes++] = a;
-    if (axes < 2) return false;
-    auto keep2 = [&](int var, int u, int v) -> bool {
-        switch (kind) {
-            case VCA_NB_VON_NEUMANN: return std::abs(u) + std::abs(v) == 1;
-            case VCA_NB_MOORE: return true;
-            case VCA_NB_PENTAGONAL: return var == 0 ? u != -1 : var == 1 ? u != 1 : var == 2 ? v != -1 : v != 1;
-            default: return var == 0 ? !((u == -1 && v == -1) || (u == 1 && v == 1)) : !((u == -1 && v == 1) || (u == 1 && v == -1));
-        }
-    };
-    auto keep3 = [&](int var, int dx, int dy, int dz) -> bool {
-        switch (kind) {
-            case VCA_NB_VON_NEUMANN: return std::abs(dx) + std::abs(dy) + std::abs(dz) == 1;
-            case VCA_NB_MOORE: return true;
-            default: {
-                const int c[6] = {dx != -1, dx != 1, dy != -1, dy != 1, dz != -1, dz != 1};
-                return c[var] != 0;
-            }
-        }
-    };
-    if (axes == 2) {
-        t.variants = kind == VCA_NB_PENTAGONAL ? 4 : kind == VCA_NB_HEXAGONAL ? 2 : 1;
-        for (int var = 0; var < t.variants; ++var) {
-            int k = 0;
-            for (int v = -1; v <= 1; ++v)
-                for (int u = -1; u <= 1; ++u) {
-                    if ((u == 0 && v == 0) || !keep2(var, u, v)) continue;
-                    int d[3] = {0, 0, 0};
-                    d[plane[0]] = u;
-                    d[plane[1]] = v;
-                    for (int a = 0; a < 3; ++a) t.off[var][k][a] = (int8_t)d[a];
-                    ++k;
-                }
-            t.count[var] = k;
-        }
-    } else {
-        if (kind == VCA_NB_HEXAGONAL) return false;
-        t.variants = kind == VCA_NB_PENTAGONAL ? 6 : 1;
-        for (int var = 0; var < t.variants; ++var) {
-            int k = 0;
-            for (int dz = -1; dz <= 1; ++dz)
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        if ((dx == 0 && dy == 0 && dz == 0) || !keep3(var, dx, dy, dz)) continue;
-                        t.off[var][k][0] = (int8_t)dx;
-                        t.off[var][k][1] = (int8_t)dy;
-                        t.off[var][k][2] = (int8_t)dz;
-                        ++k;
-                    }
-            t.count[var] = k;
-        }
-    }
-    return true;
-}
-
-}  // namespace vca
 
 namespace {
 
@@ -781,10 +789,16 @@ CaKernelArgs make_args(const vca_ca* h) {
         k.temp[b] = h->temp[b];
         k.solid[b] = h->solid[b];
         k.arrival[b] = h->arrival[b];
-        k.tile_flags[b] = h->tile_flags[b];
         k.tile_list[b] = h->tile_list[b];
     }
-    k.desc = h->desc_plane;
+    k.tile_flags = h->tile_flags;
+    k.tile_mark = h->tile_mark;
+    k.drop = h->drop_plane;
+    k.chg_list[0] = h->chg_list[0];
+    k.chg_list[1] = h->chg_list[1];
+    k.chg_cap = h->chg_cap;
+    k.cand_list = h->cand_list;
+    k.cand_cap = h->cand_cap;
     k.spill = h->has_terrain ? h->spill : nullptr;
     k.vents = h->vents;
     k.vent_slots = h->vent_slots;
@@ -813,7 +827,7 @@ vca_status sync_ctrl(vca_ca* h) {
     return VCA_OK;
 }
 
-// Tile flags, LAVA/AIR totals and the initial stop state of the current buffer, and a copy of the
+// Totals and initial stop state of the current buffer, the first tile list, and a copy of the
 // current buffer into the other one (both buffers equal: the ACTIVE schedule relies on it).
 vca_status init_state(vca_ca* h, int steps_done) {
     const int cur = steps_done & 1, oth = cur ^ 1;
@@ -823,6 +837,7 @@ vca_status init_state(vca_ca* h, int steps_done) {
     VCA_CUDA(cudaMemcpyAsync(h->temp[oth], h->temp[cur], n * 4, cudaMemcpyDeviceToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->solid[oth], h->solid[cur], n * 2, cudaMemcpyDeviceToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->arrival[oth], h->arrival[cur], n * 2, cudaMemcpyDeviceToDevice, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->tile_mark, 0, h->ntiles * 4, h->stream));
     CaCtrl c;
     std::memset(&c, 0, sizeof(c));
     c.steps = (uint32_t)steps_done;
@@ -834,7 +849,14 @@ vca_status init_state(vca_ca* h, int steps_done) {
     const int blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)h->grid_blocks * 4);
     ca_tile_init_kernel<<<blocks, kThreads, 0, h->stream>>>(k, cur);
     VCA_CUDA(cudaGetLastError());
-    if (vca_status s_ = sync_ctrl(h)) return s_;
+    ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 1);
+    VCA_CUDA(cudaGetLastError());
+    if (!k.dense) {
+        const int sb = (int)std::min<uint64_t>((h->ntiles + 255) / 256, 4096);
+        ca_init_schedule_kernel<<<sb, 256, 0, h->stream>>>(k, (uint32_t)steps_done);
+        VCA_CUDA(cudaGetLastError());
+    }
+    if (vca_status s = sync_ctrl(h)) return s;
     CaCtrl* m = h->ctrl_host;
     const uint64_t lava = m->acc_active, air = m->acc_born;
     m->acc_active = 0;
@@ -866,15 +888,11 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
     int done = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
     size_t ev_used = 0;
+    const int steps_before = h->steps;
     while (true) {
         const int n = until_stop ? chunk : std::min(chunk, max_new_steps - done);
         for (int s = 0; s < n; ++s) {
-            if (!k.dense) {
-                const int threads = 256;
-                const int blocks = (int)std::min<uint64_t>((h->ntiles + threads - 1) / threads, 148 * 8);
-                ca_schedule_kernel<<<blocks, threads, 0, h->stream>>>(k);
-            }
-            ca_descent_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
+            ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
             if (h->profile_kernels) {
                 while (h->prof_events.size() < ev_used + 2) {
                     cudaEvent_t e;
@@ -890,10 +908,12 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
             } else {
                 ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
             }
+            ca_cand_kernel<<<h->cand_blocks, kThreads, 0, h->stream>>>(k);
         }
         VCA_CUDA(cudaGetLastError());
+        h->launches += (uint64_t)n * 3;
         done += n;
-        if (vca_status s_ = sync_ctrl(h)) return s_;
+        if (vca_status s = sync_ctrl(h)) return s;
         if (h->stop != VCA_STOP_RUNNING) break;
         if (!until_stop && done >= max_new_steps) break;
         chunk = std::min(chunk * 2, 256);
@@ -904,15 +924,13 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
     VCA_CUDA(cudaEventElapsedTime(&ms, h->ev_a, h->ev_b));
     h->total_ms += ms;
     if (h->profile_kernels) {
-        // Only launches that did work (steps actually taken) count; launches after the stop exit at once.
-        const uint64_t real = std::min<uint64_t>(prof.size(), (uint64_t)h->steps);
-        for (size_t i = 0; i < prof.size(); ++i) {
+        // Launches after the stop exit at once; only the ones that did a step count.
+        const uint64_t real = std::min<uint64_t>(prof.size(), (uint64_t)(h->steps - steps_before));
+        for (size_t i = 0; i < real; ++i) {
             float m = 0.f;
             VCA_CUDA(cudaEventElapsedTime(&m, prof[i].first, prof[i].second));
-            if (i < real) {
-                h->rules_ms += m;
-                ++h->rules_launches;
-            }
+            h->rules_ms += m;
+            ++h->rules_launches;
         }
     }
     return VCA_OK;
@@ -926,10 +944,14 @@ void free_all(vca_ca* h) {
         cudaFree(h->temp[b]);
         cudaFree(h->solid[b]);
         cudaFree(h->arrival[b]);
-        cudaFree(h->tile_flags[b]);
         cudaFree(h->tile_list[b]);
     }
-    cudaFree(h->desc_plane);
+    cudaFree(h->tile_flags);
+    cudaFree(h->tile_mark);
+    cudaFree(h->drop_plane);
+    cudaFree(h->chg_list[0]);
+    cudaFree(h->chg_list[1]);
+    cudaFree(h->cand_list);
     cudaFree(h->spill);
     cudaFree(h->vents);
     cudaFree(h->tables);
@@ -958,7 +980,7 @@ vca_status upload_vents(vca_ca* h, const vca_vent* vents, int count) {
     return VCA_OK;
 }
 
-// Copy host planes (unpitched) into the pitched current buffer.
+// Host planes (unpitched) <-> pitched device planes.
 template <class T>
 vca_status put_plane(vca_ca* h, T* dst, const T* src) {
     const auto& g = h->geom;
@@ -977,10 +999,6 @@ vca_status get_plane(vca_ca* h, T* dst, const T* src) {
 }  // namespace
 
 extern "C" {
-
-const char* vca_last_error(void) { return g_last_error.c_str(); }
-
-const char* vca_version(void) { return "vca 1 sm_100a (lava CA + Potts checkerboard MC)"; }
 
 vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     if (d == nullptr || out == nullptr) {
@@ -1072,10 +1090,10 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     h->ntiles = (uint64_t)g.tiles_x * g.tiles_y * g.tiles_z;
     h->plane_cells = (size_t)g.P * ny * nz;
     const size_t n = h->plane_cells;
-#define ALLOC(ptr, bytes)                                   \
-    do {                                                    \
-        e = cudaMalloc(&(ptr), (bytes));                    \
-        if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc " #ptr)); \
+#define ALLOC(ptr, bytes)                                                         \
+    do {                                                                          \
+        e = cudaMalloc(&(ptr), (bytes));                                          \
+        if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc " #ptr));      \
     } while (0)
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
@@ -1085,10 +1103,16 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
         ALLOC(h->temp[b], n * 4);
         ALLOC(h->solid[b], n * 2);
         ALLOC(h->arrival[b], n * 2);
-        ALLOC(h->tile_flags[b], h->ntiles * 4);
         ALLOC(h->tile_list[b], h->ntiles * 4);
     }
-    ALLOC(h->desc_plane, n);
+    ALLOC(h->tile_flags, h->ntiles * 4);
+    ALLOC(h->tile_mark, h->ntiles * 4);
+    ALLOC(h->drop_plane, n);
+    h->chg_cap = (uint32_t)std::min<uint64_t>((uint64_t)nx * ny * nz, 1u << 22);
+    ALLOC(h->chg_list[0], sizeof(uint32_t) * (size_t)h->chg_cap);
+    ALLOC(h->chg_list[1], sizeof(uint32_t) * (size_t)h->chg_cap);
+    h->cand_cap = (uint32_t)((uint64_t)nx * ny * nz);
+    ALLOC(h->cand_list, sizeof(uint32_t) * (size_t)h->cand_cap);
     ALLOC(h->tables, sizeof(CaTables));
     ALLOC(h->ctrl, sizeof(CaCtrl));
     ALLOC(h->hist_active, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
@@ -1101,11 +1125,12 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
             (e = cudaMemsetAsync(h->flow[b], 0, n * 4, h->stream)) != cudaSuccess ||
             (e = cudaMemsetAsync(h->temp[b], 0, n * 4, h->stream)) != cudaSuccess ||
             (e = cudaMemsetAsync(h->solid[b], 0, n * 2, h->stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(h->arrival[b], 0, n * 2, h->stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(h->tile_flags[b], 0, h->ntiles * 4, h->stream)) != cudaSuccess)
+            (e = cudaMemsetAsync(h->arrival[b], 0, n * 2, h->stream)) != cudaSuccess)
             return fail(cuda_fail(e, "cudaMemsetAsync"));
     }
-    if ((e = cudaMemsetAsync(h->desc_plane, 0xFF, n, h->stream)) != cudaSuccess) return fail(cuda_fail(e, "cudaMemsetAsync"));
+    if ((e = cudaMemsetAsync(h->drop_plane, 0xFF, n, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->tile_mark, 0, h->ntiles * 4, h->stream)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaMemsetAsync"));
     if (g.P > nx) {
         ca_pad_kernel<<<256, 256, 0, h->stream>>>(h->type[0], h->type[1], nx, g.P, (int64_t)ny * nz);
         if ((e = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, "ca_pad_kernel"));
@@ -1116,14 +1141,13 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ca_rules_kernel, kThreads, 0);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
     h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)prop.multiProcessorCount * std::max(1, per_sm));
+    h->cand_blocks = prop.multiProcessorCount * 2;
     if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaEventCreate"));
     const char* prof = std::getenv("VCA_PROFILE_KERNELS");
     h->profile_kernels = prof != nullptr && prof[0] == '1';
-    // An empty vent table and an initial control block (no seeds yet).
     vca_vent none{0, 0, 0, 0};
-    vca_status s = upload_vents(h, &none, 0);
-    if (s != VCA_OK) return fail(s);
+    if (vca_status s = upload_vents(h, &none, 0)) return fail(s);
     e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamSynchronize"));
     *out = h;
@@ -1162,6 +1186,7 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     cudaFree(dh);
     h->has_terrain = true;
+    h->launches += 1;
     return VCA_OK;
 }
 
@@ -1175,22 +1200,37 @@ vca_status vca_ca_place_seeds(vca_ca* h, const vca_vent* vents, int count) {
     const auto& g = h->geom;
     const int cur = h->steps & 1;
     const float temp = h->desc.mode == VCA_MODE_LAVA ? h->desc.erupt_temp : 0.0f;
+    std::vector<int4> seeds((size_t)count);
     for (int i = 0; i < count; ++i) {
         const vca_vent& v = vents[i];
         if (v.x < 0 || v.x >= g.nx || v.y < 0 || v.y >= g.ny || v.z < 0 || v.z >= g.nz) {
             set_error("vca_ca_place_seeds: vent " + std::to_string(i) + " lies outside the grid");
             return VCA_ERR_ARG;
         }
-        // CellState{Lava, flowId, temp, 0, 0} (LavaCA.hpp:219)
-        const size_t p = (size_t)v.x + (size_t)g.P * ((size_t)v.y + (size_t)g.ny * v.z);
-        const uint8_t lava = VCA_LAVA;
-        const uint16_t zero16 = 0;
-        VCA_CUDA(cudaMemcpyAsync(h->type[cur] + p, &lava, 1, cudaMemcpyHostToDevice, h->stream));
-        VCA_CUDA(cudaMemcpyAsync(h->flow[cur] + p, &v.flow_id, 4, cudaMemcpyHostToDevice, h->stream));
-        VCA_CUDA(cudaMemcpyAsync(h->temp[cur] + p, &temp, 4, cudaMemcpyHostToDevice, h->stream));
-        VCA_CUDA(cudaMemcpyAsync(h->solid[cur] + p, &zero16, 2, cudaMemcpyHostToDevice, h->stream));
-        VCA_CUDA(cudaMemcpyAsync(h->arrival[cur] + p, &zero16, 2, cudaMemcpyHostToDevice, h->stream));
-        VCA_CUDA(cudaStreamSynchronize(h->stream));  // the sources live on this stack frame
+        seeds[(size_t)i] = make_int4(v.x, v.y, v.z, v.flow_id);
+    }
+    if (count > 0) {
+        // A repeated cell keeps its last entry, as the reference's sequential writes do; the
+        // remaining cells are distinct, so the scatter below is order-free.
+        std::vector<std::pair<uint64_t, int>> keyed((size_t)count);
+        for (int i = 0; i < count; ++i) {
+            const int4& s = seeds[(size_t)i];
+            keyed[(size_t)i] = {(uint64_t)s.x + (uint64_t)g.nx * ((uint64_t)s.y + (uint64_t)g.ny * s.z), i};
+        }
+        std::sort(keyed.begin(), keyed.end());
+        std::vector<int4> uniq;
+        uniq.reserve((size_t)count);
+        for (size_t i = 0; i < keyed.size(); ++i)
+            if (i + 1 == keyed.size() || keyed[i + 1].first != keyed[i].first) uniq.push_back(seeds[(size_t)keyed[i].second]);
+        const int nu = (int)uniq.size();
+        int4* ds = nullptr;
+        VCA_CUDA(cudaMalloc(&ds, sizeof(int4) * (size_t)nu));
+        VCA_CUDA(cudaMemcpyAsync(ds, uniq.data(), sizeof(int4) * (size_t)nu, cudaMemcpyHostToDevice, h->stream));
+        ca_seed_kernel<<<std::min(1184, (nu + 255) / 256), 256, 0, h->stream>>>(make_args(h), ds, nu, cur, temp);
+        VCA_CUDA(cudaGetLastError());
+        VCA_CUDA(cudaStreamSynchronize(h->stream));
+        cudaFree(ds);
+        h->launches += 1;
     }
     if (vca_status s = upload_vents(h, vents, count)) return s;
     h->seeded = true;
@@ -1257,6 +1297,7 @@ vca_status vca_ca_get_info(vca_ca* h, vca_ca_info* out) {
     out->tiles_total = h->ntiles;
     out->tiles_processed = h->ctrl_host->tiles_processed;
     out->cells_per_tile = (uint64_t)kTileX * h->geom.TY * h->geom.TZ;
+    out->kernel_launches = h->launches;
     return VCA_OK;
 }
 
@@ -1314,16 +1355,8 @@ void vca_ca_destroy(vca_ca* h) {
 
 }  // extern "C"
 
-// Accessors used by the MC half (mc.cu) to build the crystallisation domain on the device.
+// Accessor used by the MC half (mc.cu) to build the crystallisation domain on the device.
 namespace vca {
-struct CaView {
-    const uint8_t* type;
-    const uint16_t* solid;
-    const uint16_t* arrival;
-    int nx, ny, nz, P;
-    cudaStream_t stream;
-    int device;
-};
 vca_status ca_view(vca_ca* h, CaView* v) {
     if (vca_status s = check(h)) return s;
     if (vca_status s = sync_ctrl(h)) return s;

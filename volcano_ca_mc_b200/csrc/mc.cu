@@ -29,17 +29,6 @@
 
 namespace vca {
 
-bool build_nb(int kind, int nx, int ny, int nz, NbTable& t);
-struct CaView {
-    const uint8_t* type;
-    const uint16_t* solid;
-    const uint16_t* arrival;
-    int nx, ny, nz, P;
-    cudaStream_t stream;
-    int device;
-};
-vca_status ca_view(vca_ca* h, CaView* v);
-
 constexpr int kMcThreads = 256;
 constexpr int kTableSide = 27;  // unlike counts 0..26
 
@@ -365,6 +354,7 @@ struct vca_mc {
     double total_ms = 0.0;
     double color_ms = 0.0;
     uint64_t color_launches = 0;
+    uint64_t launches = 0;
     int profile_kernels = 0;
     std::vector<cudaEvent_t> prof_events;
 };
@@ -748,6 +738,7 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
                 prof.push_back({e0, e1});
             }
         }
+        h->launches += (uint64_t)h->colors;
         if (h->profile_kernels && prof.size() > 2048) break;  // bounded event pool per call
     }
     VCA_CUDA(cudaGetLastError());
@@ -777,6 +768,7 @@ vca_status vca_mc_get_info(vca_mc* h, vca_mc_info* out) {
     out->attempts = h->ctrl_host->attempts;
     out->accepted = h->ctrl_host->accepted;
     out->uphill = h->ctrl_host->uphill;
+    out->kernel_launches = h->launches;
     return VCA_OK;
 }
 
@@ -791,6 +783,7 @@ vca_status vca_mc_energy(vca_mc* h, double* energy) {
     const uint64_t total = h->color_off.back();
     const bool forward = h->nb_host.variants == 1;
     if (total) mc_energy_kernel<<<grid_for(total, h->sms), kMcThreads, 0, h->stream>>>(mc_args(h), h->list, total, forward);
+    h->launches += total ? 1 : 0;
     VCA_CUDA(cudaGetLastError());
     if (vca_status s_ = mc_sync(h)) return s_;
     const double unlike = (double)h->ctrl_host->energy_acc;

@@ -15,6 +15,8 @@ namespace vca {
 // Error channel of the C ABI: the message of the last failure on this host thread.
 void set_error(const std::string& msg);
 vca_status cuda_fail(cudaError_t e, const char* what);
+std::vector<int32_t> fill_depressions(const std::vector<int32_t>& h, int nx, int ny, bool px, bool py);
+bool build_nb(int kind, int nx, int ny, int nz, NbTable& t);
 
 #define VCA_CUDA(call)                                              \
     do {                                                            \
@@ -35,7 +37,8 @@ struct CaCtrl {
     unsigned long long acc_tiles;
     unsigned int ticket;      // blocks finished in the running rules launch
     unsigned int list_count[2];
-    unsigned int pad;
+    unsigned int chg_count[2];  // cells whose type changed in the step that wrote them
+    unsigned int cand_count;    // AIR cells listed for the candidate pass of the running step
     unsigned long long tiles_processed;  // tiles visited over all steps
     int32_t max_steps;
     int32_t random_nb;
@@ -75,18 +78,34 @@ struct CaKernelArgs {
     float* temp[2];
     uint16_t* solid[2];
     uint16_t* arrival[2];
-    int8_t* desc;
+    int8_t* drop;             // dropDepth of every AIR cell of the current state (LavaCA.hpp:404-414)
+    uint32_t* chg_list[2];    // globalIndex of cells whose type changed (step t writes [(t+1) & 1])
+    uint32_t chg_cap;         // capacity of each change list; more changes force a full rescan
+    uint32_t* cand_list;      // globalIndex of AIR cells with LAVA within one cell (this step)
+    uint32_t cand_cap;        // = cells of the grid: the list can never overflow
     const int32_t* spill;     // nx*ny or nullptr
     const int4* vents;        // (x, y, z, -) per flowId
     int vent_slots;
     const CaTables* tables;
     CaCtrl* ctrl;
-    uint32_t* tile_flags[2];  // bit 0: LAVA in tile after the step, bit 1: a cell changed
-    uint32_t* tile_list[2];
+    uint32_t* tile_flags;     // set-up only: bit 0 = LAVA in the tile
+    uint32_t* tile_mark;      // (step + 1) the tile was last scheduled for
+    uint32_t* tile_list[2];   // tiles of step t are tile_list[t & 1]
     unsigned long long* hist_active;
     unsigned long long* hist_changed;
     uint64_t ntiles;
 };
+
+// Read-only view of a CA handle's current planes (the MC domain and mobility are built from it).
+struct CaView {
+    const uint8_t* type;
+    const uint16_t* solid;
+    const uint16_t* arrival;
+    int nx, ny, nz, P;
+    cudaStream_t stream;
+    int device;
+};
+vca_status ca_view(vca_ca* h, CaView* v);
 
 }  // namespace vca
 
@@ -105,14 +124,20 @@ struct vca_ca {
     float* temp[2] = {nullptr, nullptr};
     uint16_t* solid[2] = {nullptr, nullptr};
     uint16_t* arrival[2] = {nullptr, nullptr};
-    int8_t* desc_plane = nullptr;
+    int8_t* drop_plane = nullptr;
+    uint32_t* chg_list[2] = {nullptr, nullptr};
+    uint32_t chg_cap = 0;
+    uint32_t* cand_list = nullptr;
+    uint32_t cand_cap = 0;
+    int cand_blocks = 0;      // grid of the candidate pass
     int32_t* spill = nullptr;
     int4* vents = nullptr;
     int vent_slots = 0;
     vca::CaTables* tables = nullptr;
     vca::CaCtrl* ctrl = nullptr;
     vca::CaCtrl* ctrl_host = nullptr;   // pinned mirror
-    uint32_t* tile_flags[2] = {nullptr, nullptr};
+    uint32_t* tile_flags = nullptr;
+    uint32_t* tile_mark = nullptr;
     uint32_t* tile_list[2] = {nullptr, nullptr};
     unsigned long long* hist_active = nullptr;
     unsigned long long* hist_changed = nullptr;
@@ -126,6 +151,7 @@ struct vca_ca {
     double total_ms = 0.0;
     double rules_ms = 0.0;
     uint64_t rules_launches = 0;
+    uint64_t launches = 0;    // kernel launches issued
     int profile_kernels = 0;  // bracket each rules launch with events (set by VCA_PROFILE_KERNELS=1)
     std::vector<cudaEvent_t> prof_events;
 };
