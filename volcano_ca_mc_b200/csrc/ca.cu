@@ -208,64 +208,50 @@ __device__ __forceinline__ int type_at(const CaGeom& g, const uint8_t* T, int x,
     return __ldg(T + pidx(g, x, y, z));
 }
 
-// D(n) of a LAVA cell n (descent + computeDescent, LavaCA.hpp:421-429, 551-566): -1 without support,
-// else the largest drop depth among its AIR side neighbours (at least 0).
-__device__ __forceinline__ int descent_of(const CaKernelArgs& k, const uint8_t* T, int sx, int sy, int sz) {
-    const CaGeom& g = k.g;
-    if (sz > 0) {
-        const int below = __ldg(T + pidx(g, sx, sy, sz - 1));
-        const bool sup = solid_ground(below) ||
-                         (below == kLava && k.spill != nullptr && sz - 1 < __ldg(k.spill + sx + (int64_t)g.nx * sy));
-        if (!sup) return -1;
-    }
-    const CaTables* tb = k.tables;
-    const int nside = tb->nside;
-    int best = 0;
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        if (s >= nside) break;
-        int ax = sx + tb->side[s][0], ay = sy + tb->side[s][1];
-        if (!wrap_axis(ax, g.nx, g.per[0]) || !wrap_axis(ay, g.ny, g.per[1])) continue;
-        const int64_t q = pidx(g, ax, ay, sz);
-        const int tq = __ldg(T + q);
-        const int dq = k.drop[q];
-        if (tq == kAir) best = max(best, dq);
-    }
-    return best;
-}
-
 // gatherLavaCandidates + tryPonding (LavaCA.hpp:443-519) or updateClassic's vote (1176-1182), the
 // winner (CaRules.hpp:152-173) and the solidus test.  Returns true when the cell becomes LAVA.
+// The neighbour types of the cell's variant are fetched together first (independent loads); only
+// the LAVA ones are then examined, in any order (the vote does not depend on the order).
 __device__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, const float* Te, int x, int y,
                                int z, uint64_t prefix, uint64_t gidx, int32_t* out_flow, float* out_temp) {
     const CaGeom& g = k.g;
-    const NbTable& nb = k.tables->nb;
+    const NbTable& nb = k.tables.nb;
     const int var = nb.variants == 1 ? 0 : (int)fast_mod(hash_salt(hash_index(prefix, gidx), kSaltNeighborhood), k.var_mod);
     const int cnt = nb.count[var];
+    uint32_t lava_mask = 0;
+#pragma unroll
+    for (int i = 0; i < 26; ++i) {
+        if (i < cnt) {
+            int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
+            if (resolve(g, sx, sy, sz) && __ldg(T + pidx(g, sx, sy, sz)) == kLava) lava_mask |= 1u << i;
+        }
+    }
+    if (!lava_mask) return false;
     Vote v;
     v.n = 0;
     if (k.classic) {
-        for (int i = 0; i < cnt; ++i) {
+        while (lava_mask) {
+            const int i = __ffs(lava_mask) - 1;
+            lava_mask &= lava_mask - 1;
             int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
-            if (!resolve(g, sx, sy, sz)) continue;
-            const int64_t s = pidx(g, sx, sy, sz);
-            if (__ldg(T + s) == kLava) v.add(__ldg(F + s), 0.0f);
+            resolve(g, sx, sy, sz);
+            v.add(__ldg(F + pidx(g, sx, sy, sz)), 0.0f);
         }
-        if (v.n == 0) return false;
         const int w = v.winner(prefix, gidx);
         *out_flow = v.ids[w];
         *out_temp = 0.0f;
         return true;
     }
-    int c_drop = -100;
-    for (int i = 0; i < cnt; ++i) {
+    const int c_drop = k.drop[pidx(g, x, y, z)];
+    while (lava_mask) {
+        const int i = __ffs(lava_mask) - 1;
+        lava_mask &= lava_mask - 1;
         const int dx = nb.off[var][i][0], dy = nb.off[var][i][1], dz = nb.off[var][i][2];
         if (dz < 0) {
             if (!(k.ponding && dx == 0 && dy == 0)) continue;
-            // tryPonding (LavaCA.hpp:443-461)
+            // tryPonding (LavaCA.hpp:443-461); the cell below is LAVA
             if (k.spill == nullptr || z > __ldg(k.spill + x + (int64_t)g.nx * y)) continue;
             const int bz = z - 1;
-            if (type_at(g, T, x, y, bz) != kLava) continue;
             if (bz > 0) {  // hasSupport(x, y, bz)
                 const int below = __ldg(T + pidx(g, x, y, bz - 1));
                 const bool sup = solid_ground(below) || (below == kLava && bz - 1 < __ldg(k.spill + x + (int64_t)g.nx * y));
@@ -284,16 +270,14 @@ __device__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const in
             continue;
         }
         int sx = x + dx, sy = y + dy, sz = z + dz;
-        if (!resolve(g, sx, sy, sz)) continue;  // the VOID frame is never lava
+        resolve(g, sx, sy, sz);
         const int64_t s = pidx(g, sx, sy, sz);
-        if (__ldg(T + s) != kLava) continue;
         float cooling;
         if (dz > 0 && dx == 0 && dy == 0) {
             cooling = k.cool_fall;
         } else {
-            const int d = descent_of(k, T, sx, sy, sz);
+            const int d = k.desc[s];
             if (d < 0) continue;
-            if (c_drop == -100) c_drop = k.drop[pidx(g, x, y, z)];
             if (dz > 0) {
                 if (c_drop != 0 || d != 1) continue;
                 cooling = k.cool_fall;
@@ -313,10 +297,13 @@ __device__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const in
     return true;
 }
 
-// Schedule the tiles within one tile of `tile` for step t + 1 (ACTIVE); lanes 0..26 of a warp
-// each try one target, `want` says which lanes take part.
+// Schedule the tiles within one tile of `tile` for step t + 1; lanes 0..26 of a warp each try one
+// target, `want` says which lanes take part.  The mark of a tile scheduled for step s is
+// 2 (s + 1) plus a lava bit: the bit says that LAVA lies within one tile, so the tile's cells may
+// change; without it the tile is only refreshed (its two buffers differ) by a plain copy.  Marks
+// are kept per step parity, so a mark read during step s is never raised during step s.
 __device__ __forceinline__ void schedule_around(const CaKernelArgs& k, uint32_t tile, uint32_t t, int nxt, int lane,
-                                                bool want) {
+                                                bool want, bool lava) {
     const CaGeom& g = k.g;
     bool first = false;
     uint32_t target = 0;
@@ -328,9 +315,11 @@ __device__ __forceinline__ void schedule_around(const CaKernelArgs& k, uint32_t 
         int tz = (int)(r / (uint32_t)g.tiles_y) + dz;
         if (wrap_axis(tx, g.tiles_x, g.per[0]) && wrap_axis(ty, g.tiles_y, g.per[1]) && wrap_axis(tz, g.tiles_z, g.per[2])) {
             target = (uint32_t)tx + (uint32_t)g.tiles_x * ((uint32_t)ty + (uint32_t)g.tiles_y * tz);
-            first = atomicMax(&k.tile_mark[target], t + 2) < t + 2;
+            const uint32_t m = 2u * (t + 2u);
+            first = atomicMax(&k.tile_mark[nxt][target], m + (lava ? 1u : 0u)) < m;
         }
     }
+    if (k.dense) return;  // every tile runs anyway; the marks only choose its path
     const unsigned ballot = __ballot_sync(0xFFFFFFFFu, first);
     unsigned slot = 0;
     if (lane == 0 && ballot) slot = atomicAdd(&k.ctrl->list_count[nxt], (unsigned)__popc(ballot));
@@ -338,6 +327,9 @@ __device__ __forceinline__ void schedule_around(const CaKernelArgs& k, uint32_t 
     const unsigned pos = slot + __popc(ballot & ((1u << lane) - 1u));
     if (first && pos < k.ntiles) k.tile_list[nxt][pos] = target;  // a tile is listed once per step
 }
+
+// Shared-memory row of the tile cell (ly, lz) in the staged halo layout.
+__device__ __forceinline__ int hr_of(int ly, int lz, int hy_on, int hz_on, int HY) { return (ly + hy_on) + HY * (lz + hz_on); }
 
 // Warp-aggregated append of n entries (values v[0..n-1], n <= 4) per lane to list/count.
 __device__ __forceinline__ void warp_append(uint32_t* list, unsigned int* count, uint32_t cap, int lane, unsigned n,
@@ -355,21 +347,33 @@ __device__ __forceinline__ void warp_append(uint32_t* list, unsigned int* count,
         if (base + j < cap) list[base + j] = v[j];
 }
 
+constexpr int kMaxDeferred = 64;   // tiles a rules block schedules in one batch
+constexpr int kTileCells = 1024;   // 64 x TY x TZ, TY * TZ = 16
+constexpr int kCandBuf = 3 * kTileCells;  // candidates a rules block gathers before one flush
+
 // ------------------------------------------------------------------------------------------
 // Rules, streaming pass.  A persistent block takes one tile at a time:
 //   1. its threads load their 4 cells' state (128-bit flowId and temp, 64-bit steps, 32-bit types),
 //      then stage the tile's types with a one-cell halo in shared memory (frame semantics at the
 //      grid edges), so that the two memory latencies overlap;
-//   2. LAVA cells cool (updateLava's LAVA branch, LavaCA.hpp:1135-1151); every cell is written to
-//      the next buffer unchanged otherwise; AIR cells with LAVA within one cell (3x3x3) are listed
-//      for the candidate pass, which may overwrite them;
-//   3. cells whose type changed are listed for the drop-depth rescan;
-//   4. (ACTIVE) a tile with LAVA schedules itself and its neighbours for the next step, a tile that
-//      only changed schedules itself.
+//   2. LAVA cells cool (updateLava's LAVA branch, LavaCA.hpp:1135-1151) and get their D(n);
+//      every cell is written to the next buffer, unchanged otherwise; AIR cells with LAVA within
+//      one cell (3x3x3) are gathered in shared memory and appended to the candidate list in
+//      batches (one atomic per batch), resolved by the candidate pass;
+//   3. LAVA -> BASALT cells are listed for the drop-depth rescan;
+//   4. the block batches its tiles' flags and, after the loop, schedules the next step's tiles:
+//      with LAVA a tile and its neighbours, changed only the tile itself.
+// A tile without LAVA within one tile (mark without lava bit, or not scheduled at all in the DENSE
+// schedule) cannot change and is copied through.
 // ------------------------------------------------------------------------------------------
 __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaKernelArgs k) {
     __shared__ __align__(16) uint8_t s_type[kMaxHaloRows * kSmemRowBytes];
     __shared__ unsigned s_flags[2];
+    __shared__ unsigned s_wtot[kThreads / 32];
+    __shared__ uint32_t s_sched_tile[kMaxDeferred];
+    __shared__ uint32_t s_cand[kCandBuf];
+    __shared__ unsigned s_cand_base;
+    __shared__ uint8_t s_sched_flag[kMaxDeferred];
     __shared__ unsigned long long s_red[2][kThreads / 32];
 
     CaCtrl* ctrl = k.ctrl;
@@ -380,7 +384,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     const uint8_t* T = k.type[cur];
     const uint64_t count = k.dense ? k.ntiles : ctrl->list_count[cur];
 
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int xq = tid & 15, row = tid >> 4;
     const int ly = row % g.TY, lz = row / g.TY;
     const int hy_on = g.ny > 1 ? 1 : 0, hz_on = g.nz > 1 ? 1 : 0;
@@ -391,7 +395,27 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     if (tid == 0) s_flags[0] = s_flags[1] = 0;
 
     unsigned int my_active = 0, my_changed = 0, tiles_done = 0;
-    int it = 0;
+    int it = 0, nsched = 0;
+    unsigned nbuf = 0;  // candidates in s_cand (block-uniform)
+
+    auto flush_schedule = [&]() {
+        __syncthreads();
+        for (int e = warp; e < nsched; e += kThreads / 32) {
+            const unsigned f = s_sched_flag[e];
+            schedule_around(k, s_sched_tile[e], t, nxt, lane, (f & 1u) || ((f & 2u) && lane == 13), (f & 1u) != 0);
+        }
+        __syncthreads();
+        nsched = 0;
+    };
+    auto flush_cands = [&]() {
+        __syncthreads();
+        if (tid == 0) s_cand_base = atomicAdd(&ctrl->cand_count, nbuf);
+        __syncthreads();
+        const unsigned base = s_cand_base;
+        for (unsigned j = tid; j < nbuf; j += kThreads) k.cand_list[base + j] = s_cand[j];
+        __syncthreads();
+        nbuf = 0;
+    };
 
     for (uint64_t i = blockIdx.x; i < count; i += gridDim.x, ++it) {
         const uint32_t tile = k.dense ? (uint32_t)i : k.tile_list[cur][i];
@@ -401,6 +425,17 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
         const bool valid = y < g.ny && z < g.nz;
         const int64_t p = pidx(g, valid ? x : 0, valid ? y : 0, valid ? z : 0);
+        if (k.tile_mark[cur][tile] != 2u * (t + 1u) + 1u) {
+            // No LAVA within one tile: nothing can change here, the cells go to the next buffer as they are.
+            if (valid) {
+                *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = *reinterpret_cast<const uint32_t*>(T + p);
+                *reinterpret_cast<int4*>(k.flow[nxt] + p) = *reinterpret_cast<const int4*>(k.flow[cur] + p);
+                *reinterpret_cast<float4*>(k.temp[nxt] + p) = *reinterpret_cast<const float4*>(k.temp[cur] + p);
+                *reinterpret_cast<uint2*>(k.solid[nxt] + p) = *reinterpret_cast<const uint2*>(k.solid[cur] + p);
+                *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = *reinterpret_cast<const uint2*>(k.arrival[cur] + p);
+            }
+            continue;
+        }
 
         uint32_t w = 0xFFFFFFFFu;
         int4 f4 = make_int4(0, 0, 0, 0);
@@ -446,8 +481,8 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         const uint32_t g0 = (uint32_t)(x + g.nx * (y + g.ny * z));
         const uint32_t lava_m = __vcmpeq4(w, 0x02020202u);
         uint32_t cand_m = __vcmpeq4(w, 0u);
+        const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
         if (cand_m) {
-            const int hr = (ly + hy_on) + HY * (lz + hz_on);
             uint32_t near = 0;
             for (int dz = -hz_on; dz <= hz_on; ++dz)
                 for (int dy = -hy_on; dy <= hy_on; ++dy) {
@@ -461,10 +496,37 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                 if ((cand_m >> (8 * j)) & 0xFF) cand[ncand++] = g0 + j;
         }
         uint32_t wout = w;
+        if (lava_m && !k.classic) {
+            // D(n) of each LAVA cell of the current state (descent / computeDescent, LavaCA.hpp:421-429,
+            // 551-566), read back by the candidate pass for its lava sources.
+            const uint8_t* rowp = s_type + hr * kSmemRowBytes + 4 + 4 * xq;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (!((lava_m >> (8 * j)) & 0xFF)) continue;
+                bool sup = z == 0;
+                if (!sup) {
+                    const int below = rowp[j - HY * kSmemRowBytes];
+                    sup = solid_ground(below) ||
+                          (below == kLava && k.spill != nullptr && z - 1 < __ldg(k.spill + (x + j) + (int64_t)g.nx * y));
+                }
+                int d = -1;
+                if (sup) {
+                    d = 0;
+                    for (int s = 0; s < k.tables.nside; ++s) {
+                        const int sx = k.tables.side[s][0], sy = k.tables.side[s][1];
+                        if (rowp[j + sx + sy * kSmemRowBytes] != kAir) continue;
+                        int ax = x + j + sx, ay = y + sy;
+                        wrap_axis(ax, g.nx, g.per[0]);
+                        wrap_axis(ay, g.ny, g.per[1]);
+                        d = max(d, (int)k.drop[pidx(g, ax, ay, z)]);
+                    }
+                }
+                k.desc[p + j] = (int8_t)d;
+            }
+        }
         if (lava_m) {
             if (k.classic) {
-                const unsigned nl = __popc(lava_m) >> 3;
-                my_active += nl;
+                my_active += __popc(lava_m) >> 3;
                 any_lava = true;
             } else {
                 float te[4] = {t4.x, t4.y, t4.z, t4.w};
@@ -508,20 +570,44 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
             *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
         }
-        if (__any_sync(0xFFFFFFFFu, ncand != 0))
-            warp_append(k.cand_list, &ctrl->cand_count, k.cand_cap, lane, ncand, cand);
         if (__any_sync(0xFFFFFFFFu, nbas != 0))
             warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, nbas, bas);
 
+        // candidates: block-wide positions in the shared buffer
+        unsigned incl = ncand;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const unsigned u = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+            if (lane >= off) incl += u;
+        }
+        if (lane == 31) s_wtot[warp] = incl;
         unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
         bits = __reduce_or_sync(0xFFFFFFFFu, bits);
         if (lane == 0 && bits) atomicOr(&s_flags[it & 1], bits);
         __syncthreads();
         const unsigned tf = s_flags[it & 1];
         if (tid == 32) s_flags[(it + 1) & 1] = 0;
-        if (!k.dense && tid < 32) schedule_around(k, tile, t, nxt, lane, (tf & 1u) || ((tf & 2u) && lane == 13));
+        unsigned wbase = 0, total = 0;
+        for (int w2 = 0; w2 < kThreads / 32; ++w2) {
+            const unsigned v = s_wtot[w2];
+            wbase += w2 < warp ? v : 0u;
+            total += v;
+        }
+        for (unsigned j = 0, pos = nbuf + wbase + incl - ncand; j < ncand; ++j) s_cand[pos + j] = cand[j];
+        nbuf += total;
+        if (tid == 0) {
+            if (tf) {
+                s_sched_tile[nsched] = tile;
+                s_sched_flag[nsched] = (uint8_t)tf;
+            }
+        }
+        if (tf) ++nsched;
+        if (nsched == kMaxDeferred) flush_schedule();
+        if (nbuf > kCandBuf - kTileCells) flush_cands();
     }
-    const unsigned warp = tid >> 5;
+    if (__syncthreads_or(nsched > 0)) flush_schedule();
+    if (nbuf) flush_cands();
+
     const unsigned a = __reduce_add_sync(0xFFFFFFFFu, my_active);
     const unsigned c = __reduce_add_sync(0xFFFFFFFFu, my_changed);
     if (lane == 0) {
@@ -544,11 +630,12 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
 // ------------------------------------------------------------------------------------------
 // Rules, candidate pass: resolves the listed AIR cells (gatherLavaCandidates / vote / solidus,
 // updateLava's AIR branch, LavaCA.hpp:1121-1134), writes the ones that gain LAVA into the next
-// buffer, lists their type change, schedules their tiles' neighbourhoods, and finishes the step in
-// its last block (finishStep, LavaCA.hpp:1206-1229).
+// buffer, lists their type change, schedules their tiles' neighbourhoods, and the last block
+// finishes the step (finishStep, LavaCA.hpp:1206-1229).
 // ------------------------------------------------------------------------------------------
-__global__ __launch_bounds__(kThreads) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
-    __shared__ unsigned long long s_red[kThreads / 32];
+constexpr int kCandThreads = 128;
+__global__ __launch_bounds__(kCandThreads) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
+    __shared__ unsigned long long s_red[kCandThreads / 32];
     __shared__ bool s_last;
     CaCtrl* ctrl = k.ctrl;
     if (ctrl->stop) return;
@@ -563,9 +650,9 @@ __global__ __launch_bounds__(kThreads) void ca_cand_kernel(const __grid_constant
     const unsigned n = ctrl->cand_count;
     const int lane = threadIdx.x & 31;
     unsigned born = 0;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t stride = (uint64_t)gridDim.x * kCandThreads;
     // warp-uniform loop (the appends below use full-warp collectives)
-    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += stride) {
+    for (uint64_t base = blockIdx.x * (uint64_t)kCandThreads; base < n; base += stride) {
         const uint64_t j = base + threadIdx.x;
         bool gained = false;
         uint32_t gi = 0, tile = 0;
@@ -592,15 +679,13 @@ __global__ __launch_bounds__(kThreads) void ca_cand_kernel(const __grid_constant
         }
         if (!k.classic && __any_sync(0xFFFFFFFFu, gained))
             warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, gained ? 1u : 0u, &gi);
-        if (!k.dense) {
-            // each lane that gained lava has its tile's neighbourhood scheduled by the whole warp
-            unsigned todo = __ballot_sync(0xFFFFFFFFu, gained);
-            while (todo) {
-                const int src = __ffs(todo) - 1;
-                todo &= todo - 1;
-                const uint32_t tl = __shfl_sync(0xFFFFFFFFu, tile, src);
-                schedule_around(k, tl, t, nxt, lane, true);
-            }
+        // the tiles that gained lava have their neighbourhoods scheduled by the whole warp, once each
+        unsigned todo = __ballot_sync(0xFFFFFFFFu, gained);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            const uint32_t tl = __shfl_sync(0xFFFFFFFFu, tile, src);
+            todo &= ~__ballot_sync(0xFFFFFFFFu, gained && tile == tl);
+            schedule_around(k, tl, t, nxt, lane, true, true);
         }
     }
     const unsigned b = __reduce_add_sync(0xFFFFFFFFu, born);
@@ -608,7 +693,7 @@ __global__ __launch_bounds__(kThreads) void ca_cand_kernel(const __grid_constant
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long sb = 0;
-        for (int wv = 0; wv < kThreads / 32; ++wv) sb += s_red[wv];
+        for (int wv = 0; wv < kCandThreads / 32; ++wv) sb += s_red[wv];
         if (sb) {
             atomicAdd(&ctrl->acc_active, sb);
             atomicAdd(&ctrl->acc_changed, sb);
@@ -703,7 +788,7 @@ __global__ void ca_init_schedule_kernel(const __grid_constant__ CaKernelArgs k, 
                             continue;
                         process = (k.tile_flags[xx + (uint64_t)g.tiles_x * (yy + (uint64_t)g.tiles_y * zz)] & 1u) != 0;
                     }
-            if (process) k.tile_mark[tile] = t0 + 1;
+            if (process) k.tile_mark[cur][tile] = 2u * (t0 + 1u) + 1u;
         }
         const unsigned ballot = __ballot_sync(0xFFFFFFFFu, process);
         const unsigned lane = threadIdx.x & 31;
@@ -792,17 +877,18 @@ CaKernelArgs make_args(const vca_ca* h) {
         k.tile_list[b] = h->tile_list[b];
     }
     k.tile_flags = h->tile_flags;
-    k.tile_mark = h->tile_mark;
+    k.tile_mark[0] = h->tile_mark[0];
+    k.tile_mark[1] = h->tile_mark[1];
+    k.desc = h->desc_plane;
     k.drop = h->drop_plane;
     k.chg_list[0] = h->chg_list[0];
     k.chg_list[1] = h->chg_list[1];
     k.chg_cap = h->chg_cap;
     k.cand_list = h->cand_list;
-    k.cand_cap = h->cand_cap;
     k.spill = h->has_terrain ? h->spill : nullptr;
     k.vents = h->vents;
     k.vent_slots = h->vent_slots;
-    k.tables = h->tables;
+    k.tables = h->tables_host;
     k.ctrl = h->ctrl;
     k.hist_active = h->hist_active;
     k.hist_changed = h->hist_changed;
@@ -818,6 +904,11 @@ vca_status check(const vca_ca* h) {
     return VCA_OK;
 }
 
+void drop_graph(vca_ca* h) {
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+}
+
 // Pull the control block to the host mirror.
 vca_status sync_ctrl(vca_ca* h) {
     VCA_CUDA(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(CaCtrl), cudaMemcpyDeviceToHost, h->stream));
@@ -830,6 +921,7 @@ vca_status sync_ctrl(vca_ca* h) {
 // Totals and initial stop state of the current buffer, the first tile list, and a copy of the
 // current buffer into the other one (both buffers equal: the ACTIVE schedule relies on it).
 vca_status init_state(vca_ca* h, int steps_done) {
+    drop_graph(h);  // the arguments (vents, spill) may have changed
     const int cur = steps_done & 1, oth = cur ^ 1;
     const size_t n = h->plane_cells;
     VCA_CUDA(cudaMemcpyAsync(h->type[oth], h->type[cur], n, cudaMemcpyDeviceToDevice, h->stream));
@@ -837,7 +929,8 @@ vca_status init_state(vca_ca* h, int steps_done) {
     VCA_CUDA(cudaMemcpyAsync(h->temp[oth], h->temp[cur], n * 4, cudaMemcpyDeviceToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->solid[oth], h->solid[cur], n * 2, cudaMemcpyDeviceToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->arrival[oth], h->arrival[cur], n * 2, cudaMemcpyDeviceToDevice, h->stream));
-    VCA_CUDA(cudaMemsetAsync(h->tile_mark, 0, h->ntiles * 4, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->tile_mark[0], 0, h->ntiles * 4, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->tile_mark[1], 0, h->ntiles * 4, h->stream));
     CaCtrl c;
     std::memset(&c, 0, sizeof(c));
     c.steps = (uint32_t)steps_done;
@@ -851,7 +944,7 @@ vca_status init_state(vca_ca* h, int steps_done) {
     VCA_CUDA(cudaGetLastError());
     ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 1);
     VCA_CUDA(cudaGetLastError());
-    if (!k.dense) {
+    {
         const int sb = (int)std::min<uint64_t>((h->ntiles + 255) / 256, 4096);
         ca_init_schedule_kernel<<<sb, 256, 0, h->stream>>>(k, (uint32_t)steps_done);
         VCA_CUDA(cudaGetLastError());
@@ -876,6 +969,56 @@ vca_status init_state(vca_ca* h, int steps_done) {
     return VCA_OK;
 }
 
+constexpr int kGraphSteps = 16;  // steps captured in one CUDA graph
+
+// The launches of kGraphSteps steps, captured once per state set-up (the kernel arguments only
+// change with the terrain, the vents or the state).  Launches after the stop exit at once.
+vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
+    if (h->graph_exec) return VCA_OK;
+    VCA_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < kGraphSteps; ++s) {
+        ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
+        ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
+        ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t e2 = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+        h->graph_exec = nullptr;
+        return cuda_fail(e2, "cudaGraphInstantiate");
+    }
+    return VCA_OK;
+}
+
+// Whole-run path: graphs of kGraphSteps steps; the stop test of graph i is read while graph i+1 runs.
+vca_status run_graphs(vca_ca* h, const CaKernelArgs& k) {
+    if (vca_status s = ensure_graph(h, k)) return s;
+    VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
+    int pending = -1;
+    for (int launched = 0;; ++launched) {
+        const int slot = launched & 1;
+        VCA_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
+        VCA_CUDA(cudaMemcpyAsync(&h->ctrl_ring[slot], h->ctrl, sizeof(CaCtrl), cudaMemcpyDeviceToHost, h->stream));
+        VCA_CUDA(cudaEventRecord(h->ring_ev[slot], h->stream));
+        h->launches += 3 * kGraphSteps;
+        if (pending >= 0) {
+            VCA_CUDA(cudaEventSynchronize(h->ring_ev[pending]));
+            if (h->ctrl_ring[pending].stop != VCA_STOP_RUNNING) break;
+        }
+        pending = slot;
+        if (launched > 65536 / kGraphSteps + 4) break;  // max_steps <= 65535: cannot be reached
+    }
+    VCA_CUDA(cudaEventRecord(h->ev_b, h->stream));
+    VCA_CUDA(cudaEventSynchronize(h->ev_b));
+    float ms = 0.f;
+    VCA_CUDA(cudaEventElapsedTime(&ms, h->ev_a, h->ev_b));
+    h->total_ms += ms;
+    return sync_ctrl(h);
+}
+
 vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
     if (!h->seeded) {
         set_error("vca_ca: place_seeds or set_state must come before stepping");
@@ -883,6 +1026,7 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
     }
     if (h->stop != VCA_STOP_RUNNING) return VCA_OK;
     const CaKernelArgs k = make_args(h);
+    if (until_stop && !h->profile_kernels) return run_graphs(h, k);
     VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
     int chunk = 4;
     int done = 0;
@@ -908,7 +1052,7 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
             } else {
                 ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
             }
-            ca_cand_kernel<<<h->cand_blocks, kThreads, 0, h->stream>>>(k);
+            ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
         }
         VCA_CUDA(cudaGetLastError());
         h->launches += (uint64_t)n * 3;
@@ -947,20 +1091,25 @@ void free_all(vca_ca* h) {
         cudaFree(h->tile_list[b]);
     }
     cudaFree(h->tile_flags);
-    cudaFree(h->tile_mark);
+    cudaFree(h->tile_mark[0]);
+    cudaFree(h->tile_mark[1]);
+    cudaFree(h->desc_plane);
     cudaFree(h->drop_plane);
     cudaFree(h->chg_list[0]);
     cudaFree(h->chg_list[1]);
     cudaFree(h->cand_list);
     cudaFree(h->spill);
     cudaFree(h->vents);
-    cudaFree(h->tables);
     cudaFree(h->ctrl);
     cudaFree(h->hist_active);
     cudaFree(h->hist_changed);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
+    for (cudaEvent_t e : h->ring_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->ctrl_ring) cudaFreeHost(h->ctrl_ring);
+    drop_graph(h);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -1106,14 +1255,14 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
         ALLOC(h->tile_list[b], h->ntiles * 4);
     }
     ALLOC(h->tile_flags, h->ntiles * 4);
-    ALLOC(h->tile_mark, h->ntiles * 4);
+    ALLOC(h->tile_mark[0], h->ntiles * 4);
+    ALLOC(h->tile_mark[1], h->ntiles * 4);
+    ALLOC(h->desc_plane, n);
     ALLOC(h->drop_plane, n);
     h->chg_cap = (uint32_t)std::min<uint64_t>((uint64_t)nx * ny * nz, 1u << 22);
     ALLOC(h->chg_list[0], sizeof(uint32_t) * (size_t)h->chg_cap);
     ALLOC(h->chg_list[1], sizeof(uint32_t) * (size_t)h->chg_cap);
-    h->cand_cap = (uint32_t)((uint64_t)nx * ny * nz);
-    ALLOC(h->cand_list, sizeof(uint32_t) * (size_t)h->cand_cap);
-    ALLOC(h->tables, sizeof(CaTables));
+    ALLOC(h->cand_list, sizeof(uint32_t) * (size_t)h->ntiles * kTileCells);  // never overflows
     ALLOC(h->ctrl, sizeof(CaCtrl));
     ALLOC(h->hist_active, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
     ALLOC(h->hist_changed, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
@@ -1129,21 +1278,24 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
             return fail(cuda_fail(e, "cudaMemsetAsync"));
     }
     if ((e = cudaMemsetAsync(h->drop_plane, 0xFF, n, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->tile_mark, 0, h->ntiles * 4, h->stream)) != cudaSuccess)
+        (e = cudaMemsetAsync(h->desc_plane, 0xFF, n, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->tile_mark[0], 0, h->ntiles * 4, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->tile_mark[1], 0, h->ntiles * 4, h->stream)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaMemsetAsync"));
     if (g.P > nx) {
         ca_pad_kernel<<<256, 256, 0, h->stream>>>(h->type[0], h->type[1], nx, g.P, (int64_t)ny * nz);
         if ((e = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, "ca_pad_kernel"));
     }
-    e = cudaMemcpyAsync(h->tables, &h->tables_host, sizeof(CaTables), cudaMemcpyHostToDevice, h->stream);
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemcpyAsync tables"));
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ca_rules_kernel, kThreads, 0);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
     h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)prop.multiProcessorCount * std::max(1, per_sm));
-    h->cand_blocks = prop.multiProcessorCount * 2;
-    if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess)
+    h->cand_blocks = prop.multiProcessorCount * 8;
+    if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->ring_ev[0], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->ring_ev[1], cudaEventDisableTiming)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaEventCreate"));
+    if ((e = cudaMallocHost(&h->ctrl_ring, 2 * sizeof(CaCtrl))) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
     const char* prof = std::getenv("VCA_PROFILE_KERNELS");
     h->profile_kernels = prof != nullptr && prof[0] == '1';
     vca_vent none{0, 0, 0, 0};
@@ -1187,6 +1339,7 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
     cudaFree(dh);
     h->has_terrain = true;
     h->launches += 1;
+    drop_graph(h);
     return VCA_OK;
 }
 

@@ -357,6 +357,7 @@ struct vca_mc {
     uint64_t launches = 0;
     int profile_kernels = 0;
     std::vector<cudaEvent_t> prof_events;
+    cudaGraphExec_t graph_exec = nullptr;  // the colour launches of one sweep (rebuilt by initialize)
 };
 
 namespace {
@@ -421,7 +422,44 @@ void mc_free(vca_mc* h) {
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// The colour passes of one MCS, launched on h->stream.
+void launch_sweep(vca_mc* h, const McArgs& a) {
+    const bool random_nb = h->nb_host.variants > 1;
+    for (int c = 0; c < h->colors; ++c) {
+        const uint64_t b = h->color_off[c], e = h->color_off[c + 1];
+        const uint64_t cnt = e - b;
+        const int grid = grid_for(cnt, h->sms);
+        const uint32_t* list = h->list + b;
+        const float* mob = h->mobility_on ? h->list_mob + b : nullptr;
+        const int last = c == h->colors - 1;
+        if (h->mobility_on) {
+            if (random_nb) mc_color_kernel<true, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+            else mc_color_kernel<true, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+        } else {
+            if (random_nb) mc_color_kernel<false, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+            else mc_color_kernel<false, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+        }
+    }
+}
+
+vca_status ensure_sweep_graph(vca_mc* h, const McArgs& a) {
+    if (h->graph_exec) return VCA_OK;
+    VCA_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    launch_sweep(h, a);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t e2 = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+        h->graph_exec = nullptr;
+        return cuda_fail(e2, "cudaGraphInstantiate");
+    }
+    return VCA_OK;
 }
 
 }  // namespace
@@ -685,6 +723,8 @@ vca_status vca_mc_initialize(vca_mc* h) {
     cudaFree(all);
     VCA_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream));
     VCA_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
     h->initialized = true;
     return VCA_OK;
 }
@@ -702,6 +742,20 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
     VCA_CUDA(cudaSetDevice(h->device));
     McArgs a = mc_args(h);
     VCA_CUDA(cudaMemsetAsync(&h->ctrl->sweep_accepted, 0, 8, h->stream));
+    if (!h->profile_kernels) {
+        if (vca_status s = ensure_sweep_graph(h, a)) return s;
+        VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
+        for (int s = 0; s < count; ++s) VCA_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
+        h->launches += (uint64_t)count * (uint64_t)h->colors;
+        VCA_CUDA(cudaEventRecord(h->ev_b, h->stream));
+        VCA_CUDA(cudaEventSynchronize(h->ev_b));
+        float ms = 0.f;
+        VCA_CUDA(cudaEventElapsedTime(&ms, h->ev_a, h->ev_b));
+        h->total_ms += ms;
+        if (vca_status s_ = mc_sync(h)) return s_;
+        if (accepted) *accepted = h->ctrl_host->sweep_accepted;
+        return VCA_OK;
+    }
     VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
     const bool random_nb = h->nb_host.variants > 1;
     size_t ev_used = 0;

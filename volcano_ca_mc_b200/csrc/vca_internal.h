@@ -82,14 +82,14 @@ struct CaKernelArgs {
     uint32_t* chg_list[2];    // globalIndex of cells whose type changed (step t writes [(t+1) & 1])
     uint32_t chg_cap;         // capacity of each change list; more changes force a full rescan
     uint32_t* cand_list;      // globalIndex of AIR cells with LAVA within one cell (this step)
-    uint32_t cand_cap;        // = cells of the grid: the list can never overflow
     const int32_t* spill;     // nx*ny or nullptr
     const int4* vents;        // (x, y, z, -) per flowId
     int vent_slots;
-    const CaTables* tables;
+    CaTables tables;          // by value: read from the kernel parameter (constant) bank
     CaCtrl* ctrl;
     uint32_t* tile_flags;     // set-up only: bit 0 = LAVA in the tile
-    uint32_t* tile_mark;      // (step + 1) the tile was last scheduled for
+    uint32_t* tile_mark[2];   // 2 (s + 1) + lava bit of the step s the tile is scheduled for, per parity
+    int8_t* desc;             // D(n) of LAVA cells of scheduled tiles (computeDescent, LavaCA.hpp:551-566)
     uint32_t* tile_list[2];   // tiles of step t are tile_list[t & 1]
     unsigned long long* hist_active;
     unsigned long long* hist_changed;
@@ -128,16 +128,15 @@ struct vca_ca {
     uint32_t* chg_list[2] = {nullptr, nullptr};
     uint32_t chg_cap = 0;
     uint32_t* cand_list = nullptr;
-    uint32_t cand_cap = 0;
     int cand_blocks = 0;      // grid of the candidate pass
     int32_t* spill = nullptr;
     int4* vents = nullptr;
     int vent_slots = 0;
-    vca::CaTables* tables = nullptr;
     vca::CaCtrl* ctrl = nullptr;
     vca::CaCtrl* ctrl_host = nullptr;   // pinned mirror
     uint32_t* tile_flags = nullptr;
-    uint32_t* tile_mark = nullptr;
+    uint32_t* tile_mark[2] = {nullptr, nullptr};
+    int8_t* desc_plane = nullptr;
     uint32_t* tile_list[2] = {nullptr, nullptr};
     unsigned long long* hist_active = nullptr;
     unsigned long long* hist_changed = nullptr;
@@ -154,4 +153,7 @@ struct vca_ca {
     uint64_t launches = 0;    // kernel launches issued
     int profile_kernels = 0;  // bracket each rules launch with events (set by VCA_PROFILE_KERNELS=1)
     std::vector<cudaEvent_t> prof_events;
+    cudaGraphExec_t graph_exec = nullptr;   // kGraphSteps steps of launches (rebuilt after set-up calls)
+    vca::CaCtrl* ctrl_ring = nullptr;       // pinned: two in-flight copies of the control block
+    cudaEvent_t ring_ev[2] = {nullptr, nullptr};
 };
