@@ -1,0 +1,264 @@
+"""Generates the golden fixtures under tests/golden/ by running the reference engine.
+
+Run in a checkout that has the reference sources (the reference engine is built by
+``make -C oracle ref`` into ``oracle/_ref/engine``):
+
+    python tests/golden/make_golden.py
+
+For every case in CASES it writes ``cases/<name>.json`` (the config, in the reference's schema),
+runs ``engine --config cases/<name>.json --out <tmp>`` and stores under ``<name>/``:
+
+* ``expect.json``: the SHA-256 of every result file, stats.json without its "parallel" section
+  (thread counts of the machine that ran it), the text of mc_stats.csv, the section and info keys
+  of times.json, the exit code;
+* ``initial.npz`` (CA cases): the state after terrain and vents, i.e. the reference's
+  ``snapshots/step_000000.bin``, which the CPU oracle tests start from.
+
+The configs are small (seconds of reference CPU time) and the fixtures a few hundred KB in all.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import math
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from oracle import oracle as O  # noqa: E402
+
+CASES_DIR = os.path.join(HERE, "cases")
+
+COOL_FAST = {"coolingAmbient": 2.0, "coolingLateral": 4.0, "coolingFall": 2.0, "solidusTemp": 800}
+
+CASES: dict[str, dict] = {
+    # 2D cross-section (x-z), Moore, absorbing frame, two crater vents, MC with cooling mobility, kT > 0
+    "lava2d_moore": {
+        "space": {"nx": 128, "ny": 1, "nz": 64}, "boundary": "absorbing", "neighborhood": "moore", "rngSeed": 7,
+        "terrain": {"type": "cone", "peakHeight": 40, "baseRadius": 60, "craterRadius": 8, "craterDepth": 5,
+                    "noise": 0.05, "file": None},
+        "vents": {"count": 2, "placement": "crater", "eruptionSteps": 120, "eruptTemp": 1200},
+        "ca": {"mode": "lava", "maxSteps": 3000, **COOL_FAST, "ponding": True},
+        "mc": {"enabled": True, "domain": "basalt", "Q": 32, "mcs": 30, "J": 1.0, "kT": 0.6,
+               "mobilityFromCooling": True, "mobilityMin": 0.05, "statsEvery": 5, "update": "checkerboard"},
+        "output": {"format": "both", "snapshotsEvery": 0},
+    },
+    # 2D hexagonal neighbourhood, periodic in x, MC at kT = 0 without mobility
+    "lava2d_hex_periodic": {
+        "space": {"nx": 96, "ny": 1, "nz": 48}, "boundary": "periodic", "neighborhood": "hexagonal", "rngSeed": 11,
+        "terrain": {"type": "cone", "peakHeight": 30, "baseRadius": 44, "craterRadius": 5, "craterDepth": 3,
+                    "noise": 0.08, "file": None},
+        "vents": {"count": 1, "placement": "crater", "eruptionSteps": 80, "eruptTemp": 1150},
+        "ca": {"mode": "lava", "maxSteps": 3000, **COOL_FAST, "ponding": True},
+        "mc": {"enabled": True, "domain": "basalt", "Q": 20, "mcs": 20, "J": 1.0, "kT": 0.0,
+               "mobilityFromCooling": False, "statsEvery": 4, "update": "checkerboard"},
+        "output": {"format": "bin", "snapshotsEvery": 0},
+    },
+    # 3D Moore, absorbing, three randomly placed vents on the flanks
+    "lava3d_moore_random": {
+        "space": {"nx": 40, "ny": 36, "nz": 24}, "boundary": "absorbing", "neighborhood": "moore", "rngSeed": 5,
+        "terrain": {"type": "cone", "peakHeight": 16, "baseRadius": 22, "craterRadius": 3, "craterDepth": 2,
+                    "noise": 0.1, "file": None},
+        "vents": {"count": 3, "placement": "random", "eruptionSteps": 60, "eruptTemp": 1200},
+        "ca": {"mode": "lava", "maxSteps": 3000, **COOL_FAST, "ponding": True},
+        "mc": {"enabled": True, "domain": "basalt", "Q": 64, "mcs": 20, "J": 1.0, "kT": 0.5,
+               "mobilityFromCooling": True, "mobilityMin": 0.1, "statsEvery": 5, "update": "checkerboard"},
+        "output": {"format": "both", "snapshotsEvery": 0},
+    },
+    # 3D pentagonal, periodic in x and y, vents at given columns, no ponding
+    "lava3d_pent_periodic": {
+        "space": {"nx": 36, "ny": 28, "nz": 20}, "boundary": "periodic", "neighborhood": "pentagonal", "rngSeed": 9,
+        "terrain": {"type": "cone", "peakHeight": 14, "baseRadius": 20, "craterRadius": 3, "craterDepth": 2,
+                    "noise": 0.05, "file": None},
+        "vents": {"count": 2, "placement": "positions", "positions": [[18, 14], [10, 8]], "eruptionSteps": 50,
+                  "eruptTemp": 1200},
+        "ca": {"mode": "lava", "maxSteps": 3000, **COOL_FAST, "ponding": False},
+        "mc": {"enabled": True, "domain": "basalt", "Q": 16, "mcs": 15, "J": 1.0, "kT": 0.3,
+               "mobilityFromCooling": True, "mobilityMin": 0.05, "statsEvery": 3, "update": "checkerboard"},
+        "output": {"format": "bin", "snapshotsEvery": 0},
+    },
+    # 3D von Neumann, periodic with odd nx and ny (three checkerboard colour classes per axis), stopped
+    # by ca.maxSteps
+    "lava3d_vn_odd": {
+        "space": {"nx": 33, "ny": 31, "nz": 20}, "boundary": "periodic", "neighborhood": "von_neumann",
+        "rngSeed": 13,
+        "terrain": {"type": "cone", "peakHeight": 14, "baseRadius": 18, "craterRadius": 3, "craterDepth": 2,
+                    "noise": 0.05, "file": None},
+        "vents": {"count": 2, "placement": "crater", "eruptionSteps": 200, "eruptTemp": 1200},
+        "ca": {"mode": "lava", "maxSteps": 90, "coolingAmbient": 0.3, "coolingLateral": 1.5, "coolingFall": 0.1,
+               "solidusTemp": 800, "ponding": True},
+        "mc": {"enabled": True, "domain": "basalt", "Q": 8, "mcs": 12, "J": 1.0, "kT": 1.0,
+               "mobilityFromCooling": True, "mobilityMin": 0.05, "statsEvery": 4, "update": "checkerboard"},
+        "output": {"format": "bin", "snapshotsEvery": 0},
+    },
+    # terrain from a CSV heightmap, step snapshots, text output, CA only
+    "heightmap_file": {
+        "space": {"nx": 48, "ny": 40, "nz": 24}, "boundary": "absorbing", "neighborhood": "moore", "rngSeed": 21,
+        "terrain": {"type": "file", "file": "heightmaps/ridge_48x40.csv"},
+        "vents": {"count": 1, "placement": "positions", "positions": [[14, 20]], "eruptionSteps": 70,
+                  "eruptTemp": 1200},
+        "ca": {"mode": "lava", "maxSteps": 3000, **COOL_FAST, "ponding": True},
+        "mc": {"enabled": False},
+        "output": {"format": "txt", "snapshotsEvery": 25},
+    },
+    # classic grain growth in 3D (no terrain), Moore, periodic
+    "classic3d_moore": {
+        "space": {"nx": 24, "ny": 24, "nz": 24}, "boundary": "periodic", "neighborhood": "moore", "rngSeed": 3,
+        "vents": {"count": 12}, "ca": {"mode": "classic", "maxSteps": 65535}, "mc": {"enabled": False},
+        "output": {"format": "bin", "snapshotsEvery": 0},
+    },
+    # classic grain growth in 2D (x-y plane), von Neumann, absorbing
+    "classic2d_vn": {
+        "space": {"nx": 64, "ny": 48, "nz": 1}, "boundary": "absorbing", "neighborhood": "von_neumann",
+        "rngSeed": 17, "vents": {"count": 20}, "ca": {"mode": "classic", "maxSteps": 65535},
+        "mc": {"enabled": False}, "output": {"format": "both", "snapshotsEvery": 0},
+    },
+    # Potts MC on the whole 3D space (no CA), periodic, kT > 0, MC snapshots
+    "mc_full_3d": {
+        "space": {"nx": 24, "ny": 20, "nz": 16}, "boundary": "periodic", "neighborhood": "moore", "rngSeed": 42,
+        "mc": {"enabled": True, "domain": "full", "Q": 16, "mcs": 10, "J": 1.0, "kT": 0.5,
+               "mobilityFromCooling": False, "statsEvery": 2, "snapshotsEvery": 5, "update": "checkerboard"},
+        "output": {"format": "both"},
+    },
+    # Potts MC on the whole 2D space, hexagonal, absorbing, kT = 0
+    "mc_full_2d_hex": {
+        "space": {"nx": 64, "ny": 1, "nz": 40}, "boundary": "absorbing", "neighborhood": "hexagonal", "rngSeed": 8,
+        "mc": {"enabled": True, "domain": "full", "Q": 10, "mcs": 8, "J": 1.0, "kT": 0.0,
+               "mobilityFromCooling": False, "statsEvery": 2, "update": "checkerboard"},
+        "output": {"format": "bin"},
+    },
+}
+
+# --mc-from runs: MC on the CA result of another case, read back from its result folder.
+MC_FROM: dict[str, tuple[str, dict]] = {
+    "mcfrom_lava2d": ("lava2d_moore", {
+        "boundary": "absorbing", "neighborhood": "moore", "rngSeed": 7,
+        "mc": {"enabled": True, "domain": "basalt", "Q": 24, "mcs": 10, "J": 1.0, "kT": 0.4,
+               "mobilityFromCooling": True, "mobilityMin": 0.2, "statsEvery": 5, "update": "checkerboard"},
+        "output": {"format": "bin"},
+    }),
+}
+
+RESULT_FILES = ("ca_result.bin", "ca_result.txt", "mc_result.bin", "mc_result.txt", "mc_stats.csv",
+                "config_used.json")
+
+
+def ridge_heightmap(nx: int, ny: int) -> str:
+    """A ridge along y with a bowl on its west flank, heights in cells (plain arithmetic, no noise)."""
+    rows = ["# ridge with a bowl, heights in cells"]
+    for y in range(ny):
+        vals = []
+        for x in range(nx):
+            ridge = 16.0 * math.exp(-((x - 30) / 9.0) ** 2)
+            bowl = 4.0 * math.exp(-(((x - 14) / 5.0) ** 2 + ((y - 20) / 6.0) ** 2))
+            h = max(0.0, 2.0 + ridge + 0.05 * y - bowl)
+            vals.append(f"{h:.2f}")
+        rows.append(",".join(vals))
+    return "\n".join(rows) + "\n"
+
+
+def sha256(path: str) -> str:
+    with open(path, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()
+
+
+def write_case(name: str, cfg: dict) -> str:
+    path = os.path.join(CASES_DIR, f"{name}.json")
+    with open(path, "w") as f:
+        json.dump(cfg, f, indent=2)
+        f.write("\n")
+    return path
+
+
+def expectation(out: str, rc: int) -> dict:
+    exp: dict = {"exit": rc, "files": {}, "snapshots": {}}
+    for name in RESULT_FILES:
+        p = os.path.join(out, name)
+        if os.path.exists(p):
+            exp["files"][name] = sha256(p)
+    for sub in ("snapshots", "mc_snapshots"):
+        d = os.path.join(out, sub)
+        if os.path.isdir(d):
+            for fn in sorted(os.listdir(d)):
+                exp["snapshots"][f"{sub}/{fn}"] = sha256(os.path.join(d, fn))
+    with open(os.path.join(out, "stats.json")) as f:
+        stats = json.load(f)
+    stats.pop("parallel", None)
+    exp["stats"] = stats
+    csv = os.path.join(out, "mc_stats.csv")
+    if os.path.exists(csv):
+        with open(csv) as f:
+            exp["mc_stats_csv"] = f.read()
+    with open(os.path.join(out, "times.json")) as f:
+        exp["times_keys"] = list(json.load(f).keys())
+    return exp
+
+
+def run_ref(args: list[str]) -> int:
+    r = subprocess.run([O.REF_ENGINE, *args], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stderr)
+    return r.returncode
+
+
+def save_initial(path: str, s: "O.CaState") -> None:
+    np.savez_compressed(path, dims=np.array([s.nx, s.ny, s.nz], np.int32), type=s.type, flow=s.flow,
+                        temp=s.temp, solid=s.solid, arrival=s.arrival)
+
+
+def main() -> None:
+    if not os.path.exists(O.REF_ENGINE):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
+    os.makedirs(os.path.join(CASES_DIR, "heightmaps"), exist_ok=True)
+    with open(os.path.join(CASES_DIR, "heightmaps", "ridge_48x40.csv"), "w") as f:
+        f.write(ridge_heightmap(48, 40))
+    tmp = tempfile.mkdtemp(prefix="vca_golden_")
+    try:
+        outs = {}
+        for name, cfg in CASES.items():
+            path = write_case(name, cfg)
+            out = os.path.join(tmp, name)
+            rc = run_ref(["--config", path, "--out", out])
+            assert rc == 0, name
+            outs[name] = out
+            dst = os.path.join(HERE, name)
+            os.makedirs(dst, exist_ok=True)
+            with open(os.path.join(dst, "expect.json"), "w") as f:
+                json.dump(expectation(out, rc), f, indent=1)
+                f.write("\n")
+            if not (cfg.get("mc", {}).get("enabled") and cfg["mc"].get("domain") == "full"):
+                init = os.path.join(tmp, name + "_init")
+                rc = run_ref(["--config", path, "--out", init, "--set", "output.snapshotsEvery=65535",
+                              "--set", "mc.enabled=false", "--set", "output.format=bin"])
+                assert rc == 0, name
+                save_initial(os.path.join(dst, "initial.npz"),
+                             O.read_ca_bin(os.path.join(init, "snapshots", "step_000000.bin")))
+            print(name, "ok")
+        for name, (src, cfg) in MC_FROM.items():
+            path = write_case(name, cfg)
+            out = os.path.join(tmp, name)
+            rc = run_ref(["--mc-from", outs[src], "--config", path, "--out", out])
+            assert rc == 0, name
+            dst = os.path.join(HERE, name)
+            os.makedirs(dst, exist_ok=True)
+            exp = expectation(out, rc)
+            exp["mc_from"] = src
+            exp["stats"].pop("source", None)  # holds the absolute folder path of the run
+            with open(os.path.join(dst, "expect.json"), "w") as f:
+                json.dump(exp, f, indent=1)
+                f.write("\n")
+            print(name, "ok")
+    finally:
+        shutil.rmtree(tmp)
+
+
+if __name__ == "__main__":
+    main()
