@@ -196,6 +196,22 @@ vca_status vca_mc_set_spins(vca_mc* mc, const int32_t* spins);
 vca_status vca_mc_timing(vca_mc* mc, double* total_ms, double* color_kernel_ms, uint64_t* color_launches);
 void vca_mc_destroy(vca_mc* mc);
 
+/* Potts energy (the quantity of vca_mc_energy) of an nx*ny*nz int32 spin grid that is already in
+ * the caller's device memory, written to the caller's device double *energy on the given
+ * cudaStream_t (NULL: the legacy default stream).  No counterpart in the reference: it exists for
+ * callers that own all device memory and cannot let a library allocate -- a process whose memory
+ * pool has reserved the device, or a pipeline that must not take the device-wide synchronisation
+ * of cudaMalloc/cudaFree between its launches.  It allocates nothing: its scratch (per-block sums
+ * and a counter) is a fixed static device array of 512 KiB + 256 B, so grids above 2^28 cells are
+ * rejected with VCA_ERR_ARG.  Spins: 0 outside the domain, 1..Q inside; neighborhood, boundary,
+ * domain_full and seed as in vca_mc_desc; mcs = sweeps done (the neighbourhood variant of
+ * pentagonal/hexagonal cells at that MCS).  Both pointers must be device memory of the current
+ * device.  The first call on each device looks up the scratch address (make it before any stream
+ * capture).  The call returns once the work is queued.  Calls that overlap on one device race on
+ * the shared scratch: order them (one stream, or events). */
+vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, int neighborhood, int boundary,
+                                 int domain_full, uint64_t seed, int mcs, double J, double* energy, void* stream);
+
 /* ------------------------------------------------------------------------------------------ */
 const char* vca_last_error(void);
 /* ABI version and build string ("vca <abi> sm_100a ..."). */

@@ -30,6 +30,7 @@ EXPORTS = [
     "vca_mc_create", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
     "vca_mc_energy", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
+    "vca_mc_energy_noalloc",
     "vca_last_error", "vca_version",
 ]
 
@@ -98,6 +99,7 @@ def lib() -> ctypes.CDLL:
         "vca_mc_mobility": [p, p], "vca_mc_initialize": [p], "vca_mc_sweep": [p, i32, p],
         "vca_mc_get_info": [p, p], "vca_mc_energy": [p, p], "vca_mc_crystals": [p, p],
         "vca_mc_set_spins": [p, p], "vca_mc_timing": [p, p, p, p],
+        "vca_mc_energy_noalloc": [p, i32, i32, i32, i32, i32, i32, u64, i32, f64, p, p],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -328,3 +330,14 @@ class PottsMC:
         tot, ker, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
         _check(lib().vca_mc_timing(self.h, ctypes.byref(tot), ctypes.byref(ker), ctypes.byref(n)), "vca_mc_timing")
         return tot.value, ker.value, n.value
+
+
+def mc_energy_noalloc(spins_ptr: int, nx: int, ny: int, nz: int, energy_ptr: int, *, neighborhood: str = "moore",
+                      boundary: str = "absorbing", domain_full: bool = False, seed: int = 42, mcs: int = 0,
+                      J: float = 1.0, stream: int = 0) -> None:
+    """vca_mc_energy_noalloc: queue the energy of a device spin grid (spins_ptr, nx*ny*nz int32) into
+    the device double at energy_ptr on the CUDA stream handle ``stream`` (0: legacy default stream).
+    Allocates nothing; grids above 2^28 cells raise VcaError."""
+    _check(lib().vca_mc_energy_noalloc(ctypes.c_void_p(spins_ptr), nx, ny, nz, NB[neighborhood], BC[boundary],
+                                       int(domain_full), seed, mcs, J, ctypes.c_void_p(energy_ptr),
+                                       ctypes.c_void_p(stream) if stream else None), "vca_mc_energy_noalloc")
