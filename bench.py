@@ -230,6 +230,26 @@ def cpu_baseline(w):
             "mc_attempts_per_s": st["mc"]["attempts"] / (t["mcSim"] * 1e-3)}
 
 
+def engine_cli(w):
+    """The engine command (volcano_ca_mc_b200/bin/engine) on one job of the workload, from the same
+    config file the reference engine runs; its times.json sections as the reference writes them."""
+    from volcano_ca_mc_b200 import capi
+    if not os.path.exists(capi.ENGINE_PATH):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        cfg = w.write(d)
+        out = os.path.join(d, "out")
+        r = subprocess.run([capi.ENGINE_PATH, "--config", cfg, "--out", out, "--timing-detail"], capture_output=True,
+                           text=True, timeout=900)
+        if r.returncode != 0:
+            return {"error": r.stderr.strip()[-300:]}
+        t = json.load(open(os.path.join(out, "times.json")))
+    keys = ("readConfig", "allocate", "terrain", "vents", "caSim", "save", "caStats", "mcInit", "mcSim", "mcStats",
+            "mcSave", "total")
+    return {"times_ms": {k: t[k] for k in keys if k in t}, "detail_ms": t.get("detail"), "steps": t.get("steps"),
+            "cell_updates_per_s_caSim": w.cells * int(t["steps"]) / (t["caSim"] * 1e-3)}
+
+
 def ours(args):
     import torch
     import torch.distributed as dist
@@ -296,8 +316,11 @@ def ours(args):
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
     ca_ms, mc_ms, dense_ms, e2e_ms, wall_ms = vals.tolist()
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w)
+    eng = None
+    if rank == 0 and world == 1:
+        eng = engine_cli(w)
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(w)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -331,6 +354,8 @@ def ours(args):
         "clocks": clocks,
         "wall_s_timed_loop": round(wall_ms / 1e3, 3),
     }
+    if eng is not None:
+        line["engine_cli"] = eng
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

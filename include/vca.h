@@ -131,6 +131,10 @@ vca_status vca_ca_get_spill(vca_ca* ca, int32_t* spill);
 /* Device time of the CA steps so far [ms] (CUDA events around the step launches) and the average
  * duration of one launch of the rules kernel [ms] over the last vca_ca_run / vca_ca_step calls. */
 vca_status vca_ca_timing(vca_ca* ca, double* total_ms, double* rules_kernel_ms, uint64_t* rules_launches);
+/* With VCA_PROFILE_KERNELS=1 in the environment when the handle was created, runs launch step by
+ * step with CUDA events around each kernel: the average device time [ms] of the drop-depth, rules
+ * and candidate kernels of a step, and the steps measured.  No counterpart in the reference. */
+vca_status vca_ca_kernel_times(vca_ca* ca, double* drop_ms, double* rules_ms, double* cand_ms, uint64_t* steps);
 void vca_ca_destroy(vca_ca* ca);
 
 /* ------------------------------------------------------------------------------------------

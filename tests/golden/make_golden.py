@@ -3,7 +3,8 @@
 Run in a checkout that has the reference sources (the reference engine is built by
 ``make -C oracle ref`` into ``oracle/_ref/engine``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # the small cases
+    python tests/golden/make_golden.py --large    # hashes of the full-size 1024 x 1024 x 256 workload
 
 For every case in CASES it writes ``cases/<name>.json`` (the config, in the reference's schema),
 runs ``engine --config cases/<name>.json --out <tmp>`` and stores under ``<name>/``:
@@ -214,7 +215,43 @@ def save_initial(path: str, s: "O.CaState") -> None:
                         temp=s.temp, solid=s.solid, arrival=s.arrival)
 
 
+def large(name: str = "c3") -> None:
+    """The full-size workload (volcano_ca_mc_b200.workloads, 1024 x 1024 x 256 for c3): the reference
+    engine's outputs are too large to commit, so only their hashes, the step count, the per-step
+    histories and the MC counters are kept (``<name>_large/expect.json``).  A few minutes of CPU."""
+    from volcano_ca_mc_b200 import workloads
+    w = workloads.get(name)
+    tmp = tempfile.mkdtemp(prefix="vca_golden_large_")
+    try:
+        cfg = w.write(tmp)
+        out = os.path.join(tmp, "out")
+        rc = run_ref(["--config", cfg, "--out", out, "--threads", str(os.cpu_count() or 1)])
+        assert rc == 0
+        with open(os.path.join(out, "stats.json")) as f:
+            stats = json.load(f)
+        with open(os.path.join(out, "mc_stats.csv")) as f:
+            csv_text = f.read()
+        exp = {"workload": name, "files": {n: sha256(os.path.join(out, n)) for n in ("ca_result.bin", "mc_result.bin")},
+               "steps": stats["steps"], "stopReason": stats["stopReason"], "activeCells": stats["activeCells"],
+               "changedCells": stats["changedCells"], "totalLavaVolume": stats["totalLavaVolume"],
+               "liquidLava": stats["liquidLava"],
+               "mc": {k: stats["mc"][k] for k in ("domainCells", "attempts", "accepted", "acceptedUphill", "energyStart",
+                                                  "energyEnd", "grainsStart", "grainsEnd")},
+               "mc_stats_csv": csv_text}
+        dst = os.path.join(HERE, f"{name}_large")
+        os.makedirs(dst, exist_ok=True)
+        with open(os.path.join(dst, "expect.json"), "w") as f:
+            json.dump(exp, f, indent=1)
+            f.write("\n")
+        print(name, "large ok")
+    finally:
+        shutil.rmtree(tmp)
+
+
 def main() -> None:
+    if "--large" in sys.argv:
+        large()
+        return
     if not os.path.exists(O.REF_ENGINE):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
     os.makedirs(os.path.join(CASES_DIR, "heightmaps"), exist_ok=True)

@@ -26,7 +26,7 @@ STOP_NAMES = {0: "running", 1: "no lava", 2: "no air", 3: "no change", 4: "max s
 EXPORTS = [
     "vca_ca_create", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
     "vca_ca_get_info", "vca_ca_history", "vca_ca_download", "vca_ca_set_state", "vca_ca_get_spill",
-    "vca_ca_timing", "vca_ca_destroy",
+    "vca_ca_timing", "vca_ca_kernel_times", "vca_ca_destroy",
     "vca_mc_create", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
     "vca_mc_energy", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
@@ -93,7 +93,7 @@ def lib() -> ctypes.CDLL:
         "vca_ca_step": [p, p], "vca_ca_run": [p], "vca_ca_get_info": [p, p],
         "vca_ca_history": [p, p, p, i32, p], "vca_ca_download": [p, p, p, p, p, p],
         "vca_ca_set_state": [p, p, p, p, p, p, p, p, i32, i32], "vca_ca_get_spill": [p, p],
-        "vca_ca_timing": [p, p, p, p],
+        "vca_ca_timing": [p, p, p, p], "vca_ca_kernel_times": [p, p, p, p, p],
         "vca_mc_create": [p, p], "vca_mc_set_domain": [p, p], "vca_mc_set_mobility": [p, p],
         "vca_mc_set_domain_from_ca": [p, p], "vca_mc_set_mobility_from_ca": [p, p, f64, i32],
         "vca_mc_mobility": [p, p], "vca_mc_initialize": [p], "vca_mc_sweep": [p, i32, p],
@@ -237,6 +237,13 @@ class LavaCA:
         tot, ker, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
         _check(lib().vca_ca_timing(self.h, ctypes.byref(tot), ctypes.byref(ker), ctypes.byref(n)), "vca_ca_timing")
         return tot.value, ker.value, n.value
+
+    def kernel_times(self) -> dict:
+        """Average device ms per step of each step kernel (handles created with VCA_PROFILE_KERNELS=1)."""
+        d, r, c, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
+        _check(lib().vca_ca_kernel_times(self.h, ctypes.byref(d), ctypes.byref(r), ctypes.byref(c), ctypes.byref(n)),
+               "vca_ca_kernel_times")
+        return {"drop_ms": d.value, "rules_ms": r.value, "cand_ms": c.value, "steps": n.value}
 
 
 @dataclass

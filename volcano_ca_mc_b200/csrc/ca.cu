@@ -42,8 +42,10 @@ namespace vca {
 constexpr int kThreads = 256;       // threads of a tile block: 16 per 64-cell row, 16 rows
 constexpr int kTileX = 64;
 constexpr int kMaxDrop = 16;        // LavaCA::kMaxDrop (LavaCA.hpp:1293)
-constexpr int kSmemRowBytes = 72;   // 4 pad + 64 cells + 4 pad
+constexpr int kSmemRowBytes = 96;   // 16 pad (left frame byte at 15) + 64 cells + right frame byte + pad
+constexpr int kRowOff = 16;         // first cell of a staged row (16-byte aligned for cp.async)
 constexpr int kMaxHaloRows = 36;    // (TY + 2) * (TZ + 2) for TY = TZ = 4; 18 for the 2D tiles
+constexpr int kMaxDropRows = 24;    // (TY + 2) * TZ: the drop-depth rows at the tile's own levels
 
 // ------------------------------------------------------------------------------------------
 // Addressing with the reference's frame semantics: a coordinate one step outside the interior is
@@ -110,6 +112,69 @@ struct Vote {
         const uint64_t r = hash_salt(hash_index(prefix, gidx), kSaltTieBreak);
         return tied[(int)(r % (uint64_t)k)];
     }
+    __device__ bool overflow() const { return false; }
+    __device__ void pick(uint64_t prefix, uint64_t gidx, int32_t* id, float* t) const {
+        const int w = winner(prefix, gidx);
+        *id = ids[w];
+        *t = max_temp[w];
+    }
+};
+
+// The same vote for up to 4 distinct flowIds, held in registers (every index is a compile-time
+// constant after unrolling).  A fifth distinct id sets overflow; the caller then recounts with Vote.
+struct SmallVote {
+    int n;
+    bool over;
+    int32_t ids[4];
+    int counts[4];
+    float max_temp[4];
+    __device__ void add(int32_t id, float t) {
+        bool hit = false;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            if (s < n && ids[s] == id) {
+                ++counts[s];
+                max_temp[s] = fmaxf(max_temp[s], t);
+                hit = true;
+            }
+        if (hit) return;
+        if (n == 4) {
+            over = true;
+            return;
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            if (s == n) {
+                ids[s] = id;
+                counts[s] = 1;
+                max_temp[s] = t;
+            }
+        ++n;
+    }
+    __device__ bool overflow() const { return over; }
+    // Most votes; ties: the (r % k)-th smallest tied id, r = hashRand(seed, t, idx, TieBreak).
+    __device__ void pick(uint64_t prefix, uint64_t gidx, int32_t* id, float* t) const {
+        int best = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            if (s < n) best = max(best, counts[s]);
+        int k = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) k += (s < n && counts[s] == best) ? 1 : 0;
+        int want = 0;
+        if (k > 1) want = (int)(hash_salt(hash_index(prefix, gidx), kSaltTieBreak) % (uint64_t)k);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (!(s < n && counts[s] == best)) continue;
+            int rank = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) rank += (u < n && counts[u] == best && ids[u] < ids[s]) ? 1 : 0;
+            if (rank == want) {
+                *id = ids[s];
+                *t = max_temp[s];
+            }
+        }
+    }
 };
 
 __device__ __forceinline__ void tile_origin(const CaGeom& g, uint32_t tile, int& x0, int& y0, int& z0) {
@@ -168,6 +233,49 @@ __device__ void drop_scan(const CaKernelArgs& k, const uint8_t* T, int x, int y,
     }
 }
 
+// The same closed form for the 18 cells [zc, zc + 18) above one changed cell, from one batch of
+// independent loads: the types of the window [zc - 17, zc + 18) become bit masks (bit i = cell
+// zc - 17 + i; cells below the grid floor count as solid), the run bottom w of an AIR cell is one
+// above the highest non-AIR bit below it.  A run that reaches below the window is longer than 16.
+__device__ void drop_rescan18(const CaKernelArgs& k, const uint8_t* T, int x, int y, int zc) {
+    const CaGeom& g = k.g;
+    constexpr int kWin = 2 * (kMaxDrop + 1) + 1;  // 35 cells
+    const int b = zc - (kMaxDrop + 1);
+    const int64_t col = pidx(g, x, y, 0), zs = (int64_t)g.P * g.ny;
+    const int sp = k.spill != nullptr ? __ldg(k.spill + x + (int64_t)g.nx * y) : 0;
+    uint64_t air = 0, solid = 0, lava = 0;
+#pragma unroll
+    for (int i = 0; i < kWin; ++i) {
+        const int z = b + i;
+        if (z < 0) {
+            solid |= 1ull << i;
+        } else if (z < g.nz) {
+            const int t = T[col + zs * z];
+            air |= (uint64_t)(t == kAir) << i;
+            solid |= (uint64_t)(t == kRock || t == kBasalt) << i;
+            lava |= (uint64_t)(t == kLava) << i;
+        }
+    }
+    const int hi = min(g.nz, zc + kMaxDrop + 2);
+    for (int z = zc; z < hi; ++z) {
+        const int i = z - b;
+        int dd = -1;
+        if ((air >> i) & 1ull) {
+            const uint64_t below = ~air & ((1ull << i) - 1ull);
+            if (below == 0) {
+                dd = kMaxDrop;  // i >= 17 AIR cells below z
+            } else {
+                const int j = 63 - __clzll((long long)below);  // the cell under the run bottom
+                const int kk = i - j - 1;
+                const int under = b + j;  // its z (-1: the grid floor)
+                const bool sup = ((solid >> j) & 1ull) || (((lava >> j) & 1ull) && k.spill != nullptr && under < sp);
+                dd = kk > kMaxDrop ? kMaxDrop : (sup ? kk : (kk == kMaxDrop ? kMaxDrop : -1));
+            }
+        }
+        k.drop[col + zs * z] = (int8_t)dd;
+    }
+}
+
 // Rescans the columns above last step's type changes (or every column when forced or when the
 // change list overflowed), and clears the change list this step's rules will fill.
 __global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force_full) {
@@ -196,7 +304,7 @@ __global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force
         const int x = (int)(gi - r * (uint32_t)g.nx);
         const int y = (int)(r % (uint32_t)g.ny);
         const int z = (int)(r / (uint32_t)g.ny);
-        drop_scan(k, T, x, y, z, min(g.nz, z + kMaxDrop + 2));
+        drop_rescan18(k, T, x, y, z);
     }
 }
 
@@ -210,14 +318,18 @@ __device__ __forceinline__ int type_at(const CaGeom& g, const uint8_t* T, int x,
 
 // gatherLavaCandidates + tryPonding (LavaCA.hpp:443-519) or updateClassic's vote (1176-1182), the
 // winner (CaRules.hpp:152-173) and the solidus test.  Returns true when the cell becomes LAVA.
-// The neighbour types of the cell's variant are fetched together first (independent loads); only
-// the LAVA ones are then examined, in any order (the vote does not depend on the order).
-__device__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, const float* Te, int x, int y,
-                               int z, uint64_t prefix, uint64_t gidx, int32_t* out_flow, float* out_temp) {
+// Memory rounds: the cell's own drop depth and the neighbour types of its variant are fetched
+// together (independent loads); then, for up to 8 LAVA neighbours at a time, their D(n), flowId and
+// temperature together.  The vote does not depend on the order in which sources are added.
+template <class V>
+__device__ __forceinline__ bool gather_vote(const CaKernelArgs& k, const uint8_t* T, const int32_t* F, const float* Te,
+                                            int x, int y, int z, uint64_t prefix, uint64_t gidx, V& v, int32_t* out_flow,
+                                            float* out_temp) {
     const CaGeom& g = k.g;
     const NbTable& nb = k.tables.nb;
     const int var = nb.variants == 1 ? 0 : (int)fast_mod(hash_salt(hash_index(prefix, gidx), kSaltNeighborhood), k.var_mod);
     const int cnt = nb.count[var];
+    const int c_drop = k.classic ? 0 : (int)k.drop[pidx(g, x, y, z)];
     uint32_t lava_mask = 0;
 #pragma unroll
     for (int i = 0; i < 26; ++i) {
@@ -227,74 +339,117 @@ __device__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const in
         }
     }
     if (!lava_mask) return false;
-    Vote v;
     v.n = 0;
-    if (k.classic) {
-        while (lava_mask) {
-            const int i = __ffs(lava_mask) - 1;
-            lava_mask &= lava_mask - 1;
-            int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
-            resolve(g, sx, sy, sz);
-            v.add(__ldg(F + pidx(g, sx, sy, sz)), 0.0f);
+    while (lava_mask) {
+        int src[8];
+        int8_t dsc[8];
+        int32_t fl[8];
+        float te[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            src[q] = -1;
+            if (lava_mask) {
+                const int i = __ffs(lava_mask) - 1;
+                lava_mask &= lava_mask - 1;
+                const int dx = nb.off[var][i][0], dy = nb.off[var][i][1], dz = nb.off[var][i][2];
+                if (dz < 0 && !k.classic) {
+                    // a LAVA cell below feeds only by ponding (straight below), resolved on its own
+                    if (k.ponding && dx == 0 && dy == 0) src[q] = 26;
+                    continue;
+                }
+                src[q] = i;
+            }
         }
-        const int w = v.winner(prefix, gidx);
-        *out_flow = v.ids[w];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (src[q] < 0 || src[q] == 26) continue;
+            int sx = x + nb.off[var][src[q]][0], sy = y + nb.off[var][src[q]][1], sz = z + nb.off[var][src[q]][2];
+            resolve(g, sx, sy, sz);
+            const int64_t sp = pidx(g, sx, sy, sz);
+            fl[q] = __ldg(F + sp);
+            if (!k.classic) {
+                te[q] = __ldg(Te + sp);
+                dsc[q] = k.desc[sp];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (src[q] < 0) continue;
+            if (k.classic) {
+                v.add(fl[q], 0.0f);
+                continue;
+            }
+            if (src[q] == 26) {
+                // tryPonding (LavaCA.hpp:443-461)
+                if (k.spill == nullptr || z > __ldg(k.spill + x + (int64_t)g.nx * y)) continue;
+                const int bz = z - 1;
+                if (bz > 0) {  // hasSupport(x, y, bz)
+                    const int below = __ldg(T + pidx(g, x, y, bz - 1));
+                    const bool sup = solid_ground(below) || (below == kLava && bz - 1 < __ldg(k.spill + x + (int64_t)g.nx * y));
+                    if (!sup) continue;
+                }
+                const int nh = g.ny > 1 ? 4 : 2;
+                const int hx[4] = {-1, 1, 0, 0}, hy[4] = {0, 0, -1, 1};
+                bool open_side = false;
+                for (int h = 0; h < nh; ++h) {
+                    const int n = type_at(g, T, x + hx[h], y + hy[h], bz);
+                    open_side = open_side || n == kAir || n == kVoid;
+                }
+                if (open_side) continue;
+                const int64_t b = pidx(g, x, y, bz);
+                v.add(__ldg(F + b), __fsub_rn(__ldg(Te + b), k.cool_lateral));
+                continue;
+            }
+            const int i = src[q];
+            const int dx = nb.off[var][i][0], dy = nb.off[var][i][1], dz = nb.off[var][i][2];
+            float cooling;
+            if (dz > 0 && dx == 0 && dy == 0) {
+                cooling = k.cool_fall;
+            } else {
+                const int d = dsc[q];
+                if (d < 0) continue;
+                if (dz > 0) {
+                    if (c_drop != 0 || d != 1) continue;
+                    cooling = k.cool_fall;
+                } else {
+                    if (c_drop != d || (d == 1 && k.diag_falls)) continue;
+                    cooling = k.cool_lateral;
+                }
+            }
+            v.add(fl[q], __fsub_rn(te[q], cooling));
+        }
+    }
+    if (v.n == 0 || v.overflow()) return false;
+    int32_t wid = 0;
+    float wt = 0.0f;
+    v.pick(prefix, gidx, &wid, &wt);
+    if (k.classic) {
+        *out_flow = wid;
         *out_temp = 0.0f;
         return true;
     }
-    const int c_drop = k.drop[pidx(g, x, y, z)];
-    while (lava_mask) {
-        const int i = __ffs(lava_mask) - 1;
-        lava_mask &= lava_mask - 1;
-        const int dx = nb.off[var][i][0], dy = nb.off[var][i][1], dz = nb.off[var][i][2];
-        if (dz < 0) {
-            if (!(k.ponding && dx == 0 && dy == 0)) continue;
-            // tryPonding (LavaCA.hpp:443-461); the cell below is LAVA
-            if (k.spill == nullptr || z > __ldg(k.spill + x + (int64_t)g.nx * y)) continue;
-            const int bz = z - 1;
-            if (bz > 0) {  // hasSupport(x, y, bz)
-                const int below = __ldg(T + pidx(g, x, y, bz - 1));
-                const bool sup = solid_ground(below) || (below == kLava && bz - 1 < __ldg(k.spill + x + (int64_t)g.nx * y));
-                if (!sup) continue;
-            }
-            const int nh = g.ny > 1 ? 4 : 2;
-            const int hx[4] = {-1, 1, 0, 0}, hy[4] = {0, 0, -1, 1};
-            bool open_side = false;
-            for (int h = 0; h < nh; ++h) {
-                const int n = type_at(g, T, x + hx[h], y + hy[h], bz);
-                open_side = open_side || n == kAir || n == kVoid;
-            }
-            if (open_side) continue;
-            const int64_t b = pidx(g, x, y, bz);
-            v.add(__ldg(F + b), __fsub_rn(__ldg(Te + b), k.cool_lateral));
-            continue;
-        }
-        int sx = x + dx, sy = y + dy, sz = z + dz;
-        resolve(g, sx, sy, sz);
-        const int64_t s = pidx(g, sx, sy, sz);
-        float cooling;
-        if (dz > 0 && dx == 0 && dy == 0) {
-            cooling = k.cool_fall;
-        } else {
-            const int d = k.desc[s];
-            if (d < 0) continue;
-            if (dz > 0) {
-                if (c_drop != 0 || d != 1) continue;
-                cooling = k.cool_fall;
-            } else {
-                if (c_drop != d || (d == 1 && k.diag_falls)) continue;
-                cooling = k.cool_lateral;
-            }
-        }
-        v.add(__ldg(F + s), __fsub_rn(__ldg(Te + s), cooling));
-    }
-    if (v.n == 0) return false;
-    const int w = v.winner(prefix, gidx);
-    const float wt = v.max_temp[w];
     if (!(wt >= k.solidus)) return false;
-    *out_flow = v.ids[w];
+    *out_flow = wid;
     *out_temp = wt;
     return true;
+}
+
+// A cell with five or more distinct flowIds among its sources: the vote with room for 26.
+__device__ __noinline__ bool air_gains_lava_wide(const CaKernelArgs& k, const uint8_t* T, const int32_t* F,
+                                                 const float* Te, int x, int y, int z, uint64_t prefix, uint64_t gidx,
+                                                 int32_t* out_flow, float* out_temp) {
+    Vote v;
+    return gather_vote(k, T, F, Te, x, y, z, prefix, gidx, v, out_flow, out_temp);
+}
+
+__device__ __forceinline__ bool air_gains_lava(const CaKernelArgs& k, const uint8_t* T, const int32_t* F,
+                                               const float* Te, int x, int y, int z, uint64_t prefix, uint64_t gidx,
+                                               int32_t* out_flow, float* out_temp) {
+    SmallVote v;
+    v.over = false;
+    const bool gained = gather_vote(k, T, F, Te, x, y, z, prefix, gidx, v, out_flow, out_temp);
+    if (v.over) return air_gains_lava_wide(k, T, F, Te, x, y, z, prefix, gidx, out_flow, out_temp);
+    return gained;
 }
 
 // Schedule the tiles within one tile of `tile` for step t + 1; lanes 0..26 of a warp each try one
@@ -327,6 +482,18 @@ __device__ __forceinline__ void schedule_around(const CaKernelArgs& k, uint32_t 
     const unsigned pos = slot + __popc(ballot & ((1u << lane) - 1u));
     if (first && pos < k.ntiles) k.tile_list[nxt][pos] = target;  // a tile is listed once per step
 }
+
+// Asynchronous global -> shared copies (cp.async): the data lands without passing through registers;
+// cp_async_wait_all waits for all of this thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Shared-memory row of the tile cell (ly, lz) in the staged halo layout.
 __device__ __forceinline__ int hr_of(int ly, int lz, int hy_on, int hz_on, int HY) { return (ly + hy_on) + HY * (lz + hz_on); }
@@ -368,6 +535,8 @@ constexpr int kCandBuf = 3 * kTileCells;  // candidates a rules block gathers be
 // ------------------------------------------------------------------------------------------
 __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaKernelArgs k) {
     __shared__ __align__(16) uint8_t s_type[kMaxHaloRows * kSmemRowBytes];
+    __shared__ __align__(16) int8_t s_drop[kMaxDropRows * kSmemRowBytes];
+    __shared__ int s_spill[kTileCells];
     __shared__ unsigned s_flags[2];
     __shared__ unsigned s_wtot[kThreads / 32];
     __shared__ uint32_t s_sched_tile[kMaxDeferred];
@@ -448,32 +617,81 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             s2 = *reinterpret_cast<const uint2*>(k.solid[cur] + p);
             a2 = *reinterpret_cast<const uint2*>(k.arrival[cur] + p);
         }
-        for (int wi = tid; wi < halo_rows * 16; wi += kThreads) {
-            const int r = wi >> 4, word = wi & 15;
+        // Stage the tile's types with a one-cell halo (and, in lava mode, the drop depths of its levels
+        // and the spill levels of its columns) in shared memory: asynchronous 16-byte copies of whole
+        // row chunks, all in flight together with the state loads above; rows outside the grid are
+        // VOID (drop -1), the two frame bytes of each row come through registers.
+        for (int c = tid; c < halo_rows * 4; c += kThreads) {
+            const int r = c >> 2, ch = c & 3;
             int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-            uint32_t v = 0xFFFFFFFFu;
-            const int xw = x0 + 4 * word;
-            if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2])) {
-                v = *reinterpret_cast<const uint32_t*>(T + pidx(g, xw, yy, zz));
-                // Periodic x with padded rows: the frame cell x = nx inside this word is the copy of x = 0.
-                if (g.per[0] && g.nx < g.P && xw <= g.nx && g.nx < xw + 4) {
-                    const int b = g.nx - xw;
-                    const uint32_t c0 = T[pidx(g, 0, yy, zz)];
-                    v = (v & ~(0xFFu << (8 * b))) | (c0 << (8 * b));
-                }
-            }
-            *reinterpret_cast<uint32_t*>(s_type + r * kSmemRowBytes + 4 + 4 * word) = v;
+            uint8_t* dst = s_type + r * kSmemRowBytes + kRowOff + 16 * ch;
+            if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                cp_async16(dst, T + pidx(g, x0 + 16 * ch, yy, zz));
+            else
+                *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
         }
-        for (int e = tid; e < halo_rows * 2; e += kThreads) {
-            const int r = e >> 1, right = e & 1;
+        int edge_at = -1, dedge_at = -1;
+        uint8_t edge = kVoid;
+        int8_t dedge = -1;
+        if (tid < halo_rows * 2) {
+            const int r = tid >> 1, right = tid & 1;
             int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
             int xx = right ? x0 + kTileX : x0 - 1;
-            uint8_t v = kVoid;
             if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                v = T[pidx(g, xx, yy, zz)];
-            s_type[r * kSmemRowBytes + (right ? 4 + kTileX : 3)] = v;
+                edge = T[pidx(g, xx, yy, zz)];
+            edge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
         }
+        if (!k.classic) {
+            // drop depths of the tile's rows and their y neighbours at the same levels (descent reads
+            // the side cells, dz = 0), and the spill levels of the tile's columns
+            for (int c = tid; c < HY * g.TZ * 4; c += kThreads) {
+                const int r = c >> 2, ch = c & 3;
+                int yy = y0 - hy_on + r % HY;
+                const int zz = z0 + r / HY;
+                int8_t* dst = s_drop + r * kSmemRowBytes + kRowOff + 16 * ch;
+                if (zz < g.nz && halo_axis(yy, g.ny, g.per[1]))
+                    cp_async16(dst, k.drop + pidx(g, x0 + 16 * ch, yy, zz));
+                else
+                    *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
+            }
+            const int de = tid - 128;
+            if (de >= 0 && de < HY * g.TZ * 2) {
+                const int r = de >> 1, right = de & 1;
+                int yy = y0 - hy_on + r % HY;
+                const int zz = z0 + r / HY;
+                int xx = right ? x0 + kTileX : x0 - 1;
+                if (zz < g.nz && halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) dedge = k.drop[pidx(g, xx, yy, zz)];
+                dedge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
+            }
+            if (k.spill != nullptr)
+                for (int e = tid; e < kTileX * g.TY; e += kThreads) {
+                    const int xx = x0 + (e & (kTileX - 1)), yy = y0 + e / kTileX;
+                    if (xx < g.nx && yy < g.ny)
+                        cp_async4(&s_spill[e], k.spill + xx + (int64_t)g.nx * yy);
+                    else
+                        s_spill[e] = 0;
+                }
+        }
+        cp_async_wait_all();
+        if (edge_at >= 0) s_type[edge_at] = edge;
+        if (dedge_at >= 0) s_drop[dedge_at] = dedge;
         __syncthreads();
+        if (g.per[0] && g.nx < g.P && x0 + kTileX > g.nx) {
+            // periodic x with padded rows: the frame cell x = nx inside the staged row is the copy of x = 0
+            const int b = g.nx - x0;
+            for (int r = tid; r < halo_rows; r += kThreads) {
+                int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
+                if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                    s_type[r * kSmemRowBytes + kRowOff + b] = T[pidx(g, 0, yy, zz)];
+            }
+            if (!k.classic)
+                for (int r = tid; r < HY * g.TZ; r += kThreads) {
+                    int yy = y0 - hy_on + r % HY;
+                    const int zz = z0 + r / HY;
+                    if (zz < g.nz && halo_axis(yy, g.ny, g.per[1])) s_drop[r * kSmemRowBytes + kRowOff + b] = k.drop[pidx(g, 0, yy, zz)];
+                }
+            __syncthreads();
+        }
 
         bool any_lava = false, any_changed = false;
         unsigned nbas = 0, ncand = 0;
@@ -483,13 +701,26 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         uint32_t cand_m = __vcmpeq4(w, 0u);
         const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
         if (cand_m) {
+            // An AIR cell can gain LAVA only from a source at its own level or above (same-level
+            // spread, falls), or, in lava mode, by ponding from the cell straight below when it lies at
+            // or below its column's spill level (gatherLavaCandidates, LavaCA.hpp:462-519); in classic
+            // mode from any LAVA neighbour.
             uint32_t near = 0;
-            for (int dz = -hz_on; dz <= hz_on; ++dz)
+            const int dz_lo = k.classic ? -hz_on : 0;
+            for (int dz = dz_lo; dz <= hz_on; ++dz)
                 for (int dy = -hy_on; dy <= hy_on; ++dy) {
-                    const uint8_t* rp = s_type + (hr + dy + HY * dz) * kSmemRowBytes + 4 + 4 * xq;
+                    const uint8_t* rp = s_type + (hr + dy + HY * dz) * kSmemRowBytes + kRowOff + 4 * xq;
                     const uint32_t m = __vcmpeq4(*reinterpret_cast<const uint32_t*>(rp), 0x02020202u);
                     near |= m | (m << 8) | (m >> 8) | (rp[-1] == kLava ? 0xFFu : 0u) | (rp[4] == kLava ? 0xFF000000u : 0u);
                 }
+            if (!k.classic && hz_on && k.ponding && k.spill != nullptr) {
+                const uint8_t* rp = s_type + (hr - HY) * kSmemRowBytes + kRowOff + 4 * xq;
+                uint32_t m = __vcmpeq4(*reinterpret_cast<const uint32_t*>(rp), 0x02020202u);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (z > s_spill[ly * kTileX + 4 * xq + j]) m &= ~(0xFFu << (8 * j));
+                near |= m;
+            }
             cand_m &= near;
 #pragma unroll
             for (int j = 0; j < 4; ++j)
@@ -499,7 +730,8 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         if (lava_m && !k.classic) {
             // D(n) of each LAVA cell of the current state (descent / computeDescent, LavaCA.hpp:421-429,
             // 551-566), read back by the candidate pass for its lava sources.
-            const uint8_t* rowp = s_type + hr * kSmemRowBytes + 4 + 4 * xq;
+            const uint8_t* rowp = s_type + hr * kSmemRowBytes + kRowOff + 4 * xq;
+            const int8_t* dropp = s_drop + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (!((lava_m >> (8 * j)) & 0xFF)) continue;
@@ -507,7 +739,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                 if (!sup) {
                     const int below = rowp[j - HY * kSmemRowBytes];
                     sup = solid_ground(below) ||
-                          (below == kLava && k.spill != nullptr && z - 1 < __ldg(k.spill + (x + j) + (int64_t)g.nx * y));
+                          (below == kLava && k.spill != nullptr && z - 1 < s_spill[ly * kTileX + 4 * xq + j]);
                 }
                 int d = -1;
                 if (sup) {
@@ -515,10 +747,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                     for (int s = 0; s < k.tables.nside; ++s) {
                         const int sx = k.tables.side[s][0], sy = k.tables.side[s][1];
                         if (rowp[j + sx + sy * kSmemRowBytes] != kAir) continue;
-                        int ax = x + j + sx, ay = y + sy;
-                        wrap_axis(ax, g.nx, g.per[0]);
-                        wrap_axis(ay, g.ny, g.per[1]);
-                        d = max(d, (int)k.drop[pidx(g, ax, ay, z)]);
+                        d = max(d, (int)dropp[j + sx + sy * kSmemRowBytes]);
                     }
                 }
                 k.desc[p + j] = (int8_t)d;
@@ -634,7 +863,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
 // finishes the step (finishStep, LavaCA.hpp:1206-1229).
 // ------------------------------------------------------------------------------------------
 constexpr int kCandThreads = 128;
-__global__ __launch_bounds__(kCandThreads) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
+__global__ __launch_bounds__(kCandThreads, 6) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
     __shared__ unsigned long long s_red[kCandThreads / 32];
     __shared__ bool s_last;
     CaCtrl* ctrl = k.ctrl;
@@ -1030,29 +1259,30 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
     VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
     int chunk = 4;
     int done = 0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
+    std::vector<cudaEvent_t> prof;  // profile mode: 4 events a step around drop, rules, cand
     size_t ev_used = 0;
     const int steps_before = h->steps;
+    auto mark = [&]() -> cudaError_t {
+        while (h->prof_events.size() < ev_used + 1) {
+            cudaEvent_t e;
+            const cudaError_t ce = cudaEventCreate(&e);
+            if (ce != cudaSuccess) return ce;
+            h->prof_events.push_back(e);
+        }
+        cudaEvent_t e = h->prof_events[ev_used++];
+        prof.push_back(e);
+        return cudaEventRecord(e, h->stream);
+    };
     while (true) {
         const int n = until_stop ? chunk : std::min(chunk, max_new_steps - done);
         for (int s = 0; s < n; ++s) {
+            if (h->profile_kernels) VCA_CUDA(mark());
             ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
-            if (h->profile_kernels) {
-                while (h->prof_events.size() < ev_used + 2) {
-                    cudaEvent_t e;
-                    VCA_CUDA(cudaEventCreate(&e));
-                    h->prof_events.push_back(e);
-                }
-                cudaEvent_t e0 = h->prof_events[ev_used], e1 = h->prof_events[ev_used + 1];
-                ev_used += 2;
-                VCA_CUDA(cudaEventRecord(e0, h->stream));
-                ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
-                VCA_CUDA(cudaEventRecord(e1, h->stream));
-                prof.push_back({e0, e1});
-            } else {
-                ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
-            }
+            if (h->profile_kernels) VCA_CUDA(mark());
+            ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
+            if (h->profile_kernels) VCA_CUDA(mark());
             ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
+            if (h->profile_kernels) VCA_CUDA(mark());
         }
         VCA_CUDA(cudaGetLastError());
         h->launches += (uint64_t)n * 3;
@@ -1069,11 +1299,13 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
     h->total_ms += ms;
     if (h->profile_kernels) {
         // Launches after the stop exit at once; only the ones that did a step count.
-        const uint64_t real = std::min<uint64_t>(prof.size(), (uint64_t)(h->steps - steps_before));
+        const uint64_t real = std::min<uint64_t>(prof.size() / 4, (uint64_t)(h->steps - steps_before));
         for (size_t i = 0; i < real; ++i) {
-            float m = 0.f;
-            VCA_CUDA(cudaEventElapsedTime(&m, prof[i].first, prof[i].second));
-            h->rules_ms += m;
+            float m[3] = {0.f, 0.f, 0.f};
+            for (int j = 0; j < 3; ++j) VCA_CUDA(cudaEventElapsedTime(&m[j], prof[4 * i + j], prof[4 * i + j + 1]));
+            h->drop_ms += m[0];
+            h->rules_ms += m[1];
+            h->cand_ms += m[2];
             ++h->rules_launches;
         }
     }
@@ -1290,7 +1522,10 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ca_rules_kernel, kThreads, 0);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
     h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)prop.multiProcessorCount * std::max(1, per_sm));
-    h->cand_blocks = prop.multiProcessorCount * 8;
+    int cand_per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cand_per_sm, ca_cand_kernel, kCandThreads, 0);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
+    h->cand_blocks = prop.multiProcessorCount * std::max(1, cand_per_sm);  // one wave
     if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&h->ring_ev[0], cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&h->ring_ev[1], cudaEventDisableTiming)) != cudaSuccess)
@@ -1489,6 +1724,16 @@ vca_status vca_ca_get_spill(vca_ca* h, int32_t* spill) {
     }
     VCA_CUDA(cudaSetDevice(h->device));
     VCA_CUDA(cudaMemcpy(spill, h->spill, sizeof(int32_t) * (size_t)h->geom.nx * h->geom.ny, cudaMemcpyDeviceToHost));
+    return VCA_OK;
+}
+
+vca_status vca_ca_kernel_times(vca_ca* h, double* drop_ms, double* rules_ms, double* cand_ms, uint64_t* steps) {
+    if (vca_status s = check(h)) return s;
+    const double n = h->rules_launches ? (double)h->rules_launches : 1.0;
+    if (drop_ms) *drop_ms = h->drop_ms / n;
+    if (rules_ms) *rules_ms = h->rules_ms / n;
+    if (cand_ms) *cand_ms = h->cand_ms / n;
+    if (steps) *steps = h->rules_launches;
     return VCA_OK;
 }
 

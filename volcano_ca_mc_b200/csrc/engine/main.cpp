@@ -337,7 +337,7 @@ RunSummary run_ca(const Config& cfg, const std::string& out_dir, Timing& timing,
     double dev_ms = 0.0, rules_ms = 0.0;
     uint64_t rules_n = 0;
     vca_ca_timing(ca.h, &dev_ms, &rules_ms, &rules_n);
-    if (timing.detail) timing.add_detail("caDevice", dev_ms);
+    timing.add_detail("caDevice", dev_ms);
 
     if (progress.on) progress.report("save", 0, 1, true);
     t = Clock::now();
@@ -559,6 +559,8 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     d.device = device_ordinal();
     McHandle mc;
     vcheck(vca_mc_create(&d, &mc.h), "vca_mc_create");
+    timing.add_detail("mcCreate", ms_since(t));
+    auto td = Clock::now();
     std::vector<float> cell_mob;
     if (full) {
         vcheck(vca_mc_set_domain(mc.h, nullptr), "vca_mc_set_domain");
@@ -586,7 +588,10 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
         if (cooling == Cooling::SolidOnly)
             s.warnings.push_back("ca_result.bin version 1 has no arrivalStep, liquid time counted from step 0 (= solidStep)");
     }
+    timing.add_detail("mcDomainMobility", ms_since(td));
+    td = Clock::now();
     vcheck(vca_mc_initialize(mc.h), "vca_mc_initialize");
+    timing.add_detail("mcInitialize", ms_since(td));
     vca_mc_info info{};
     vcheck(vca_mc_get_info(mc.h, &info), "vca_mc_get_info");
     s.domain_cells = info.domain_cells;
@@ -600,9 +605,14 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     CrystalMap cmap;
     cmap.dims = dims;
     cmap.crystal.resize((size_t)dims.cells());
+    double grains_ms = 0.0, crystals_ms = 0.0;
     auto measure = [&](GrainLabels* keep) {
+        auto tm = Clock::now();
         vcheck(vca_mc_crystals(mc.h, cmap.crystal.data()), "vca_mc_crystals");
+        crystals_ms += ms_since(tm);
+        tm = Clock::now();
         GrainLabels g = label_grains(cmap, moore, periodic);
+        grains_ms += ms_since(tm);
         McStats st;
         vca_mc_info mi{};
         vcheck(vca_mc_get_info(mc.h, &mi), "vca_mc_get_info");
@@ -672,7 +682,9 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     double dev_ms = 0.0, color_ms = 0.0;
     uint64_t color_n = 0;
     vca_mc_timing(mc.h, &dev_ms, &color_ms, &color_n);
-    if (timing.detail) timing.add_detail("mcDevice", dev_ms);
+    timing.add_detail("mcDevice", dev_ms);
+    timing.add_detail("mcStatsCrystals", crystals_ms);
+    timing.add_detail("mcStatsGrains", grains_ms);
 
     // stats.json "mc" (McStage::statsJson, McStage.cpp:326-383)
     t = Clock::now();

@@ -150,6 +150,7 @@ struct vca_ca {
     double total_ms = 0.0;
     double rules_ms = 0.0;
     uint64_t rules_launches = 0;
+    double drop_ms = 0.0, cand_ms = 0.0;  // profile mode: the other two kernels of a step
     uint64_t launches = 0;    // kernel launches issued
     int profile_kernels = 0;  // bracket each rules launch with events (set by VCA_PROFILE_KERNELS=1)
     std::vector<cudaEvent_t> prof_events;
