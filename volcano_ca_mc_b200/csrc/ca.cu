@@ -494,6 +494,9 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// all committed groups but the most recent one are complete
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Shared-memory row of the tile cell (ly, lz) in the staged halo layout.
 __device__ __forceinline__ int hr_of(int ly, int lz, int hy_on, int hz_on, int HY) { return (ly + hy_on) + HY * (lz + hz_on); }
@@ -516,27 +519,52 @@ __device__ __forceinline__ void warp_append(uint32_t* list, unsigned int* count,
 
 constexpr int kMaxDeferred = 64;   // tiles a rules block schedules in one batch
 constexpr int kTileCells = 1024;   // 64 x TY x TZ, TY * TZ = 16
-constexpr int kCandBuf = 3 * kTileCells;  // candidates a rules block gathers before one flush
+constexpr int kCandBuf = 2 * kTileCells;  // candidates a rules block gathers before one flush
 
 // ------------------------------------------------------------------------------------------
-// Rules, streaming pass.  A persistent block takes one tile at a time:
-//   1. its threads load their 4 cells' state (128-bit flowId and temp, 64-bit steps, 32-bit types),
-//      then stage the tile's types with a one-cell halo in shared memory (frame semantics at the
-//      grid edges), so that the two memory latencies overlap;
-//   2. LAVA cells cool (updateLava's LAVA branch, LavaCA.hpp:1135-1151) and get their D(n);
-//      every cell is written to the next buffer, unchanged otherwise; AIR cells with LAVA within
-//      one cell (3x3x3) are gathered in shared memory and appended to the candidate list in
-//      batches (one atomic per batch), resolved by the candidate pass;
-//   3. LAVA -> BASALT cells are listed for the drop-depth rescan;
-//   4. the block batches its tiles' flags and, after the loop, schedules the next step's tiles:
+// Rules, streaming pass.  A persistent block walks its tiles through a two-slot pipeline in
+// shared memory: while tile i is computed from slot i & 1, the asynchronous copies (cp.async) of
+// tile i + 1 fill the other slot -- its state (flowId, temp, solidStep, arrivalStep rows), its
+// types with a one-cell halo, and in lava mode the drop depths of its levels and the spill levels
+// of its columns.  The control loads run two tiles ahead (tile id of i + 2, mark of i + 1).
+// Per tile:
+//   1. LAVA cells cool (updateLava's LAVA branch, LavaCA.hpp:1135-1151) and get their D(n)
+//      (descent / computeDescent, LavaCA.hpp:421-429, 551-566) from byte windows of the staged
+//      types and drop depths; every cell is written to the next buffer, unchanged otherwise; AIR
+//      cells that a source could reach are gathered in shared memory and appended to the
+//      candidate list in batches, resolved by the candidate pass;
+//   2. LAVA -> BASALT cells are listed for the drop-depth rescan;
+//   3. the block batches its tiles' flags and, after the loop, schedules the next step's tiles:
 //      with LAVA a tile and its neighbours, changed only the tile itself.
 // A tile without LAVA within one tile (mark without lava bit, or not scheduled at all in the DENSE
-// schedule) cannot change and is copied through.
+// schedule) cannot change: only its state is staged, and copied through.
 // ------------------------------------------------------------------------------------------
+constexpr int kSpillCols = kTileX * 4;  // columns of a tile with nz > 1 (TY <= 4)
+
+struct __align__(16) RulesSlot {
+    int32_t flow[kTileCells];
+    float temp[kTileCells];
+    uint16_t solid[kTileCells];
+    uint16_t arrival[kTileCells];
+    uint8_t type[kMaxHaloRows * kSmemRowBytes];
+    int8_t drop[kMaxDropRows * kSmemRowBytes];
+    int32_t spill[kSpillCols];
+};
+constexpr size_t kRulesDynSmem = 2 * sizeof(RulesSlot);
+
+// Bytes x-1 .. x+2 / x .. x+3 / x+1 .. x+4 of a staged row around the 4 cells at p (p = row start +
+// kRowOff + 4 * xq; the frame bytes sit at kRowOff - 1 and kRowOff + 64).
+__device__ __forceinline__ uint32_t win_left(const uint8_t* p) {
+    return __funnelshift_r(*reinterpret_cast<const uint32_t*>(p - 4), *reinterpret_cast<const uint32_t*>(p), 24);
+}
+__device__ __forceinline__ uint32_t win_mid(const uint8_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
+__device__ __forceinline__ uint32_t win_right(const uint8_t* p) {
+    return __funnelshift_r(*reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 4), 8);
+}
+
 __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaKernelArgs k) {
-    __shared__ __align__(16) uint8_t s_type[kMaxHaloRows * kSmemRowBytes];
-    __shared__ __align__(16) int8_t s_drop[kMaxDropRows * kSmemRowBytes];
-    __shared__ int s_spill[kTileCells];
+    extern __shared__ __align__(16) uint8_t s_dyn[];
+    RulesSlot* slots = reinterpret_cast<RulesSlot*>(s_dyn);
     __shared__ unsigned s_flags[2];
     __shared__ unsigned s_wtot[kThreads / 32];
     __shared__ uint32_t s_sched_tile[kMaxDeferred];
@@ -559,13 +587,17 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     const int hy_on = g.ny > 1 ? 1 : 0, hz_on = g.nz > 1 ? 1 : 0;
     const int HY = hy_on ? g.TY + 2 : 1, HZ = hz_on ? g.TZ + 2 : 1;
     const int halo_rows = HY * HZ;
+    const int drop_rows = HY * g.TZ;
+    const bool lava_mode = !k.classic;
+    const bool stage_spill = lava_mode && hz_on && k.spill != nullptr;
     const bool erupting = (int64_t)t < (int64_t)k.eruption_steps;
     const uint32_t stamp = min(t, 65535u);
+    const uint32_t live_mark = 2u * (t + 1u) + 1u;
     if (tid == 0) s_flags[0] = s_flags[1] = 0;
 
     unsigned int my_active = 0, my_changed = 0, tiles_done = 0;
-    int it = 0, nsched = 0;
-    unsigned nbuf = 0;  // candidates in s_cand (block-uniform)
+    int nsched = 0, rit = 0;  // rit: rules tiles so far (parity of s_flags)
+    unsigned nbuf = 0;        // candidates in s_cand (block-uniform)
 
     auto flush_schedule = [&]() {
         __syncthreads();
@@ -585,255 +617,331 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         __syncthreads();
         nbuf = 0;
     };
+    auto tile_at = [&](uint64_t i) -> uint32_t { return k.dense ? (uint32_t)i : k.tile_list[cur][i]; };
 
-    for (uint64_t i = blockIdx.x; i < count; i += gridDim.x, ++it) {
-        const uint32_t tile = k.dense ? (uint32_t)i : k.tile_list[cur][i];
+    // Issue the copies of one tile into a slot.  Frame bytes of the halo rows come through
+    // registers (edge / dedge, stored by the caller once they have arrived).
+    int edge_at = -1, dedge_at = -1;
+    uint8_t edge = kVoid;
+    int8_t dedge = -1;
+    auto stage = [&](RulesSlot& sl, uint32_t tile, bool rules) {
+        int x0, y0, z0;
+        tile_origin(g, tile, x0, y0, z0);
+        {  // state rows: flowId and temp 16 chunks of 16 B each, solidStep / arrivalStep 8 each
+            const int yy = y0 + ly, zz = z0 + lz;
+            if (yy < g.ny && zz < g.nz) {
+                const int64_t p = pidx(g, x0, yy, zz);
+                const int c = xq;
+                cp_async16(&sl.flow[row * kTileX + 4 * c], k.flow[cur] + p + 4 * c);
+                cp_async16(&sl.temp[row * kTileX + 4 * c], k.temp[cur] + p + 4 * c);
+                if (c < 8)
+                    cp_async16(&sl.solid[row * kTileX + 8 * c], k.solid[cur] + p + 8 * c);
+                else
+                    cp_async16(&sl.arrival[row * kTileX + 8 * (c - 8)], k.arrival[cur] + p + 8 * (c - 8));
+            }
+        }
+        if (!rules) {
+            // own rows of the types only, in their halo positions
+            if (tid < 64) {
+                const int r = tid >> 2, ch = tid & 3;
+                const int rly = r % g.TY, rlz = r / g.TY;
+                const int yy = y0 + rly, zz = z0 + rlz;
+                uint8_t* dst = sl.type + hr_of(rly, rlz, hy_on, hz_on, HY) * kSmemRowBytes + kRowOff + 16 * ch;
+                if (yy < g.ny && zz < g.nz)
+                    cp_async16(dst, T + pidx(g, x0 + 16 * ch, yy, zz));
+                else
+                    *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
+            }
+            return;
+        }
+        if (tid < halo_rows * 4) {
+            const int r = tid >> 2, ch = tid & 3;
+            int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
+            uint8_t* dst = sl.type + r * kSmemRowBytes + kRowOff + 16 * ch;
+            if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                cp_async16(dst, T + pidx(g, x0 + 16 * ch, yy, zz));
+            else
+                *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
+        }
+        if (tid < halo_rows * 2) {
+            const int r = tid >> 1, right = tid & 1;
+            int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
+            int xx = right ? x0 + kTileX : x0 - 1;
+            edge = kVoid;
+            if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                edge = T[pidx(g, xx, yy, zz)];
+            edge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
+        }
+        if (!lava_mode) return;
+        {
+            const int c = tid - 144;  // threads 144 .. 239: the drop-depth rows (at most 24 x 4 chunks)
+            if (c >= 0 && c < drop_rows * 4) {
+                const int r = c >> 2, ch = c & 3;
+                int yy = y0 - hy_on + r % HY;
+                const int zz = z0 + r / HY;
+                int8_t* dst = sl.drop + r * kSmemRowBytes + kRowOff + 16 * ch;
+                if (zz < g.nz && halo_axis(yy, g.ny, g.per[1]))
+                    cp_async16(dst, k.drop + pidx(g, x0 + 16 * ch, yy, zz));
+                else
+                    *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
+            }
+            const int de = tid - 128;  // threads 128 .. 175: their frame bytes
+            if (de >= 0 && de < drop_rows * 2) {
+                const int r = de >> 1, right = de & 1;
+                int yy = y0 - hy_on + r % HY;
+                const int zz = z0 + r / HY;
+                int xx = right ? x0 + kTileX : x0 - 1;
+                dedge = -1;
+                if (zz < g.nz && halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) dedge = k.drop[pidx(g, xx, yy, zz)];
+                dedge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
+            }
+        }
+        if (stage_spill && tid < kTileX * g.TY) {
+            const int xx = x0 + (tid & (kTileX - 1)), yy = y0 + tid / kTileX;
+            if (xx < g.nx && yy < g.ny)
+                cp_async4(&sl.spill[tid], k.spill + xx + (int64_t)g.nx * yy);
+            else
+                sl.spill[tid] = 0;
+        }
+    };
+
+    // control pipeline: tile ids of the next two iterations, the mark of the next
+    const uint64_t G = gridDim.x;
+    uint64_t i = blockIdx.x;
+    uint32_t tile_a = 0, mark_a = 0, vent_a = 0;  // iteration it
+    uint32_t tile_b = 0, mark_b = 0, vent_b = 0;  // it + 1
+    uint32_t tile_c = 0;                          // it + 2
+    if (i < count) {
+        tile_a = tile_at(i);
+        mark_a = k.tile_mark[cur][tile_a];
+        vent_a = k.tile_flags[tile_a];
+        if (i + G < count) tile_b = tile_at(i + G);
+        if (i + 2 * G < count) tile_c = tile_at(i + 2 * G);
+        stage(slots[0], tile_a, mark_a == live_mark);
+    }
+    cp_async_commit();
+    if (i + G < count) {
+        mark_b = k.tile_mark[cur][tile_b];
+        vent_b = k.tile_flags[tile_b];
+    }
+
+    for (int it = 0; i < count; i += G, ++it) {
+        RulesSlot& sl = slots[it & 1];
+        const uint32_t tile = tile_a;
+        const bool rules = mark_a == live_mark;
+        const bool tile_vent = (vent_a & 2u) != 0;
+        // the frame bytes of this slot have arrived by now (loaded one iteration ago)
+        const int my_edge_at = edge_at, my_dedge_at = dedge_at;
+        const uint8_t my_edge = edge;
+        const int8_t my_dedge = dedge;
+        edge_at = dedge_at = -1;
+        // next tile's copies into the other slot, then the control loads of the tiles after it
+        if (i + G < count) stage(slots[(it + 1) & 1], tile_b, mark_b == live_mark);
+        cp_async_commit();
+        uint32_t mark_c = 0, vent_c = 0, tile_d = 0;
+        if (i + 2 * G < count) {
+            mark_c = k.tile_mark[cur][tile_c];
+            vent_c = k.tile_flags[tile_c];
+        }
+        if (i + 3 * G < count) tile_d = tile_at(i + 3 * G);
+        cp_async_wait_prior();  // this slot's copies
+        if (my_edge_at >= 0) sl.type[my_edge_at] = my_edge;
+        if (my_dedge_at >= 0) sl.drop[my_dedge_at] = my_dedge;
+        __syncthreads();
+
         int x0, y0, z0;
         tile_origin(g, tile, x0, y0, z0);
         ++tiles_done;
         const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
         const bool valid = y < g.ny && z < g.nz;
         const int64_t p = pidx(g, valid ? x : 0, valid ? y : 0, valid ? z : 0);
-        if (k.tile_mark[cur][tile] != 2u * (t + 1u) + 1u) {
+        const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
+        const uint8_t* rowp = sl.type + hr * kSmemRowBytes + kRowOff + 4 * xq;
+        const uint32_t w = valid ? win_mid(rowp) : 0xFFFFFFFFu;
+        int4 f4 = *reinterpret_cast<const int4*>(&sl.flow[row * kTileX + 4 * xq]);
+        float4 t4 = *reinterpret_cast<const float4*>(&sl.temp[row * kTileX + 4 * xq]);
+        uint2 s2 = *reinterpret_cast<const uint2*>(&sl.solid[row * kTileX + 4 * xq]);
+        const uint2 a2 = *reinterpret_cast<const uint2*>(&sl.arrival[row * kTileX + 4 * xq]);
+
+        if (!rules) {
             // No LAVA within one tile: nothing can change here, the cells go to the next buffer as they are.
             if (valid) {
-                *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = *reinterpret_cast<const uint32_t*>(T + p);
-                *reinterpret_cast<int4*>(k.flow[nxt] + p) = *reinterpret_cast<const int4*>(k.flow[cur] + p);
-                *reinterpret_cast<float4*>(k.temp[nxt] + p) = *reinterpret_cast<const float4*>(k.temp[cur] + p);
-                *reinterpret_cast<uint2*>(k.solid[nxt] + p) = *reinterpret_cast<const uint2*>(k.solid[cur] + p);
-                *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = *reinterpret_cast<const uint2*>(k.arrival[cur] + p);
+                *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = w;
+                *reinterpret_cast<int4*>(k.flow[nxt] + p) = f4;
+                *reinterpret_cast<float4*>(k.temp[nxt] + p) = t4;
+                *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
+                *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
             }
-            continue;
-        }
+            __syncthreads();  // the slot is refilled next iteration
+        } else {
+            if (g.per[0] && g.nx < g.P && x0 + kTileX > g.nx) {
+                // periodic x with padded rows: the frame cell x = nx inside the staged row is the copy of x = 0
+                const int b = g.nx - x0;
+                for (int r = tid; r < halo_rows; r += kThreads) {
+                    int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
+                    if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                        sl.type[r * kSmemRowBytes + kRowOff + b] = T[pidx(g, 0, yy, zz)];
+                }
+                if (lava_mode)
+                    for (int r = tid; r < drop_rows; r += kThreads) {
+                        int yy = y0 - hy_on + r % HY;
+                        const int zz = z0 + r / HY;
+                        if (zz < g.nz && halo_axis(yy, g.ny, g.per[1]))
+                            sl.drop[r * kSmemRowBytes + kRowOff + b] = k.drop[pidx(g, 0, yy, zz)];
+                    }
+                __syncthreads();
+            }
 
-        uint32_t w = 0xFFFFFFFFu;
-        int4 f4 = make_int4(0, 0, 0, 0);
-        float4 t4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        uint2 s2 = make_uint2(0, 0), a2 = make_uint2(0, 0);
-        if (valid) {
-            w = *reinterpret_cast<const uint32_t*>(T + p);
-            f4 = *reinterpret_cast<const int4*>(k.flow[cur] + p);
-            t4 = *reinterpret_cast<const float4*>(k.temp[cur] + p);
-            s2 = *reinterpret_cast<const uint2*>(k.solid[cur] + p);
-            a2 = *reinterpret_cast<const uint2*>(k.arrival[cur] + p);
-        }
-        // Stage the tile's types with a one-cell halo (and, in lava mode, the drop depths of its levels
-        // and the spill levels of its columns) in shared memory: asynchronous 16-byte copies of whole
-        // row chunks, all in flight together with the state loads above; rows outside the grid are
-        // VOID (drop -1), the two frame bytes of each row come through registers.
-        for (int c = tid; c < halo_rows * 4; c += kThreads) {
-            const int r = c >> 2, ch = c & 3;
-            int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-            uint8_t* dst = s_type + r * kSmemRowBytes + kRowOff + 16 * ch;
-            if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                cp_async16(dst, T + pidx(g, x0 + 16 * ch, yy, zz));
-            else
-                *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
-        }
-        int edge_at = -1, dedge_at = -1;
-        uint8_t edge = kVoid;
-        int8_t dedge = -1;
-        if (tid < halo_rows * 2) {
-            const int r = tid >> 1, right = tid & 1;
-            int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-            int xx = right ? x0 + kTileX : x0 - 1;
-            if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                edge = T[pidx(g, xx, yy, zz)];
-            edge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
-        }
-        if (!k.classic) {
-            // drop depths of the tile's rows and their y neighbours at the same levels (descent reads
-            // the side cells, dz = 0), and the spill levels of the tile's columns
-            for (int c = tid; c < HY * g.TZ * 4; c += kThreads) {
-                const int r = c >> 2, ch = c & 3;
-                int yy = y0 - hy_on + r % HY;
-                const int zz = z0 + r / HY;
-                int8_t* dst = s_drop + r * kSmemRowBytes + kRowOff + 16 * ch;
-                if (zz < g.nz && halo_axis(yy, g.ny, g.per[1]))
-                    cp_async16(dst, k.drop + pidx(g, x0 + 16 * ch, yy, zz));
-                else
-                    *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
-            }
-            const int de = tid - 128;
-            if (de >= 0 && de < HY * g.TZ * 2) {
-                const int r = de >> 1, right = de & 1;
-                int yy = y0 - hy_on + r % HY;
-                const int zz = z0 + r / HY;
-                int xx = right ? x0 + kTileX : x0 - 1;
-                if (zz < g.nz && halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) dedge = k.drop[pidx(g, xx, yy, zz)];
-                dedge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
-            }
-            if (k.spill != nullptr)
-                for (int e = tid; e < kTileX * g.TY; e += kThreads) {
-                    const int xx = x0 + (e & (kTileX - 1)), yy = y0 + e / kTileX;
-                    if (xx < g.nx && yy < g.ny)
-                        cp_async4(&s_spill[e], k.spill + xx + (int64_t)g.nx * yy);
-                    else
-                        s_spill[e] = 0;
+            bool any_lava = false, any_changed = false;
+            unsigned nbas = 0, ncand = 0;
+            uint32_t bas[4], cand[4];
+            const uint32_t g0 = (uint32_t)(x + g.nx * (y + g.ny * z));
+            const uint32_t lava_m = __vcmpeq4(w, 0x02020202u);
+            uint32_t cand_m = __vcmpeq4(w, 0u);
+            if (cand_m) {
+                // An AIR cell can gain LAVA only from a source at its own level or above (same-level
+                // spread, falls), or, in lava mode, by ponding from the cell straight below when it lies at
+                // or below its column's spill level (gatherLavaCandidates, LavaCA.hpp:462-519); in classic
+                // mode from any LAVA neighbour.
+                uint32_t near = 0;
+                const int dz_lo = lava_mode ? 0 : -hz_on;
+                for (int dz = dz_lo; dz <= hz_on; ++dz)
+                    for (int dy = -hy_on; dy <= hy_on; ++dy) {
+                        const uint8_t* rp = sl.type + (hr + dy + HY * dz) * kSmemRowBytes + kRowOff + 4 * xq;
+                        near |= __vcmpeq4(win_left(rp), 0x02020202u) | __vcmpeq4(win_mid(rp), 0x02020202u) |
+                                __vcmpeq4(win_right(rp), 0x02020202u);
+                    }
+                if (stage_spill && k.ponding) {
+                    uint32_t m = __vcmpeq4(win_mid(rowp - HY * kSmemRowBytes), 0x02020202u);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (z > sl.spill[ly * kTileX + 4 * xq + j]) m &= ~(0xFFu << (8 * j));
+                    near |= m;
                 }
-        }
-        cp_async_wait_all();
-        if (edge_at >= 0) s_type[edge_at] = edge;
-        if (dedge_at >= 0) s_drop[dedge_at] = dedge;
-        __syncthreads();
-        if (g.per[0] && g.nx < g.P && x0 + kTileX > g.nx) {
-            // periodic x with padded rows: the frame cell x = nx inside the staged row is the copy of x = 0
-            const int b = g.nx - x0;
-            for (int r = tid; r < halo_rows; r += kThreads) {
-                int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-                if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                    s_type[r * kSmemRowBytes + kRowOff + b] = T[pidx(g, 0, yy, zz)];
-            }
-            if (!k.classic)
-                for (int r = tid; r < HY * g.TZ; r += kThreads) {
-                    int yy = y0 - hy_on + r % HY;
-                    const int zz = z0 + r / HY;
-                    if (zz < g.nz && halo_axis(yy, g.ny, g.per[1])) s_drop[r * kSmemRowBytes + kRowOff + b] = k.drop[pidx(g, 0, yy, zz)];
-                }
-            __syncthreads();
-        }
-
-        bool any_lava = false, any_changed = false;
-        unsigned nbas = 0, ncand = 0;
-        uint32_t bas[4], cand[4];
-        const uint32_t g0 = (uint32_t)(x + g.nx * (y + g.ny * z));
-        const uint32_t lava_m = __vcmpeq4(w, 0x02020202u);
-        uint32_t cand_m = __vcmpeq4(w, 0u);
-        const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
-        if (cand_m) {
-            // An AIR cell can gain LAVA only from a source at its own level or above (same-level
-            // spread, falls), or, in lava mode, by ponding from the cell straight below when it lies at
-            // or below its column's spill level (gatherLavaCandidates, LavaCA.hpp:462-519); in classic
-            // mode from any LAVA neighbour.
-            uint32_t near = 0;
-            const int dz_lo = k.classic ? -hz_on : 0;
-            for (int dz = dz_lo; dz <= hz_on; ++dz)
-                for (int dy = -hy_on; dy <= hy_on; ++dy) {
-                    const uint8_t* rp = s_type + (hr + dy + HY * dz) * kSmemRowBytes + kRowOff + 4 * xq;
-                    const uint32_t m = __vcmpeq4(*reinterpret_cast<const uint32_t*>(rp), 0x02020202u);
-                    near |= m | (m << 8) | (m >> 8) | (rp[-1] == kLava ? 0xFFu : 0u) | (rp[4] == kLava ? 0xFF000000u : 0u);
-                }
-            if (!k.classic && hz_on && k.ponding && k.spill != nullptr) {
-                const uint8_t* rp = s_type + (hr - HY) * kSmemRowBytes + kRowOff + 4 * xq;
-                uint32_t m = __vcmpeq4(*reinterpret_cast<const uint32_t*>(rp), 0x02020202u);
+                cand_m &= near;
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    if (z > s_spill[ly * kTileX + 4 * xq + j]) m &= ~(0xFFu << (8 * j));
-                near |= m;
+                    if ((cand_m >> (8 * j)) & 0xFF) cand[ncand++] = g0 + j;
             }
-            cand_m &= near;
+            uint32_t wout = w;
+            if (lava_m && lava_mode) {
+                // D(n) of the LAVA cells: support from the cell below, then the largest drop depth of
+                // the AIR side cells (dz = 0 offsets of every variant), -1 without support.
+                uint32_t sup = 0xFFFFFFFFu;
+                if (z > 0) {
+                    const uint32_t below = win_mid(rowp - HY * kSmemRowBytes);
+                    sup = __vcmpeq4(below, 0x01010101u) | __vcmpeq4(below, 0x03030303u);
+                    uint32_t lb = __vcmpeq4(below, 0x02020202u);
+                    if (lb && stage_spill) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if ((cand_m >> (8 * j)) & 0xFF) cand[ncand++] = g0 + j;
-        }
-        uint32_t wout = w;
-        if (lava_m && !k.classic) {
-            // D(n) of each LAVA cell of the current state (descent / computeDescent, LavaCA.hpp:421-429,
-            // 551-566), read back by the candidate pass for its lava sources.
-            const uint8_t* rowp = s_type + hr * kSmemRowBytes + kRowOff + 4 * xq;
-            const int8_t* dropp = s_drop + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (!((lava_m >> (8 * j)) & 0xFF)) continue;
-                bool sup = z == 0;
-                if (!sup) {
-                    const int below = rowp[j - HY * kSmemRowBytes];
-                    sup = solid_ground(below) ||
-                          (below == kLava && k.spill != nullptr && z - 1 < s_spill[ly * kTileX + 4 * xq + j]);
-                }
-                int d = -1;
-                if (sup) {
-                    d = 0;
-                    for (int s = 0; s < k.tables.nside; ++s) {
-                        const int sx = k.tables.side[s][0], sy = k.tables.side[s][1];
-                        if (rowp[j + sx + sy * kSmemRowBytes] != kAir) continue;
-                        d = max(d, (int)dropp[j + sx + sy * kSmemRowBytes]);
+                        for (int j = 0; j < 4; ++j)
+                            if (!(z - 1 < sl.spill[ly * kTileX + 4 * xq + j])) lb &= ~(0xFFu << (8 * j));
+                        sup |= lb;
                     }
                 }
-                k.desc[p + j] = (int8_t)d;
-            }
-        }
-        if (lava_m) {
-            if (k.classic) {
-                my_active += __popc(lava_m) >> 3;
-                any_lava = true;
-            } else {
-                float te[4] = {t4.x, t4.y, t4.z, t4.w};
-                const int32_t fl[4] = {f4.x, f4.y, f4.z, f4.w};
-                uint32_t so[2] = {s2.x, s2.y};
+                uint32_t acc = 0;
+                const int8_t* dropc = sl.drop + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    if (!((lava_m >> (8 * j)) & 0xFF)) continue;
-                    const float before = te[j];
-                    bool vent = false;
-                    if (erupting && fl[j] > 0 && fl[j] < k.vent_slots) {
-                        const int4 vc = __ldg(k.vents + fl[j]);
-                        vent = vc.x == x + j && vc.y == y && vc.z == z;
-                    }
-                    const float nt = vent ? k.erupt_temp : __fsub_rn(before, k.cool_ambient);
-                    te[j] = nt;
-                    if (nt < k.solidus) {
-                        const uint32_t half = (j & 1) * 16;
-                        wout = (wout & ~(0xFFu << (8 * j))) | ((uint32_t)kBasalt << (8 * j));
-                        so[j >> 1] = (so[j >> 1] & ~(0xFFFFu << half)) | (stamp << half);
-                        ++my_changed;
-                        bas[nbas++] = g0 + j;
-                        any_changed = true;
-                    } else {
-                        ++my_active;
-                        any_lava = true;
-                        if (nt != before) {
+                for (int sy = -1; sy <= 1; ++sy) {
+                    const unsigned bits = (k.side_mask >> (3 * (sy + 1))) & 7u;
+                    if (!bits) continue;
+                    const uint8_t* tp = rowp + sy * kSmemRowBytes;
+                    const uint8_t* dp = reinterpret_cast<const uint8_t*>(dropc) + sy * kSmemRowBytes;
+                    if (bits & 1u) acc = __vmaxs4(acc, win_left(dp) & __vcmpeq4(win_left(tp), 0u));
+                    if (bits & 2u) acc = __vmaxs4(acc, win_mid(dp) & __vcmpeq4(win_mid(tp), 0u));
+                    if (bits & 4u) acc = __vmaxs4(acc, win_right(dp) & __vcmpeq4(win_right(tp), 0u));
+                }
+                *reinterpret_cast<uint32_t*>(k.desc + p) = (acc & sup) | ~sup;
+            }
+            if (lava_m) {
+                if (k.classic) {
+                    my_active += __popc(lava_m) >> 3;
+                    any_lava = true;
+                } else {
+                    float te[4] = {t4.x, t4.y, t4.z, t4.w};
+                    const int32_t fl[4] = {f4.x, f4.y, f4.z, f4.w};
+                    uint32_t so[2] = {s2.x, s2.y};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (!((lava_m >> (8 * j)) & 0xFF)) continue;
+                        const float before = te[j];
+                        bool vent = false;
+                        if (erupting && tile_vent && fl[j] > 0 && fl[j] < k.vent_slots) {
+                            const int4 vc = __ldg(k.vents + fl[j]);
+                            vent = vc.x == x + j && vc.y == y && vc.z == z;
+                        }
+                        const float nt = vent ? k.erupt_temp : __fsub_rn(before, k.cool_ambient);
+                        te[j] = nt;
+                        if (nt < k.solidus) {
+                            const uint32_t half = (j & 1) * 16;
+                            wout = (wout & ~(0xFFu << (8 * j))) | ((uint32_t)kBasalt << (8 * j));
+                            so[j >> 1] = (so[j >> 1] & ~(0xFFFFu << half)) | (stamp << half);
                             ++my_changed;
+                            bas[nbas++] = g0 + j;
                             any_changed = true;
+                        } else {
+                            ++my_active;
+                            any_lava = true;
+                            if (nt != before) {
+                                ++my_changed;
+                                any_changed = true;
+                            }
                         }
                     }
+                    t4 = make_float4(te[0], te[1], te[2], te[3]);
+                    s2 = make_uint2(so[0], so[1]);
                 }
-                t4 = make_float4(te[0], te[1], te[2], te[3]);
-                s2 = make_uint2(so[0], so[1]);
             }
-        }
-        if (valid) {
-            *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = wout;
-            *reinterpret_cast<int4*>(k.flow[nxt] + p) = f4;
-            *reinterpret_cast<float4*>(k.temp[nxt] + p) = t4;
-            *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
-            *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
-        }
-        if (__any_sync(0xFFFFFFFFu, nbas != 0))
-            warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, nbas, bas);
+            if (valid) {
+                *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = wout;
+                *reinterpret_cast<int4*>(k.flow[nxt] + p) = f4;
+                *reinterpret_cast<float4*>(k.temp[nxt] + p) = t4;
+                *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
+                *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
+            }
+            if (__any_sync(0xFFFFFFFFu, nbas != 0))
+                warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, nbas, bas);
 
-        // candidates: block-wide positions in the shared buffer
-        unsigned incl = ncand;
+            // candidates: block-wide positions in the shared buffer
+            unsigned incl = ncand;
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const unsigned u = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-            if (lane >= off) incl += u;
-        }
-        if (lane == 31) s_wtot[warp] = incl;
-        unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
-        bits = __reduce_or_sync(0xFFFFFFFFu, bits);
-        if (lane == 0 && bits) atomicOr(&s_flags[it & 1], bits);
-        __syncthreads();
-        const unsigned tf = s_flags[it & 1];
-        if (tid == 32) s_flags[(it + 1) & 1] = 0;
-        unsigned wbase = 0, total = 0;
-        for (int w2 = 0; w2 < kThreads / 32; ++w2) {
-            const unsigned v = s_wtot[w2];
-            wbase += w2 < warp ? v : 0u;
-            total += v;
-        }
-        for (unsigned j = 0, pos = nbuf + wbase + incl - ncand; j < ncand; ++j) s_cand[pos + j] = cand[j];
-        nbuf += total;
-        if (tid == 0) {
-            if (tf) {
+            for (int off = 1; off < 32; off <<= 1) {
+                const unsigned u = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                if (lane >= off) incl += u;
+            }
+            if (lane == 31) s_wtot[warp] = incl;
+            unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
+            bits = __reduce_or_sync(0xFFFFFFFFu, bits);
+            if (lane == 0 && bits) atomicOr(&s_flags[rit & 1], bits);
+            __syncthreads();  // also: the slot is refilled next iteration
+            const unsigned tf = s_flags[rit & 1];
+            if (tid == 32) s_flags[(rit + 1) & 1] = 0;
+            ++rit;
+            unsigned wbase = 0, total = 0;
+            for (int w2 = 0; w2 < kThreads / 32; ++w2) {
+                const unsigned v = s_wtot[w2];
+                wbase += w2 < warp ? v : 0u;
+                total += v;
+            }
+            for (unsigned j = 0, pos = nbuf + wbase + incl - ncand; j < ncand; ++j) s_cand[pos + j] = cand[j];
+            nbuf += total;
+            if (tid == 0 && tf) {
                 s_sched_tile[nsched] = tile;
                 s_sched_flag[nsched] = (uint8_t)tf;
             }
+            if (tf) ++nsched;
+            if (nsched == kMaxDeferred) flush_schedule();
+            if (nbuf > kCandBuf - kTileCells) flush_cands();
         }
-        if (tf) ++nsched;
-        if (nsched == kMaxDeferred) flush_schedule();
-        if (nbuf > kCandBuf - kTileCells) flush_cands();
+        tile_a = tile_b;
+        mark_a = mark_b;
+        vent_a = vent_b;
+        tile_b = tile_c;
+        mark_b = mark_c;
+        vent_b = vent_c;
+        tile_c = tile_d;
     }
+    cp_async_wait_all();
     if (__syncthreads_or(nsched > 0)) flush_schedule();
     if (nbuf) flush_cands();
 
@@ -981,7 +1089,7 @@ __global__ __launch_bounds__(kThreads) void ca_tile_init_kernel(const __grid_con
             air = __popc(__vcmpeq4(w, 0u)) >> 3;  // padding cells are VOID, so they count as neither
         }
         const int any = __syncthreads_or(lava > 0);
-        if (threadIdx.x == 0) k.tile_flags[tile] = any ? 1u : 0u;
+        if (threadIdx.x == 0) k.tile_flags[tile] = (k.tile_flags[tile] & 2u) | (any ? 1u : 0u);
         const unsigned la = __reduce_add_sync(0xFFFFFFFFu, lava);
         const unsigned ai = __reduce_add_sync(0xFFFFFFFFu, air);
         if ((threadIdx.x & 31) == 0) {
@@ -1097,6 +1205,9 @@ CaKernelArgs make_args(const vca_ca* h) {
             if (o[2] == -1 && (o[0] != 0 || o[1] != 0)) diag = true;
         }
     k.diag_falls = diag;
+    k.side_mask = 0;
+    for (int i = 0; i < h->tables_host.nside; ++i)
+        k.side_mask |= 1u << (3 * (h->tables_host.side[i][1] + 1) + (h->tables_host.side[i][0] + 1));
     for (int b = 0; b < 2; ++b) {
         k.type[b] = h->type[b];
         k.flow[b] = h->flow[b];
@@ -1207,7 +1318,7 @@ vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
     VCA_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < kGraphSteps; ++s) {
         ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
-        ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
+        ca_rules_kernel<<<h->grid_blocks, kThreads, kRulesDynSmem, h->stream>>>(k);
         ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
     }
     cudaGraph_t graph = nullptr;
@@ -1279,7 +1390,7 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
             if (h->profile_kernels) VCA_CUDA(mark());
             ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
             if (h->profile_kernels) VCA_CUDA(mark());
-            ca_rules_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k);
+            ca_rules_kernel<<<h->grid_blocks, kThreads, kRulesDynSmem, h->stream>>>(k);
             if (h->profile_kernels) VCA_CUDA(mark());
             ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
             if (h->profile_kernels) VCA_CUDA(mark());
@@ -1356,6 +1467,15 @@ vca_status upload_vents(vca_ca* h, const vca_vent* vents, int count) {
     h->vents = nullptr;
     VCA_CUDA(cudaMalloc(&h->vents, sizeof(int4) * table.size()));
     VCA_CUDA(cudaMemcpyAsync(h->vents, table.data(), sizeof(int4) * table.size(), cudaMemcpyHostToDevice, h->stream));
+    // bit 1 of the tile flags: the tiles that hold a vent (the only ones whose LAVA can be reheated)
+    const auto& g = h->geom;
+    std::vector<uint32_t> flags(h->ntiles, 0u);
+    for (int i = 0; i < count; ++i) {
+        const vca_vent& v = vents[i];
+        if (v.x < 0 || v.x >= g.nx || v.y < 0 || v.y >= g.ny || v.z < 0 || v.z >= g.nz) continue;
+        flags[(size_t)(v.x / kTileX) + (size_t)g.tiles_x * ((size_t)(v.y / g.TY) + (size_t)g.tiles_y * (size_t)(v.z / g.TZ))] = 2u;
+    }
+    VCA_CUDA(cudaMemcpyAsync(h->tile_flags, flags.data(), 4 * flags.size(), cudaMemcpyHostToDevice, h->stream));
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->vent_slots = slots;
     return VCA_OK;
@@ -1519,7 +1639,9 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
         if ((e = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, "ca_pad_kernel"));
     }
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ca_rules_kernel, kThreads, 0);
+    e = cudaFuncSetAttribute(ca_rules_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRulesDynSmem);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ca_rules_kernel, kThreads, kRulesDynSmem);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
     h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)prop.multiProcessorCount * std::max(1, per_sm));
     int cand_per_sm = 0;

@@ -67,6 +67,7 @@ struct CaKernelArgs {
     int classic;
     int ponding;
     int diag_falls;           // LavaCA::diagonalFalls_ (LavaCA.hpp:108-110)
+    uint32_t side_mask;       // side offsets (dz = 0) as bits 3 (dy + 1) + (dx + 1)
     int dense;
     uint64_t seed;
     int max_steps;
@@ -87,7 +88,7 @@ struct CaKernelArgs {
     int vent_slots;
     CaTables tables;          // by value: read from the kernel parameter (constant) bank
     CaCtrl* ctrl;
-    uint32_t* tile_flags;     // set-up only: bit 0 = LAVA in the tile
+    uint32_t* tile_flags;     // bit 0 (set-up only) = LAVA in the tile, bit 1 = a vent in the tile
     uint32_t* tile_mark[2];   // 2 (s + 1) + lava bit of the step s the tile is scheduled for, per parity
     int8_t* desc;             // D(n) of LAVA cells of scheduled tiles (computeDescent, LavaCA.hpp:551-566)
     uint32_t* tile_list[2];   // tiles of step t are tile_list[t & 1]
