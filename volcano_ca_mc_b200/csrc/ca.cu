@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -280,7 +281,7 @@ __device__ void drop_rescan18(const CaKernelArgs& k, const uint8_t* T, int x, in
 // change list overflowed), and clears the change list this step's rules will fill.
 __global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force_full) {
     CaCtrl* ctrl = k.ctrl;
-    if (!force_full && ctrl->stop) return;
+    if (!force_full && (ctrl->stop || ctrl->error)) return;
     const uint32_t t = ctrl->steps;
     const int cur = t & 1, nxt = cur ^ 1;
     if (!force_full && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -522,35 +523,86 @@ constexpr int kTileCells = 1024;   // 64 x TY x TZ, TY * TZ = 16
 constexpr int kCandBuf = 2 * kTileCells;  // candidates a rules block gathers before one flush
 
 // ------------------------------------------------------------------------------------------
+// TMA and mbarrier primitives (PTX ISA: cp.async.bulk.tensor, mbarrier).  Tiled loads land in shared
+// memory and complete transaction bytes on an mbarrier; tiled stores read shared memory as bulk
+// groups.  Every wait is bounded: a wait that runs out reports failure to the caller.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Waits for the completion of the phase with the given parity; false after ~2^20 suspended tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (int i = 0; i < (1 << 20); ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity), "r"(1000u)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(map), "r"(x),
+                 "r"(y), "r"(z), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the shared-memory sources of all committed bulk stores have been read
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// orders this thread's generic-proxy shared-memory accesses before later async-proxy (TMA) ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// ------------------------------------------------------------------------------------------
 // Rules, streaming pass.  A persistent block walks its tiles through a two-slot pipeline in
-// shared memory: while tile i is computed from slot i & 1, the asynchronous copies (cp.async) of
-// tile i + 1 fill the other slot -- its state (flowId, temp, solidStep, arrivalStep rows), its
-// types with a one-cell halo, and in lava mode the drop depths of its levels and the spill levels
-// of its columns.  The control loads run two tiles ahead (tile id of i + 2, mark of i + 1).
+// shared memory.  Thread 0 issues the TMA box copies of tile i + 1 into one slot while tile i is
+// computed from the other: the tile's state boxes (flowId, temp, solidStep, arrivalStep), its types
+// with a one-cell halo (one box, x from x0 - 16 so that both frame bytes come along), and in lava
+// mode the drop depths of its levels; the threads add the spill levels of its columns (cp.async).
+// The control loads run two tiles ahead (tile id of i + 2, mark of i + 1).  Results are written back
+// into the slot and leave by TMA stores, which clip at the grid edges.
 // Per tile:
 //   1. LAVA cells cool (updateLava's LAVA branch, LavaCA.hpp:1135-1151) and get their D(n)
 //      (descent / computeDescent, LavaCA.hpp:421-429, 551-566) from byte windows of the staged
-//      types and drop depths; every cell is written to the next buffer, unchanged otherwise; AIR
-//      cells that a source could reach are gathered in shared memory and appended to the
-//      candidate list in batches, resolved by the candidate pass;
+//      types and drop depths; AIR cells that a source could reach are gathered in shared memory and
+//      appended to the candidate list in batches, resolved by the candidate pass;
 //   2. LAVA -> BASALT cells are listed for the drop-depth rescan;
 //   3. the block batches its tiles' flags and, after the loop, schedules the next step's tiles:
 //      with LAVA a tile and its neighbours, changed only the tile itself.
 // A tile without LAVA within one tile (mark without lava bit, or not scheduled at all in the DENSE
-// schedule) cannot change: only its state is staged, and copied through.
+// schedule) cannot change: thread 0 alone moves its state boxes from the current to the next buffer.
+// Tiles at the grid edge get their frame cells (VOID, or the periodic copy) patched after the load.
 // ------------------------------------------------------------------------------------------
 constexpr int kSpillCols = kTileX * 4;  // columns of a tile with nz > 1 (TY <= 4)
 
-struct __align__(16) RulesSlot {
+struct __align__(128) RulesSlot {
     int32_t flow[kTileCells];
     float temp[kTileCells];
     uint16_t solid[kTileCells];
     uint16_t arrival[kTileCells];
+    uint8_t own_type[kTileCells];
     uint8_t type[kMaxHaloRows * kSmemRowBytes];
     int8_t drop[kMaxDropRows * kSmemRowBytes];
     int32_t spill[kSpillCols];
 };
-constexpr size_t kRulesDynSmem = 2 * sizeof(RulesSlot);
+static_assert(offsetof(RulesSlot, type) % 128 == 0 && offsetof(RulesSlot, drop) % 128 == 0 &&
+                  offsetof(RulesSlot, own_type) % 128 == 0 && offsetof(RulesSlot, solid) % 128 == 0,
+              "TMA destinations are 128-byte aligned");
+constexpr size_t kRulesDynSmem = 2 * sizeof(RulesSlot) + 128;
 
 // Bytes x-1 .. x+2 / x .. x+3 / x+1 .. x+4 of a staged row around the 4 cells at p (p = row start +
 // kRowOff + 4 * xq; the frame bytes sit at kRowOff - 1 and kRowOff + 64).
@@ -563,8 +615,10 @@ __device__ __forceinline__ uint32_t win_right(const uint8_t* p) {
 }
 
 __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaKernelArgs k) {
-    extern __shared__ __align__(16) uint8_t s_dyn[];
-    RulesSlot* slots = reinterpret_cast<RulesSlot*>(s_dyn);
+    extern __shared__ __align__(128) uint8_t s_dyn[];
+    // the slots start on a 128-byte boundary (TMA destinations); the launch adds 128 bytes of slack
+    RulesSlot* slots = reinterpret_cast<RulesSlot*>(s_dyn + ((128u - (smem_u32(s_dyn) & 127u)) & 127u));
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ unsigned s_flags[2];
     __shared__ unsigned s_wtot[kThreads / 32];
     __shared__ uint32_t s_sched_tile[kMaxDeferred];
@@ -574,7 +628,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     __shared__ unsigned long long s_red[2][kThreads / 32];
 
     CaCtrl* ctrl = k.ctrl;
-    if (ctrl->stop) return;
+    if (ctrl->stop || ctrl->error) return;
     const uint32_t t = ctrl->steps;
     const int cur = t & 1, nxt = cur ^ 1;
     const CaGeom& g = k.g;
@@ -593,11 +647,22 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     const bool erupting = (int64_t)t < (int64_t)k.eruption_steps;
     const uint32_t stamp = min(t, 65535u);
     const uint32_t live_mark = 2u * (t + 1u) + 1u;
-    if (tid == 0) s_flags[0] = s_flags[1] = 0;
+    // transaction bytes of one slot fill
+    const uint32_t tx_copy = kTileCells * (1 + 4 + 4 + 2 + 2);
+    const uint32_t tx_rules = kTileCells * (4 + 4 + 2 + 2) + kSmemRowBytes * halo_rows + (lava_mode ? kSmemRowBytes * drop_rows : 0);
+    if (tid == 0) {
+        s_flags[0] = s_flags[1] = 0;
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async();
+    }
+    __syncthreads();
 
     unsigned int my_active = 0, my_changed = 0, tiles_done = 0;
     int nsched = 0, rit = 0;  // rit: rules tiles so far (parity of s_flags)
     unsigned nbuf = 0;        // candidates in s_cand (block-uniform)
+    bool failed = false;      // a bounded wait ran out (block-uniform once set)
 
     auto flush_schedule = [&]() {
         __syncthreads();
@@ -619,90 +684,43 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     };
     auto tile_at = [&](uint64_t i) -> uint32_t { return k.dense ? (uint32_t)i : k.tile_list[cur][i]; };
 
-    // Issue the copies of one tile into a slot.  Frame bytes of the halo rows come through
-    // registers (edge / dedge, stored by the caller once they have arrived).
-    int edge_at = -1, dedge_at = -1;
-    uint8_t edge = kVoid;
-    int8_t dedge = -1;
-    auto stage = [&](RulesSlot& sl, uint32_t tile, bool rules) {
+    // Fill a slot: TMA boxes by thread 0 (the slot's earlier stores must have been read first),
+    // spill levels by the threads.
+    auto stage = [&](int s, uint32_t tile, bool rules) {
+        RulesSlot& sl = slots[s];
         int x0, y0, z0;
         tile_origin(g, tile, x0, y0, z0);
-        {  // state rows: flowId and temp 16 chunks of 16 B each, solidStep / arrivalStep 8 each
-            const int yy = y0 + ly, zz = z0 + lz;
-            if (yy < g.ny && zz < g.nz) {
-                const int64_t p = pidx(g, x0, yy, zz);
-                const int c = xq;
-                cp_async16(&sl.flow[row * kTileX + 4 * c], k.flow[cur] + p + 4 * c);
-                cp_async16(&sl.temp[row * kTileX + 4 * c], k.temp[cur] + p + 4 * c);
-                if (c < 8)
-                    cp_async16(&sl.solid[row * kTileX + 8 * c], k.solid[cur] + p + 8 * c);
-                else
-                    cp_async16(&sl.arrival[row * kTileX + 8 * (c - 8)], k.arrival[cur] + p + 8 * (c - 8));
+        if (tid == 0) {
+            bulk_wait_read_all();
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&s_bar[s], rules ? tx_rules : tx_copy);
+            tma_load_3d(sl.flow, &k.tm.flow[cur], x0, y0, z0, &s_bar[s]);
+            tma_load_3d(sl.temp, &k.tm.temp[cur], x0, y0, z0, &s_bar[s]);
+            tma_load_3d(sl.solid, &k.tm.solid[cur], x0, y0, z0, &s_bar[s]);
+            tma_load_3d(sl.arrival, &k.tm.arrival[cur], x0, y0, z0, &s_bar[s]);
+            if (rules) {
+                tma_load_3d(sl.type, &k.tm.halo_type[cur], x0 - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
+                if (lava_mode) tma_load_3d(sl.drop, &k.tm.drop, x0 - 16, y0 - hy_on, z0, &s_bar[s]);
+            } else {
+                tma_load_3d(sl.own_type, &k.tm.own_type[cur], x0, y0, z0, &s_bar[s]);
             }
         }
-        if (!rules) {
-            // own rows of the types only, in their halo positions
-            if (tid < 64) {
-                const int r = tid >> 2, ch = tid & 3;
-                const int rly = r % g.TY, rlz = r / g.TY;
-                const int yy = y0 + rly, zz = z0 + rlz;
-                uint8_t* dst = sl.type + hr_of(rly, rlz, hy_on, hz_on, HY) * kSmemRowBytes + kRowOff + 16 * ch;
-                if (yy < g.ny && zz < g.nz)
-                    cp_async16(dst, T + pidx(g, x0 + 16 * ch, yy, zz));
-                else
-                    *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
-            }
-            return;
-        }
-        if (tid < halo_rows * 4) {
-            const int r = tid >> 2, ch = tid & 3;
-            int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-            uint8_t* dst = sl.type + r * kSmemRowBytes + kRowOff + 16 * ch;
-            if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                cp_async16(dst, T + pidx(g, x0 + 16 * ch, yy, zz));
-            else
-                *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
-        }
-        if (tid < halo_rows * 2) {
-            const int r = tid >> 1, right = tid & 1;
-            int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-            int xx = right ? x0 + kTileX : x0 - 1;
-            edge = kVoid;
-            if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                edge = T[pidx(g, xx, yy, zz)];
-            edge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
-        }
-        if (!lava_mode) return;
-        {
-            const int c = tid - 144;  // threads 144 .. 239: the drop-depth rows (at most 24 x 4 chunks)
-            if (c >= 0 && c < drop_rows * 4) {
-                const int r = c >> 2, ch = c & 3;
-                int yy = y0 - hy_on + r % HY;
-                const int zz = z0 + r / HY;
-                int8_t* dst = sl.drop + r * kSmemRowBytes + kRowOff + 16 * ch;
-                if (zz < g.nz && halo_axis(yy, g.ny, g.per[1]))
-                    cp_async16(dst, k.drop + pidx(g, x0 + 16 * ch, yy, zz));
-                else
-                    *reinterpret_cast<uint4*>(dst) = make_uint4(~0u, ~0u, ~0u, ~0u);
-            }
-            const int de = tid - 128;  // threads 128 .. 175: their frame bytes
-            if (de >= 0 && de < drop_rows * 2) {
-                const int r = de >> 1, right = de & 1;
-                int yy = y0 - hy_on + r % HY;
-                const int zz = z0 + r / HY;
-                int xx = right ? x0 + kTileX : x0 - 1;
-                dedge = -1;
-                if (zz < g.nz && halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) dedge = k.drop[pidx(g, xx, yy, zz)];
-                dedge_at = r * kSmemRowBytes + (right ? kRowOff + kTileX : kRowOff - 1);
-            }
-        }
-        if (stage_spill && tid < kTileX * g.TY) {
+        if (rules && stage_spill && tid < kTileX * g.TY) {
             const int xx = x0 + (tid & (kTileX - 1)), yy = y0 + tid / kTileX;
             if (xx < g.nx && yy < g.ny)
                 cp_async4(&sl.spill[tid], k.spill + xx + (int64_t)g.nx * yy);
             else
                 sl.spill[tid] = 0;
         }
+    };
+    auto store_tile = [&](int s, int x0, int y0, int z0) {  // thread 0
+        RulesSlot& sl = slots[s];
+        tma_store_3d(&k.tm.own_type[nxt], x0, y0, z0, sl.own_type);
+        tma_store_3d(&k.tm.flow[nxt], x0, y0, z0, sl.flow);
+        tma_store_3d(&k.tm.temp[nxt], x0, y0, z0, sl.temp);
+        tma_store_3d(&k.tm.solid[nxt], x0, y0, z0, sl.solid);
+        tma_store_3d(&k.tm.arrival[nxt], x0, y0, z0, sl.arrival);
+        bulk_commit();
     };
 
     // control pipeline: tile ids of the next two iterations, the mark of the next
@@ -717,7 +735,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         vent_a = k.tile_flags[tile_a];
         if (i + G < count) tile_b = tile_at(i + G);
         if (i + 2 * G < count) tile_c = tile_at(i + 2 * G);
-        stage(slots[0], tile_a, mark_a == live_mark);
+        stage(0, tile_a, mark_a == live_mark);
     }
     cp_async_commit();
     if (i + G < count) {
@@ -726,17 +744,13 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     }
 
     for (int it = 0; i < count; i += G, ++it) {
-        RulesSlot& sl = slots[it & 1];
+        const int si = it & 1;
+        RulesSlot& sl = slots[si];
         const uint32_t tile = tile_a;
         const bool rules = mark_a == live_mark;
         const bool tile_vent = (vent_a & 2u) != 0;
-        // the frame bytes of this slot have arrived by now (loaded one iteration ago)
-        const int my_edge_at = edge_at, my_dedge_at = dedge_at;
-        const uint8_t my_edge = edge;
-        const int8_t my_dedge = dedge;
-        edge_at = dedge_at = -1;
-        // next tile's copies into the other slot, then the control loads of the tiles after it
-        if (i + G < count) stage(slots[(it + 1) & 1], tile_b, mark_b == live_mark);
+        // next tile into the other slot, then the control loads of the tiles after it
+        if (i + G < count) stage(si ^ 1, tile_b, mark_b == live_mark);
         cp_async_commit();
         uint32_t mark_c = 0, vent_c = 0, tile_d = 0;
         if (i + 2 * G < count) {
@@ -744,53 +758,108 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             vent_c = k.tile_flags[tile_c];
         }
         if (i + 3 * G < count) tile_d = tile_at(i + 3 * G);
-        cp_async_wait_prior();  // this slot's copies
-        if (my_edge_at >= 0) sl.type[my_edge_at] = my_edge;
-        if (my_dedge_at >= 0) sl.drop[my_dedge_at] = my_dedge;
-        __syncthreads();
 
         int x0, y0, z0;
         tile_origin(g, tile, x0, y0, z0);
         ++tiles_done;
-        const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
-        const bool valid = y < g.ny && z < g.nz;
-        const int64_t p = pidx(g, valid ? x : 0, valid ? y : 0, valid ? z : 0);
-        const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
-        const uint8_t* rowp = sl.type + hr * kSmemRowBytes + kRowOff + 4 * xq;
-        const uint32_t w = valid ? win_mid(rowp) : 0xFFFFFFFFu;
-        int4 f4 = *reinterpret_cast<const int4*>(&sl.flow[row * kTileX + 4 * xq]);
-        float4 t4 = *reinterpret_cast<const float4*>(&sl.temp[row * kTileX + 4 * xq]);
-        uint2 s2 = *reinterpret_cast<const uint2*>(&sl.solid[row * kTileX + 4 * xq]);
-        const uint2 a2 = *reinterpret_cast<const uint2*>(&sl.arrival[row * kTileX + 4 * xq]);
-
-        if (!rules) {
-            // No LAVA within one tile: nothing can change here, the cells go to the next buffer as they are.
-            if (valid) {
-                *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = w;
-                *reinterpret_cast<int4*>(k.flow[nxt] + p) = f4;
-                *reinterpret_cast<float4*>(k.temp[nxt] + p) = t4;
-                *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
-                *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
+        const uint32_t parity = (uint32_t)(it >> 1) & 1u;
+        const bool ok = mbar_wait(&s_bar[si], parity);
+        if (rules) cp_async_wait_prior();  // this thread's spill copies
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(&ctrl->error, 1);
+                // the copies of the next slot, if any were issued, before the block gives up
+                if (i + G < count) mbar_wait(&s_bar[si ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
             }
-            __syncthreads();  // the slot is refilled next iteration
+            failed = true;
+            break;
+        }
+        if (!rules) {
+            // No LAVA within one tile: nothing can change, the boxes go to the next buffer as they are.
+            if (tid == 0) {
+                fence_proxy_async();
+                store_tile(si, x0, y0, z0);
+            }
         } else {
-            if (g.per[0] && g.nx < g.P && x0 + kTileX > g.nx) {
-                // periodic x with padded rows: the frame cell x = nx inside the staged row is the copy of x = 0
-                const int b = g.nx - x0;
-                for (int r = tid; r < halo_rows; r += kThreads) {
+            const bool edge_tile = x0 == 0 || x0 + kTileX >= g.nx || (hy_on && (y0 == 0 || y0 + g.TY >= g.ny)) ||
+                                   (hz_on && (z0 == 0 || z0 + g.TZ >= g.nz));
+            if (edge_tile) {
+                // Frame cells of the staged rows.  Outside the tensor the TMA filled zeros; the
+                // reference's frame is VOID (absorbing) or the opposite layer (periodic,
+                // Boundary.hpp:75-131).  Rows outside in y or z are whole-row copies or VOID; the two
+                // frame bytes of every row and, for periodic x with padded rows, the copy of x = 0 at
+                // x = nx are recomputed one by one.  One round of loads, then the stores.
+                const int xpad = (g.per[0] && g.nx < g.P && x0 < g.nx && x0 + kTileX > g.nx) ? g.nx : -1;
+                const bool drop_wrap = lava_mode && (g.per[0] || g.per[1]);
+                int row_at = -1, frame_at = -1, drow_at = -1, dframe_at = -1;
+                uint4 row_v = make_uint4(~0u, ~0u, ~0u, ~0u), drow_v = row_v;
+                uint8_t frame_v = kVoid;
+                int8_t dframe_v = -1;
+                if (tid < halo_rows * 4) {
+                    const int r = tid >> 2, ch = tid & 3;
                     int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
-                    if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
-                        sl.type[r * kSmemRowBytes + kRowOff + b] = T[pidx(g, 0, yy, zz)];
+                    if (!(yy >= 0 && yy < g.ny && zz >= 0 && zz < g.nz)) {
+                        row_at = r * kSmemRowBytes + kRowOff + 16 * ch;
+                        if (halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                            row_v = *reinterpret_cast<const uint4*>(T + pidx(g, x0 + 16 * ch, yy, zz));
+                    }
                 }
-                if (lava_mode)
-                    for (int r = tid; r < drop_rows; r += kThreads) {
+                if (tid < halo_rows * 3) {
+                    const int r = tid / 3, which = tid % 3;
+                    int xx = which == 0 ? x0 - 1 : (which == 1 ? x0 + kTileX : xpad);
+                    int yy = y0 - hy_on + r % HY, zz = z0 - hz_on + r / HY;
+                    if (!(which == 2 && xpad < 0) &&
+                        !(xx >= 0 && xx < g.nx && yy >= 0 && yy < g.ny && zz >= 0 && zz < g.nz)) {
+                        frame_at = r * kSmemRowBytes + kRowOff + (xx - x0);
+                        if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                            frame_v = T[pidx(g, xx, yy, zz)];
+                    }
+                }
+                if (drop_wrap) {
+                    // drop depths are read only where the staged type is AIR: only periodic copies matter
+                    const int c = tid - 144;
+                    if (c >= 0 && c < drop_rows * 4) {
+                        const int r = c >> 2, ch = c & 3;
                         int yy = y0 - hy_on + r % HY;
                         const int zz = z0 + r / HY;
-                        if (zz < g.nz && halo_axis(yy, g.ny, g.per[1]))
-                            sl.drop[r * kSmemRowBytes + kRowOff + b] = k.drop[pidx(g, 0, yy, zz)];
+                        if (zz < g.nz && !(yy >= 0 && yy < g.ny) && halo_axis(yy, g.ny, g.per[1])) {
+                            drow_at = r * kSmemRowBytes + kRowOff + 16 * ch;
+                            drow_v = *reinterpret_cast<const uint4*>(k.drop + pidx(g, x0 + 16 * ch, yy, zz));
+                        }
                     }
+                    const int f = tid - 128;
+                    if (f >= 0 && f < drop_rows * 3) {
+                        const int r = f / 3, which = f % 3;
+                        int xx = which == 0 ? x0 - 1 : (which == 1 ? x0 + kTileX : xpad);
+                        int yy = y0 - hy_on + r % HY;
+                        const int zz = z0 + r / HY;
+                        const int at = r * kSmemRowBytes + kRowOff + (xx - x0);
+                        if (!(which == 2 && xpad < 0) && zz < g.nz && !(xx >= 0 && xx < g.nx && yy >= 0 && yy < g.ny) &&
+                            halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) {
+                            dframe_at = at;
+                            dframe_v = k.drop[pidx(g, xx, yy, zz)];
+                        }
+                    }
+                }
+                if (row_at >= 0) *reinterpret_cast<uint4*>(sl.type + row_at) = row_v;
+                if (drow_at >= 0) *reinterpret_cast<uint4*>(sl.drop + drow_at) = drow_v;
+                __syncthreads();  // frame bytes after the row copies (a frame byte of an outside row)
+                if (frame_at >= 0) sl.type[frame_at] = frame_v;
+                if (dframe_at >= 0) sl.drop[dframe_at] = dframe_v;
                 __syncthreads();
             }
+
+            const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
+            const bool valid = y < g.ny && z < g.nz;
+            const int64_t p = pidx(g, valid ? x : 0, valid ? y : 0, valid ? z : 0);
+            const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
+            const uint8_t* rowp = sl.type + hr * kSmemRowBytes + kRowOff + 4 * xq;
+            uint32_t w = valid ? win_mid(rowp) : 0xFFFFFFFFu;
+            if (x + 4 > g.nx) w |= 0xFFFFFFFFu << (8 * max(0, g.nx - x));  // padding cells stay VOID
+            const int cell = row * kTileX + 4 * xq;
+            int4 f4 = *reinterpret_cast<const int4*>(&sl.flow[cell]);
+            float4 t4 = *reinterpret_cast<const float4*>(&sl.temp[cell]);
+            uint2 s2 = *reinterpret_cast<const uint2*>(&sl.solid[cell]);
 
             bool any_lava = false, any_changed = false;
             unsigned nbas = 0, ncand = 0;
@@ -840,13 +909,14 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                     }
                 }
                 uint32_t acc = 0;
-                const int8_t* dropc = sl.drop + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
+                const uint8_t* dropc =
+                    reinterpret_cast<const uint8_t*>(sl.drop) + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
 #pragma unroll
                 for (int sy = -1; sy <= 1; ++sy) {
                     const unsigned bits = (k.side_mask >> (3 * (sy + 1))) & 7u;
                     if (!bits) continue;
                     const uint8_t* tp = rowp + sy * kSmemRowBytes;
-                    const uint8_t* dp = reinterpret_cast<const uint8_t*>(dropc) + sy * kSmemRowBytes;
+                    const uint8_t* dp = dropc + sy * kSmemRowBytes;
                     if (bits & 1u) acc = __vmaxs4(acc, win_left(dp) & __vcmpeq4(win_left(tp), 0u));
                     if (bits & 2u) acc = __vmaxs4(acc, win_mid(dp) & __vcmpeq4(win_mid(tp), 0u));
                     if (bits & 4u) acc = __vmaxs4(acc, win_right(dp) & __vcmpeq4(win_right(tp), 0u));
@@ -888,17 +958,11 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                             }
                         }
                     }
-                    t4 = make_float4(te[0], te[1], te[2], te[3]);
-                    s2 = make_uint2(so[0], so[1]);
+                    *reinterpret_cast<float4*>(&sl.temp[cell]) = make_float4(te[0], te[1], te[2], te[3]);
+                    *reinterpret_cast<uint2*>(&sl.solid[cell]) = make_uint2(so[0], so[1]);
                 }
             }
-            if (valid) {
-                *reinterpret_cast<uint32_t*>(k.type[nxt] + p) = wout;
-                *reinterpret_cast<int4*>(k.flow[nxt] + p) = f4;
-                *reinterpret_cast<float4*>(k.temp[nxt] + p) = t4;
-                *reinterpret_cast<uint2*>(k.solid[nxt] + p) = s2;
-                *reinterpret_cast<uint2*>(k.arrival[nxt] + p) = a2;
-            }
+            *reinterpret_cast<uint32_t*>(&sl.own_type[cell]) = wout;
             if (__any_sync(0xFFFFFFFFu, nbas != 0))
                 warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, nbas, bas);
 
@@ -913,7 +977,9 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
             bits = __reduce_or_sync(0xFFFFFFFFu, bits);
             if (lane == 0 && bits) atomicOr(&s_flags[rit & 1], bits);
-            __syncthreads();  // also: the slot is refilled next iteration
+            fence_proxy_async();  // the slot's results are read by the TMA stores below
+            __syncthreads();
+            if (tid == 0) store_tile(si, x0, y0, z0);
             const unsigned tf = s_flags[rit & 1];
             if (tid == 32) s_flags[(rit + 1) & 1] = 0;
             ++rit;
@@ -942,6 +1008,12 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         tile_c = tile_d;
     }
     cp_async_wait_all();
+    if (tid == 0) {
+        // every slot fill that was issued has completed or is abandoned with the error flag set; the
+        // stores must have left shared memory before the block exits
+        bulk_wait_all();
+    }
+    if (failed) return;
     if (__syncthreads_or(nsched > 0)) flush_schedule();
     if (nbuf) flush_cands();
 
@@ -975,7 +1047,7 @@ __global__ __launch_bounds__(kCandThreads, 6) void ca_cand_kernel(const __grid_c
     __shared__ unsigned long long s_red[kCandThreads / 32];
     __shared__ bool s_last;
     CaCtrl* ctrl = k.ctrl;
-    if (ctrl->stop) return;
+    if (ctrl->stop || ctrl->error) return;
     const uint32_t t = ctrl->steps;
     const int cur = t & 1, nxt = cur ^ 1;
     const CaGeom& g = k.g;
@@ -1217,6 +1289,7 @@ CaKernelArgs make_args(const vca_ca* h) {
         k.tile_list[b] = h->tile_list[b];
     }
     k.tile_flags = h->tile_flags;
+    k.tm = h->tmaps;
     k.tile_mark[0] = h->tile_mark[0];
     k.tile_mark[1] = h->tile_mark[1];
     k.desc = h->desc_plane;
@@ -1255,6 +1328,10 @@ vca_status sync_ctrl(vca_ca* h) {
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->steps = (int)h->ctrl_host->steps;
     h->stop = h->ctrl_host->stop;
+    if (h->ctrl_host->error) {
+        set_error("vca_ca: a bounded device wait (TMA tile copy) ran out; the run was stopped");
+        return VCA_ERR_TIMEOUT;
+    }
     return VCA_OK;
 }
 
@@ -1346,7 +1423,7 @@ vca_status run_graphs(vca_ca* h, const CaKernelArgs& k) {
         h->launches += 3 * kGraphSteps;
         if (pending >= 0) {
             VCA_CUDA(cudaEventSynchronize(h->ring_ev[pending]));
-            if (h->ctrl_ring[pending].stop != VCA_STOP_RUNNING) break;
+            if (h->ctrl_ring[pending].stop != VCA_STOP_RUNNING || h->ctrl_ring[pending].error) break;
         }
         pending = slot;
         if (launched > 65536 / kGraphSteps + 4) break;  // max_steps <= 65535: cannot be reached
@@ -1455,6 +1532,64 @@ void free_all(vca_ca* h) {
     drop_graph(h);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                   const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// A pitched plane as a 3D tensor (P, ny, nz) of elem-byte cells with a box of (bx, by, bz) cells.
+vca_status encode_plane(CUtensorMap* m, CUtensorMapDataType type, size_t elem, void* base, const CaGeom& g, uint32_t bx,
+                        uint32_t by, uint32_t bz, const char* what) {
+    const EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("vca_ca_create: cuTensorMapEncodeTiled is not available from the driver");
+        return VCA_ERR_CUDA;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)g.P, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.P * elem, (cuuint64_t)g.P * g.ny * elem};
+    const cuuint32_t box[3] = {bx, by, bz};
+    const cuuint32_t step[3] = {1, 1, 1};
+    const CUresult r = fn(m, type, 3, base, dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error(std::string("vca_ca_create: cuTensorMapEncodeTiled failed for ") + what + " (CUresult " + std::to_string((int)r) + ")");
+        return VCA_ERR_CUDA;
+    }
+    return VCA_OK;
+}
+
+// Tensor maps of the rules pass (boxes of one 64 x TY x TZ tile, halo rows 96 bytes from x0 - 16).
+vca_status encode_maps(vca_ca* h) {
+    const CaGeom& g = h->geom;
+    CaTensorMaps& m = h->tmaps;
+    const uint32_t TY = (uint32_t)g.TY, TZ = (uint32_t)g.TZ;
+    const uint32_t HY = g.ny > 1 ? TY + 2 : 1, HZ = g.nz > 1 ? TZ + 2 : 1;
+    for (int b = 0; b < 2; ++b) {
+        if (vca_status s = encode_plane(&m.own_type[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->type[b], g, kTileX, TY, TZ, "type")) return s;
+        if (vca_status s = encode_plane(&m.halo_type[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->type[b], g, kTileX + 32, HY, HZ, "type halo"))
+            return s;
+        if (vca_status s = encode_plane(&m.flow[b], CU_TENSOR_MAP_DATA_TYPE_INT32, 4, h->flow[b], g, kTileX, TY, TZ, "flowId")) return s;
+        if (vca_status s = encode_plane(&m.temp[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->temp[b], g, kTileX, TY, TZ, "temp")) return s;
+        if (vca_status s = encode_plane(&m.solid[b], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->solid[b], g, kTileX, TY, TZ, "solidStep"))
+            return s;
+        if (vca_status s = encode_plane(&m.arrival[b], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->arrival[b], g, kTileX, TY, TZ, "arrivalStep"))
+            return s;
+    }
+    return encode_plane(&m.drop, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->drop_plane, g, kTileX + 32, HY, TZ, "drop depth");
 }
 
 vca_status upload_vents(vca_ca* h, const vca_vent* vents, int count) {
@@ -1619,6 +1754,8 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     ALLOC(h->hist_active, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
     ALLOC(h->hist_changed, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
 #undef ALLOC
+    if ((e = cudaMemsetAsync(h->drop_plane, 0xFF, n, h->stream)) != cudaSuccess) return fail(cuda_fail(e, "cudaMemsetAsync"));
+    if (vca_status st = encode_maps(h)) return fail(st);
     e = cudaMallocHost(&h->ctrl_host, sizeof(CaCtrl));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
     for (int b = 0; b < 2; ++b) {

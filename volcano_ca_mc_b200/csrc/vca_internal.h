@@ -1,6 +1,7 @@
 // vca_internal.h -- handle layouts and helpers shared by the CA and MC halves of libvca.so.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point, no libcuda link)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -43,7 +44,7 @@ struct CaCtrl {
     int32_t max_steps;
     int32_t random_nb;
     int32_t classic;
-    int32_t pad2;
+    int32_t error;            // bit 0: a bounded device wait ran out (the run stops, VCA_ERR_TIMEOUT)
 };
 
 // Geometry of the pitched device planes.  Each (y, z) row holds P >= nx cells, P a multiple of 64,
@@ -62,7 +63,15 @@ struct CaTables {
     int8_t side[8][3];        // union of the dz == 0 offsets of all variants (LavaCA.hpp:104-112)
 };
 
+// TMA descriptors of the pitched planes, seen as 3D tensors (P, ny, nz): per buffer the tile's own
+// box {64, TY, TZ} of each plane, the type halo box {96, TY + 2, TZ + 2} from (x0 - 16, y0 - 1,
+// z0 - 1), and the drop-depth rows {96, TY + 2, TZ} from (x0 - 16, y0 - 1, z0).
+struct CaTensorMaps {
+    CUtensorMap own_type[2], halo_type[2], flow[2], temp[2], solid[2], arrival[2], drop;
+};
+
 struct CaKernelArgs {
+    CaTensorMaps tm;
     CaGeom g;
     int classic;
     int ponding;
@@ -111,6 +120,7 @@ vca_status ca_view(vca_ca* h, CaView* v);
 }  // namespace vca
 
 struct vca_ca {
+    vca::CaTensorMaps tmaps;  // first member: CUtensorMap needs 64-byte alignment
     vca_ca_desc desc;
     vca::CaGeom geom;
     vca::CaTables tables_host;
