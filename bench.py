@@ -12,10 +12,16 @@ handle is set up beforehand); L2 is flushed before every job outside the job's d
                  default), whole job over all ranks.
   mc             MC trials/s and attempts/s of the same jobs (attempts exclude mobility skips).
   dense          the same jobs with the DENSE schedule (every cell every step).
-  roofline       the rules kernel: 26 B per processed cell (13 B state read + 13 B written) over
-                 its CUDA-event launch time, against the measured HBM copy bandwidth.
-  e2e            CA cell-updates/s through the C ABI from host heights/vents to host planes
-                 (allocation, uploads, run, download of all five planes inside the timed region).
+  roofline       the rules kernel of the DENSE jobs: 26 B per cell (13 B state read + 13 B written)
+                 over its CUDA-event launch time, against the measured HBM copy bandwidth; traffic =
+                 the ncu DRAM bytes per launch recorded in profiles/.  roofline_active: the same for
+                 the ACTIVE jobs (26 B per cell of the processed tiles).
+  kernels_ms     device time per step of the drop-depth, rules and candidate kernels.
+  large          the full-size workload c3 (1024 x 1024 x 256, random pentagonal, 800 steps, 200 MCS):
+                 one ACTIVE job with its MC, one DENSE job, the DENSE rules-kernel roofline.
+  e2e            CA cell-updates/s through the C ABI on one resident handle: reset, terrain and vents
+                 from host memory, run, the five planes back into pinned host memory.
+  engine_cli     the engine command on one job of the workload, its times.json sections.
   cpu_baseline   the reference engine (oracle/_ref/engine, --threads = host cores) on one job.
 
 With --impl reference the reference engine itself is timed on the host cores (rank 0 only).
@@ -48,6 +54,7 @@ def parse():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large", action="store_true", help="skip the full-size 1024x1024x256 sub-benchmark")
     ap.add_argument("--profile-job", choices=["active", "dense"], default=None,
                     help="run exactly one CA job with this schedule (no warm-up, no MC) and exit: the case "
                          "ncu captures")
@@ -59,6 +66,21 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def ncu_traffic(kernel: str, workload: str, schedule: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summaries (profiles/*.md lines
+    `traffic: kernel=<k> workload=<w> schedule=<s> bytes_per_launch=<n>`), or None."""
+    import glob
+    import re
+    pat = re.compile(r"traffic:\s*kernel=(\S+)\s+workload=(\S+)\s+schedule=(\S+)\s+bytes_per_launch=(\d+)")
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for line in f:
+                m = pat.search(line)
+                if m and m.group(1) == kernel and m.group(2) == workload and m.group(3) == schedule:
+                    return int(m.group(4))
+    return None
 
 
 def measured_peaks():
@@ -154,7 +176,7 @@ class L2Flush:
         torch.cuda.synchronize()
 
 
-def run_job(w, sweep, device, flush, profile=False):
+def run_job(w, sweep, device, flush, profile=False, mc=True):
     """One job with resident inputs; returns device-timed figures."""
     from volcano_ca_mc_b200 import capi
     if profile:
@@ -170,7 +192,7 @@ def run_job(w, sweep, device, flush, profile=False):
     ca_ms, rules_ms, rules_n = ca.timing()
     info = ca.info()
     mc_out = None
-    if not profile:
+    if not profile and mc:
         mc = capi.PottsMC(mc_params(w, device))
         mc.set_domain_from_ca(ca)
         mc.set_mobility_from_ca(ca, 0.05, True)
@@ -185,27 +207,44 @@ def run_job(w, sweep, device, flush, profile=False):
     out = {"ca_ms": ca_ms, "steps": info.steps, "stop": info.stop_reason, "tiles": info.tiles_processed,
            "cells_per_tile": info.cells_per_tile, "tiles_total": info.tiles_total, "launches": info.kernel_launches,
            "rules_ms": rules_ms, "rules_n": rules_n, "mc": mc_out}
+    if profile:
+        out["kernels"] = ca.kernel_times()
     ca.close()
     return out
 
 
-def run_e2e(w, device):
-    """Host buffers in, host planes out, through the C ABI (the call sequence an engine makes)."""
-    import numpy as np
-    from volcano_ca_mc_b200 import capi
-    n = w.cells
-    t0 = time.perf_counter()
-    ca = capi.LavaCA(ca_params(w, capi.SWEEP_ACTIVE, device))
-    ca.apply_terrain(w.heights)
-    ca.place_seeds(w.vent_cells())
-    ca.run()
-    planes = ca.download()
-    steps = ca.info().steps
-    t1 = time.perf_counter()
-    ca.close()
-    h2d = w.heights.nbytes + 16 * len(w.vents) + 13 * len(w.vents)
-    d2h = sum(int(np.asarray(p).nbytes) for p in planes)
-    return (t1 - t0) * 1e3, steps, h2d, d2h, n
+class E2E:
+    """The call sequence of a job through the C ABI on one resident handle: reset, terrain and vents
+    from host memory, run to the stop rule, all five planes back into pinned host memory.  The handle
+    and the pinned buffers are set up once, outside the timed steps."""
+
+    def __init__(self, w, device):
+        import torch
+        from volcano_ca_mc_b200 import capi
+        self.w = w
+        self.ca = capi.LavaCA(ca_params(w, capi.SWEEP_ACTIVE, device))
+        n = w.cells
+        pin = lambda dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()
+        self.out = (pin(torch.uint8), pin(torch.int32), pin(torch.float32), pin(torch.int16).view("uint16"),
+                    pin(torch.int16).view("uint16"))
+        self.heights = torch.from_numpy(w.heights.copy()).pin_memory().numpy()
+
+    def step(self):
+        """One job; returns (ms, steps)."""
+        t0 = time.perf_counter()
+        self.ca.reset()
+        self.ca.apply_terrain(self.heights)
+        self.ca.place_seeds(self.w.vent_cells())
+        self.ca.run()
+        self.ca.download(self.out)
+        steps = self.ca.info().steps
+        return (time.perf_counter() - t0) * 1e3, steps
+
+    def bytes(self):
+        return self.heights.nbytes + 16 * len(self.w.vents), sum(int(a.nbytes) for a in self.out)
+
+    def close(self):
+        self.ca.close()
 
 
 def cpu_baseline(w):
@@ -296,20 +335,44 @@ def ours(args):
     prof_dense = run_job(w, capi.SWEEP_DENSE, local, flush, profile=True)
     peak, peak_kind = measured_peaks()
 
-    def roof(p):
+    def roof(p, wl_name, schedule):
         cells = p["tiles"] * p["cells_per_tile"] / max(1, p["rules_n"])
         bytes_per_launch = BYTES_PER_CELL_UPDATE * cells
         ach = bytes_per_launch / (p["rules_ms"] * 1e-3) / 1e9 if p["rules_ms"] > 0 else 0.0
         return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
-                "traffic": None, "kernel": "ca_rules_kernel", "launch_ms": round(p["rules_ms"], 5),
-                "bytes_per_launch": int(bytes_per_launch), "launches": p["rules_n"], "peak_kind": peak_kind}
+                "traffic": ncu_traffic("ca_rules_kernel", wl_name, schedule), "kernel": "ca_rules_kernel",
+                "schedule": schedule, "launch_ms": round(p["rules_ms"], 5), "bytes_per_launch": int(bytes_per_launch),
+                "launches": p["rules_n"], "peak_kind": peak_kind,
+                "note": "26 B per cell of the processed tiles (13 B state read + 13 B written); frac of measured HBM copy "
+                        "bandwidth; traffic = ncu dram bytes read+write per launch (profiles/)"}
 
-    roof_active, roof_dense = roof(prof), roof(prof_dense)
+    roof_active, roof_dense = roof(prof, w.name, "active"), roof(prof_dense, w.name, "dense")
 
-    # e2e through host buffers
-    e2e_runs = [run_e2e(w, local) for _ in range(max(1, min(3, args.steps)))]
+    # the full-size 3D workload: one ACTIVE job (CA + MC), one DENSE job, one DENSE job with per-kernel events
+    large = None
+    if not args.no_large:
+        wl3 = workloads.get("c3")
+        j3 = run_job(wl3, capi.SWEEP_ACTIVE, local, flush)
+        d3 = run_job(wl3, capi.SWEEP_DENSE, local, flush, mc=False)
+        p3 = run_job(wl3, capi.SWEEP_DENSE, local, flush, profile=True)
+        m3 = j3["mc"]
+        large = {"workload": f"{wl3.name}: {wl3.description}", "grid": [wl3.nx, wl3.ny, wl3.nz], "ca_steps": j3["steps"],
+                 "value": wl3.cells * j3["steps"] / (j3["ca_ms"] * 1e-3), "unit": "cell-updates/s",
+                 "ms_per_job": j3["ca_ms"],
+                 "dense": {"value": wl3.cells * d3["steps"] / (d3["ca_ms"] * 1e-3), "ms_per_job": d3["ca_ms"]},
+                 "roofline": roof(p3, wl3.name, "dense"), "kernels_dense_ms": p3["kernels"],
+                 "mc": {"attempts_per_s": m3["attempts"] / (m3["ms"] * 1e-3), "trials_per_s": m3["trials"] / (m3["ms"] * 1e-3),
+                        "ms_per_job": m3["ms"], "domain_cells": m3["domain_cells"],
+                        "hbm_frac_12B_per_trial": round(BYTES_PER_TRIAL * m3["trials"] / (m3["ms"] * 1e-3) / 1e9 / peak, 4)}}
+
+    # e2e through the C ABI with host buffers, on a resident handle
+    e2e = E2E(w, local)
+    e2e.step()  # warm-up
+    e2e_runs = [e2e.step() for _ in range(max(1, min(3, args.steps)))]
     e2e_ms = sum(r[0] for r in e2e_runs)
-    e2e_cu = sum(r[1] * r[4] for r in e2e_runs)
+    e2e_cu = sum(r[1] * w.cells for r in e2e_runs)
+    e2e_h2d, e2e_d2h = e2e.bytes()
+    e2e.close()
 
     vals = torch.tensor([ca_ms, mc_ms, dense_ms, e2e_ms, wall * 1e3], dtype=torch.float64, device=f"cuda:{local}")
     if world > 1:
@@ -343,17 +406,21 @@ def ours(args):
                "trials_per_s": world * trials / (mc_ms * 1e-3), "ms_per_job": mc_ms / args.steps,
                "domain_cells": jobs[0]["mc"]["domain_cells"],
                "hbm_frac_12B_per_trial": round(BYTES_PER_TRIAL * trials / (mc_ms * 1e-3) / 1e9 / peak, 4)},
-        "dense": {"value": world * dense_cu / (dense_ms * 1e-3), "ms_per_step": dense_ms / len(dense),
-                  "roofline": roof_dense},
-        "roofline": roof_active,
+        "dense": {"value": world * dense_cu / (dense_ms * 1e-3), "ms_per_step": dense_ms / len(dense)},
+        "roofline": roof_dense,
+        "roofline_active": roof_active,
+        "kernels_ms": {"active": prof["kernels"], "dense": prof_dense["kernels"]},
         "active_tiles_frac": round(prof["tiles"] / max(1, prof["tiles_total"] * prof["steps"]), 4),
         "e2e": {"value": world * e2e_cu / (e2e_ms * 1e-3), "unit": "cell-updates/s",
-                "h2d_bytes_per_step": e2e_runs[0][2], "d2h_bytes_per_step": e2e_runs[0][3],
-                "ms_per_step": e2e_ms / len(e2e_runs)},
+                "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h, "ms_per_step": e2e_ms / len(e2e_runs),
+                "path": "vca_ca_reset + apply_terrain (host priority flood + upload) + place_seeds + run + download of "
+                        "the five planes into pinned memory, one resident handle, host wall clock"},
         "gpu_launches": launches,
         "clocks": clocks,
         "wall_s_timed_loop": round(wall_ms / 1e3, 3),
     }
+    if large is not None:
+        line["large"] = large
     if eng is not None:
         line["engine_cli"] = eng
     if cpu is not None:

@@ -100,6 +100,10 @@ typedef struct {
 
 /* LavaCA ctor (LavaCA.hpp:84-144): all cells AIR, buffers on the device. */
 vca_status vca_ca_create(const vca_ca_desc* desc, vca_ca** out);
+/* Back to the state of a new handle (all cells AIR, no terrain, no vents, step 0) without
+ * freeing or allocating device memory, so that one resident handle can run job after job of the
+ * same dimensions.  No counterpart in the reference (it builds a new LavaCA per run). */
+vca_status vca_ca_reset(vca_ca* ca);
 /* LavaCA::applyTerrain (LavaCA.hpp:185-211): ROCK for z < h(x,y); spill levels by priority flood
  * (TerrainGenerator::fillDepressions, engine/src/terrain/TerrainGenerator.cpp:86-161).
  * heights: nx*ny values, x fastest.  Lava mode only. */

@@ -142,3 +142,37 @@ def test_set_state_resumes():
         ca.step()
         assert C.state_diff(s, ca.download()) == "", f"step {t + 1}"
     ca.close()
+
+
+def test_reset_reuses_handle():
+    """vca_ca_reset: a handle that ran one job runs the next one (other terrain, other vents) exactly
+    like a new handle, and the first job again exactly as before."""
+    nx, ny, nz = 40, 24, 20
+    jobs = []
+    for seed in (7, 8):
+        heights = C.terrain(nx, ny, nz, seed)
+        vents = C.pick_vents(heights, nx, ny, nz, 2, seed)
+        jobs.append((heights, vents))
+    p = _params(nx, ny, nz, "moore", "periodic", 5000, capi.SWEEP_ACTIVE, 3)
+    p.eruption_steps = 30
+
+    def run(ca, job):
+        ca.apply_terrain(job[0])
+        ca.place_seeds(job[1])
+        ca.run()
+        return ca.info().steps, ca.info().stop_reason, ca.history(), ca.download()
+
+    fresh = []
+    for job in jobs:
+        ca = capi.LavaCA(p)
+        fresh.append(run(ca, job))
+        ca.close()
+    ca = capi.LavaCA(p)
+    for n, k in enumerate((0, 1, 0)):
+        if n:
+            ca.reset()
+        got = run(ca, jobs[k])
+        assert got[:3] == fresh[k][:3]
+        for a, b in zip(got[3], fresh[k][3]):
+            assert np.array_equal(a, b)
+    ca.close()

@@ -24,7 +24,7 @@ STOP_NAMES = {0: "running", 1: "no lava", 2: "no air", 3: "no change", 4: "max s
 
 # Every entry point declared in include/vca.h.
 EXPORTS = [
-    "vca_ca_create", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
+    "vca_ca_create", "vca_ca_reset", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
     "vca_ca_get_info", "vca_ca_history", "vca_ca_download", "vca_ca_set_state", "vca_ca_get_spill",
     "vca_ca_timing", "vca_ca_kernel_times", "vca_ca_destroy",
     "vca_mc_create", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
@@ -89,7 +89,7 @@ def lib() -> ctypes.CDLL:
         raise VcaError(f"cannot load {LIB_PATH}: {e}") from e
     p, i32, u64, f64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_double
     sig = {
-        "vca_ca_create": [p, p], "vca_ca_apply_terrain": [p, p], "vca_ca_place_seeds": [p, p, i32],
+        "vca_ca_create": [p, p], "vca_ca_reset": [p], "vca_ca_apply_terrain": [p, p], "vca_ca_place_seeds": [p, p, i32],
         "vca_ca_step": [p, p], "vca_ca_run": [p], "vca_ca_get_info": [p, p],
         "vca_ca_history": [p, p, p, i32, p], "vca_ca_download": [p, p, p, p, p, p],
         "vca_ca_set_state": [p, p, p, p, p, p, p, p, i32, i32], "vca_ca_get_spill": [p, p],
@@ -178,6 +178,10 @@ class LavaCA:
         except Exception:
             pass
 
+    def reset(self) -> None:
+        """All cells AIR, no terrain, no vents, step 0 (device memory kept)."""
+        _check(lib().vca_ca_reset(self.h), "vca_ca_reset")
+
     def apply_terrain(self, heights: np.ndarray) -> None:
         h = np.ascontiguousarray(heights, np.int32)
         _check(lib().vca_ca_apply_terrain(self.h, _ptr(h)), "vca_ca_apply_terrain")
@@ -218,13 +222,14 @@ class LavaCA:
         _check(lib().vca_ca_history(self.h, _ptr(a), _ptr(c), steps, ctypes.byref(cnt)), "vca_ca_history")
         return [int(v) for v in a[:steps]], [int(v) for v in c[:steps]]
 
-    def download(self):
+    def download(self, out=None):
+        """The five planes (type, flowId, temp, solidStep, arrivalStep) in globalIndex order, into new
+        arrays or into ``out`` (five C-contiguous arrays of those dtypes, e.g. views of pinned memory)."""
         n = self.n
-        t = np.empty(n, np.uint8)
-        f = np.empty(n, np.int32)
-        te = np.empty(n, np.float32)
-        s = np.empty(n, np.uint16)
-        a = np.empty(n, np.uint16)
+        if out is None:
+            out = (np.empty(n, np.uint8), np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.uint16),
+                   np.empty(n, np.uint16))
+        t, f, te, s, a = out
         _check(lib().vca_ca_download(self.h, _ptr(t), _ptr(f), _ptr(te), _ptr(s), _ptr(a)), "vca_ca_download")
         return t, f, te, s, a
 

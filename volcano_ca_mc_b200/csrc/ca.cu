@@ -1519,6 +1519,7 @@ void free_all(vca_ca* h) {
     cudaFree(h->chg_list[1]);
     cudaFree(h->cand_list);
     cudaFree(h->spill);
+    cudaFree(h->heights_dev);
     cudaFree(h->vents);
     cudaFree(h->ctrl);
     cudaFree(h->hist_active);
@@ -1532,6 +1533,28 @@ void free_all(vca_ca* h) {
     drop_graph(h);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// All cells AIR (padding VOID), drop depths and D(n) -1, no tile scheduled: the state of a new handle.
+vca_status clear_planes(vca_ca* h) {
+    const auto& g = h->geom;
+    const size_t n = h->plane_cells;
+    for (int b = 0; b < 2; ++b) {
+        VCA_CUDA(cudaMemsetAsync(h->type[b], 0, n, h->stream));
+        VCA_CUDA(cudaMemsetAsync(h->flow[b], 0, n * 4, h->stream));
+        VCA_CUDA(cudaMemsetAsync(h->temp[b], 0, n * 4, h->stream));
+        VCA_CUDA(cudaMemsetAsync(h->solid[b], 0, n * 2, h->stream));
+        VCA_CUDA(cudaMemsetAsync(h->arrival[b], 0, n * 2, h->stream));
+    }
+    VCA_CUDA(cudaMemsetAsync(h->drop_plane, 0xFF, n, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->desc_plane, 0xFF, n, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->tile_mark[0], 0, h->ntiles * 4, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->tile_mark[1], 0, h->ntiles * 4, h->stream));
+    if (g.P > g.nx) {
+        ca_pad_kernel<<<256, 256, 0, h->stream>>>(h->type[0], h->type[1], g.nx, g.P, (int64_t)g.ny * g.nz);
+        VCA_CUDA(cudaGetLastError());
+    }
+    return VCA_OK;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
@@ -1758,23 +1781,7 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     if (vca_status st = encode_maps(h)) return fail(st);
     e = cudaMallocHost(&h->ctrl_host, sizeof(CaCtrl));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
-    for (int b = 0; b < 2; ++b) {
-        if ((e = cudaMemsetAsync(h->type[b], 0, n, h->stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(h->flow[b], 0, n * 4, h->stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(h->temp[b], 0, n * 4, h->stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(h->solid[b], 0, n * 2, h->stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(h->arrival[b], 0, n * 2, h->stream)) != cudaSuccess)
-            return fail(cuda_fail(e, "cudaMemsetAsync"));
-    }
-    if ((e = cudaMemsetAsync(h->drop_plane, 0xFF, n, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->desc_plane, 0xFF, n, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->tile_mark[0], 0, h->ntiles * 4, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->tile_mark[1], 0, h->ntiles * 4, h->stream)) != cudaSuccess)
-        return fail(cuda_fail(e, "cudaMemsetAsync"));
-    if (g.P > nx) {
-        ca_pad_kernel<<<256, 256, 0, h->stream>>>(h->type[0], h->type[1], nx, g.P, (int64_t)ny * nz);
-        if ((e = cudaGetLastError()) != cudaSuccess) return fail(cuda_fail(e, "ca_pad_kernel"));
-    }
+    if (vca_status st = clear_planes(h)) return fail(st);
     int per_sm = 0;
     e = cudaFuncSetAttribute(ca_rules_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRulesDynSmem);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
@@ -1800,6 +1807,20 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     return VCA_OK;
 }
 
+vca_status vca_ca_reset(vca_ca* h) {
+    if (vca_status s = check(h)) return s;
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (vca_status s = clear_planes(h)) return s;
+    vca_vent none{0, 0, 0, 0};
+    if (vca_status s = upload_vents(h, &none, 0)) return s;  // synchronizes the stream
+    drop_graph(h);
+    h->has_terrain = false;
+    h->seeded = false;
+    h->steps = 0;
+    h->stop = VCA_STOP_RUNNING;
+    return VCA_OK;
+}
+
 vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
     if (vca_status s = check(h)) return s;
     if (heights == nullptr) {
@@ -1822,15 +1843,13 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
     }
     const std::vector<int32_t> spill = fill_depressions(hv, g.nx, g.ny, g.per[0] != 0, g.per[1] != 0);
     if (h->spill == nullptr) VCA_CUDA(cudaMalloc(&h->spill, sizeof(int32_t) * cols));
-    int32_t* dh = nullptr;
-    VCA_CUDA(cudaMalloc(&dh, sizeof(int32_t) * cols));
-    VCA_CUDA(cudaMemcpyAsync(dh, hv.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
+    if (h->heights_dev == nullptr) VCA_CUDA(cudaMalloc(&h->heights_dev, sizeof(int32_t) * cols));
+    VCA_CUDA(cudaMemcpyAsync(h->heights_dev, hv.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->spill, spill.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
     const int cur = h->steps & 1;
-    ca_terrain_kernel<<<1184, 256, 0, h->stream>>>(h->type[cur], dh, g.nx, g.ny, g.nz, g.P);
+    ca_terrain_kernel<<<1184, 256, 0, h->stream>>>(h->type[cur], h->heights_dev, g.nx, g.ny, g.nz, g.P);
     VCA_CUDA(cudaGetLastError());
     VCA_CUDA(cudaStreamSynchronize(h->stream));
-    cudaFree(dh);
     h->has_terrain = true;
     h->launches += 1;
     drop_graph(h);

@@ -151,6 +151,7 @@ struct vca_ca {
     uint32_t* tile_list[2] = {nullptr, nullptr};
     unsigned long long* hist_active = nullptr;
     unsigned long long* hist_changed = nullptr;
+    int32_t* heights_dev = nullptr;  // nx*ny heights of the last apply_terrain
     bool has_terrain = false;
     bool seeded = false;
     // host mirror of the control state after the last sync
