@@ -68,6 +68,18 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(values, device, world):
+    """Element-wise maximum of per-rank timings over all ranks (the job is as slow as its slowest
+    replica); a no-op for one rank.  The process group must be initialised when world > 1."""
+    if world <= 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def ncu_traffic(kernel: str, workload: str, schedule: str):
     """DRAM bytes per launch of a kernel from the committed ncu summaries (profiles/*.md lines
     `traffic: kernel=<k> workload=<w> schedule=<s> bytes_per_launch=<n>`), or None."""
@@ -374,10 +386,8 @@ def ours(args):
     e2e_h2d, e2e_d2h = e2e.bytes()
     e2e.close()
 
-    vals = torch.tensor([ca_ms, mc_ms, dense_ms, e2e_ms, wall * 1e3], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ca_ms, mc_ms, dense_ms, e2e_ms, wall_ms = vals.tolist()
+    ca_ms, mc_ms, dense_ms, e2e_ms, wall_ms = max_over_ranks([ca_ms, mc_ms, dense_ms, e2e_ms, wall * 1e3],
+                                                             f"cuda:{local}", world)
     cpu = None
     eng = None
     if rank == 0 and world == 1:
