@@ -48,6 +48,10 @@ struct McCtrl {
     unsigned long long uphill;
     unsigned long long energy_acc;
     unsigned long long sweep_accepted;  // accepted in the running sweep
+    unsigned int bar_count;             // grid barrier of the fused sweep kernel: arrivals
+    unsigned int bar_gen;               // and generation
+    int error;                          // bit 0: a bounded barrier wait ran out
+    int pad;
 };
 
 struct McArgs {
@@ -215,6 +219,135 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
     }
 }
 
+// Colour classes of the domain list: colour c is list[off[c] .. off[c + 1]).
+struct McColors {
+    int colors;
+    uint64_t off[28];
+};
+
+// Grid-wide barrier of a cooperative launch (all blocks resident): arrivals counted in ctrl, the
+// last arrival opens the next generation.  The wait is bounded; a block that gives up, or sees that
+// another gave up, returns false (ctrl->error is then set).
+__device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = &ctrl->bar_gen;
+        volatile int* err = &ctrl->error;
+        const unsigned g = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(&ctrl->bar_count, 1u) == nblocks - 1) {
+            atomicExch(&ctrl->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&ctrl->bar_gen, 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g) {
+                if (*err || ++spins > (1ll << 26)) {
+                    ok = 0;
+                    atomicOr(&ctrl->error, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// `sweeps` checkerboard MCS in one cooperative launch: the colour classes in ascending order
+// (sweepColors, PottsMC.cpp:495-514), a grid barrier after each, the same trial as mc_color_kernel
+// (colorTrials, PottsMC.cpp:394-493).  Replaces `sweeps` x `colors` launches; for domains of a few
+// hundred thousand cells the launches, not the trials, were the cost.
+template <bool kMobility, bool kRandomNb>
+__global__ __launch_bounds__(kMcThreads) void mc_sweeps_kernel(McArgs a, McColors col, int sweeps) {
+    __shared__ unsigned long long s_table[kTableSide * kTableSide];
+    __shared__ unsigned long long s_red[3][kMcThreads / 32];
+    for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
+    __syncthreads();
+    McCtrl* ctrl = a.ctrl;
+    const uint32_t t0 = ctrl->sweeps;
+    const NbTable& nb = *a.nb;
+    unsigned long long my_att = 0, my_acc = 0, my_up = 0;
+    bool ok = true;
+    for (int s = 0; s < sweeps && ok; ++s) {
+        const uint64_t prefix = hash_prefix(a.seed, t0 + (uint32_t)s);
+        for (int c = 0; c < col.colors && ok; ++c) {
+            const uint64_t b = col.off[c], e = col.off[c + 1];
+            for (uint64_t j = b + blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < e; j += (uint64_t)gridDim.x * kMcThreads) {
+                const uint32_t g = a.list[j];
+                const uint64_t h = hash_index(prefix, g);
+                if (kMobility) {
+                    const uint64_t r = hash_salt(h, kSaltMcMobility);
+                    if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)a.list_mob[j]) continue;
+                }
+                ++my_att;
+                int var = 0;
+                if (kRandomNb) var = (int)fast_mod(hash_salt(h, kSaltNeighborhood), a.var_mod);
+                int x, y, z;
+                decode(a, g, x, y, z);
+                const int32_t cur = a.spin[g];
+                int32_t prop = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
+                if (prop >= cur) ++prop;
+                int in_dom = 0, same_a = 0, same_b = 0;
+                const int cnt = nb.count[var];
+                for (int k = 0; k < cnt; ++k) {
+                    const int32_t sj = spin_at(a, x + nb.off[var][k][0], y + nb.off[var][k][1], z + nb.off[var][k][2]);
+                    in_dom += sj != 0;
+                    same_a += sj == cur;
+                    same_b += sj == prop;
+                }
+                const unsigned long long th = s_table[(in_dom - same_a) * kTableSide + (in_dom - same_b)];
+                bool accept;
+                if (th >> 63) {
+                    accept = true;
+                } else {
+                    accept = th != 0 && (hash_salt(h, kSaltMcAccept) >> 11) < th;
+                    my_up += accept ? 1u : 0u;
+                }
+                if (accept) {
+                    a.spin[g] = prop;
+                    ++my_acc;
+                }
+            }
+            ok = mc_grid_barrier(ctrl, gridDim.x);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long ra = my_att, rc = my_acc, ru = my_up;
+    for (int off = 16; off > 0; off >>= 1) {
+        ra += __shfl_down_sync(0xFFFFFFFFu, ra, off);
+        rc += __shfl_down_sync(0xFFFFFFFFu, rc, off);
+        ru += __shfl_down_sync(0xFFFFFFFFu, ru, off);
+    }
+    if (lane == 0) {
+        s_red[0][warp] = ra;
+        s_red[1][warp] = rc;
+        s_red[2][warp] = ru;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long sa = 0, sc = 0, su = 0;
+        for (int w = 0; w < kMcThreads / 32; ++w) {
+            sa += s_red[0][w];
+            sc += s_red[1][w];
+            su += s_red[2][w];
+        }
+        if (sa) atomicAdd(&ctrl->attempts, sa);
+        if (sc) {
+            atomicAdd(&ctrl->accepted, sc);
+            atomicAdd(&ctrl->sweep_accepted, sc);
+        }
+        if (su) atomicAdd(&ctrl->uphill, su);
+        // every block passed the last barrier, so no block reads ctrl->sweeps any more
+        if (blockIdx.x == 0 && ok) ctrl->sweeps = t0 + (uint32_t)sweeps;
+    }
+}
+
 // PottsMC::totalEnergy (PottsMC.cpp:590-664): unlike pairs.  Deterministic neighbourhoods count
 // each pair once through the forward offsets; random ones sum E_i over the cells with the
 // variant of MCS t (the caller halves it).
@@ -357,7 +490,6 @@ struct vca_mc {
     uint64_t launches = 0;
     int profile_kernels = 0;
     std::vector<cudaEvent_t> prof_events;
-    cudaGraphExec_t graph_exec = nullptr;  // the colour launches of one sweep (rebuilt by initialize)
 };
 
 namespace {
@@ -422,43 +554,25 @@ void mc_free(vca_mc* h) {
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
-// The colour passes of one MCS, launched on h->stream.
-void launch_sweep(vca_mc* h, const McArgs& a) {
+using SweepsKernel = void (*)(McArgs, McColors, int);
+
+SweepsKernel sweeps_kernel_for(const vca_mc* h) {
     const bool random_nb = h->nb_host.variants > 1;
-    for (int c = 0; c < h->colors; ++c) {
-        const uint64_t b = h->color_off[c], e = h->color_off[c + 1];
-        const uint64_t cnt = e - b;
-        const int grid = grid_for(cnt, h->sms);
-        const uint32_t* list = h->list + b;
-        const float* mob = h->mobility_on ? h->list_mob + b : nullptr;
-        const int last = c == h->colors - 1;
-        if (h->mobility_on) {
-            if (random_nb) mc_color_kernel<true, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
-            else mc_color_kernel<true, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
-        } else {
-            if (random_nb) mc_color_kernel<false, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
-            else mc_color_kernel<false, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
-        }
-    }
+    if (h->mobility_on) return random_nb ? mc_sweeps_kernel<true, true> : mc_sweeps_kernel<true, false>;
+    return random_nb ? mc_sweeps_kernel<false, true> : mc_sweeps_kernel<false, false>;
 }
 
-vca_status ensure_sweep_graph(vca_mc* h, const McArgs& a) {
-    if (h->graph_exec) return VCA_OK;
-    VCA_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    launch_sweep(h, a);
-    cudaGraph_t graph = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    const cudaError_t e2 = cudaGraphInstantiate(&h->graph_exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e2 != cudaSuccess) {
-        h->graph_exec = nullptr;
-        return cuda_fail(e2, "cudaGraphInstantiate");
-    }
+// Blocks of the cooperative sweep launch: all resident at once, no more than the largest colour needs.
+vca_status sweeps_grid(vca_mc* h, int* grid) {
+    int per_sm = 0;
+    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweeps_kernel_for(h), kMcThreads, 0));
+    uint64_t widest = 0;
+    for (int c = 0; c < h->colors; ++c) widest = std::max<uint64_t>(widest, h->color_off[c + 1] - h->color_off[c]);
+    const uint64_t need = (widest + kMcThreads - 1) / kMcThreads;
+    *grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * std::max(1, per_sm)));
     return VCA_OK;
 }
 
@@ -723,8 +837,6 @@ vca_status vca_mc_initialize(vca_mc* h) {
     cudaFree(all);
     VCA_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream));
     VCA_CUDA(cudaStreamSynchronize(h->stream));
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-    h->graph_exec = nullptr;
     h->initialized = true;
     return VCA_OK;
 }
@@ -743,16 +855,37 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
     McArgs a = mc_args(h);
     VCA_CUDA(cudaMemsetAsync(&h->ctrl->sweep_accepted, 0, 8, h->stream));
     if (!h->profile_kernels) {
-        if (vca_status s = ensure_sweep_graph(h, a)) return s;
+        // all sweeps in one cooperative launch (colour passes separated by grid barriers)
+        McColors col;
+        std::memset(&col, 0, sizeof(col));
+        col.colors = h->colors;
+        for (int c = 0; c <= h->colors; ++c) col.off[c] = h->color_off[c];
+        int grid = 1;
+        if (vca_status s = sweeps_grid(h, &grid)) return s;
         VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
-        for (int s = 0; s < count; ++s) VCA_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
-        h->launches += (uint64_t)count * (uint64_t)h->colors;
+        if (count > 0 && h->color_off.back() > 0) {
+            int n = count;
+            void* args[] = {&a, &col, &n};
+            VCA_CUDA(cudaLaunchCooperativeKernel((const void*)sweeps_kernel_for(h), grid, kMcThreads, args, 0, h->stream));
+            h->launches += 1;
+        } else if (count > 0) {
+            // empty domain: the sweeps still count (sweepsDone)
+            McCtrl* c = h->ctrl_host;
+            VCA_CUDA(cudaMemcpyAsync(c, h->ctrl, sizeof(McCtrl), cudaMemcpyDeviceToHost, h->stream));
+            VCA_CUDA(cudaStreamSynchronize(h->stream));
+            c->sweeps += (uint32_t)count;
+            VCA_CUDA(cudaMemcpyAsync(h->ctrl, c, sizeof(McCtrl), cudaMemcpyHostToDevice, h->stream));
+        }
         VCA_CUDA(cudaEventRecord(h->ev_b, h->stream));
         VCA_CUDA(cudaEventSynchronize(h->ev_b));
         float ms = 0.f;
         VCA_CUDA(cudaEventElapsedTime(&ms, h->ev_a, h->ev_b));
         h->total_ms += ms;
         if (vca_status s_ = mc_sync(h)) return s_;
+        if (h->ctrl_host->error) {
+            set_error("vca_mc_sweep: a bounded grid-barrier wait ran out");
+            return VCA_ERR_TIMEOUT;
+        }
         if (accepted) *accepted = h->ctrl_host->sweep_accepted;
         return VCA_OK;
     }
