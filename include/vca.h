@@ -195,6 +195,28 @@ vca_status vca_mc_sweep(vca_mc* mc, int count, uint64_t* accepted);
 vca_status vca_mc_get_info(vca_mc* mc, vca_mc_info* out);
 /* PottsMC::totalEnergy (PottsMC.cpp:590-664). */
 vca_status vca_mc_energy(vca_mc* mc, double* energy);
+/* Grain statistics of the current orientations (labelGrains, engine/src/mc/Grains.cpp:33-150, and
+ * the majority classes of McStage, engine/src/app/McStage.cpp:38-66): grains are connected sets of
+ * one orientation, Moore (moore != 0) or von Neumann connectivity, periodic axes as the sweep's.
+ * The high / low split uses the mobility values held by the handle (vca_mc_set_mobility*,
+ * vca_mc_set_mobility_from_ca): a grain is high when at least half of its cells have mobility >=
+ * mobility_threshold; without mobility values every grain is low. */
+typedef struct {
+    uint64_t grains;            /* grains */
+    uint64_t cells;             /* cells in grains (the domain) */
+    uint64_t largest;           /* cells of the largest grain */
+    uint64_t high_cells;        /* domain cells with mobility >= threshold */
+    uint64_t high_grains;       /* grains of the high class, their cells, the largest */
+    uint64_t high_grain_cells;
+    uint64_t high_largest;
+    uint64_t low_grains;        /* the same for the low class */
+    uint64_t low_grain_cells;
+    uint64_t low_largest;
+} vca_mc_grain_stats;
+vca_status vca_mc_grains(vca_mc* mc, int moore, double mobility_threshold, vca_mc_grain_stats* out);
+/* setMobility with a choice: the values are kept for vca_mc_grains' classes and, when
+ * use_in_dynamics != 0, also gate the trials (vca_mc_set_mobility is use_in_dynamics = 1). */
+vca_status vca_mc_set_mobility_values(vca_mc* mc, const float* mobility, int use_in_dynamics);
 /* PottsMC::crystals (PottsMC.cpp:666-697): N int32, 0 outside the domain. */
 vca_status vca_mc_crystals(vca_mc* mc, int32_t* out);
 /* Overwrite all orientations (setOrientation for every cell, PottsMC.cpp:566-576); values

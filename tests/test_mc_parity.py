@@ -117,3 +117,81 @@ def test_domain_and_mobility_from_ca_on_device():
     assert np.array_equal(mc.crystals(), spin)
     mc.close()
     ca.close()
+
+
+def _grains_host(spins, dims, moore, periodic, mob=None, thr=0.5):
+    """labelGrains (engine/src/mc/Grains.cpp:33-150) and the majority classes of McStage
+    (engine/src/app/McStage.cpp:38-66), restated with a plain union-find for the check."""
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    parent = list(range(n))
+
+    def find(i):
+        while parent[i] != i:
+            parent[i] = parent[parent[i]]
+            i = parent[i]
+        return i
+
+    offs = [(dx, dy, dz) for dz in (0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
+            if (dz > 0 or (dz == 0 and (dy > 0 or (dy == 0 and dx > 0))))
+            and not ((nx == 1 and dx) or (ny == 1 and dy) or (nz == 1 and dz))
+            and (moore or abs(dx) + abs(dy) + abs(dz) == 1)]
+    for i in range(n):
+        s = spins[i]
+        if s <= 0:
+            continue
+        x, y, z = i % nx, (i // nx) % ny, i // (nx * ny)
+        for dx, dy, dz in offs:
+            q = []
+            for v, d, size, per in ((x, dx, nx, periodic[0]), (y, dy, ny, periodic[1]), (z, dz, nz, periodic[2])):
+                w = v + d
+                if 0 <= w < size:
+                    q.append(w)
+                elif per and size > 1:
+                    q.append(w % size)
+                else:
+                    q = None
+                    break
+            if q is None:
+                continue
+            j = q[0] + nx * (q[1] + ny * q[2])
+            if spins[j] == s:
+                a, b = find(i), find(j)
+                if a != b:
+                    parent[max(a, b)] = min(a, b)
+    size, high = {}, {}
+    for i in range(n):
+        if spins[i] > 0:
+            r = find(i)
+            size[r] = size.get(r, 0) + 1
+            if mob is not None and float(mob[i]) >= thr:
+                high[r] = high.get(r, 0) + 1
+    hi = [s for r, s in size.items() if 2 * high.get(r, 0) >= s]
+    lo = [s for r, s in size.items() if 2 * high.get(r, 0) < s]
+    hc = sum(1 for i in range(n) if spins[i] > 0 and mob is not None and float(mob[i]) >= thr)
+    return (len(size), sum(size.values()), max(size.values(), default=0), hc, len(hi), sum(hi), max(hi, default=0),
+            len(lo), sum(lo), max(lo, default=0))
+
+
+@pytest.mark.parametrize("case", [(20, 16, 12, "moore", "periodic", True), (24, 1, 30, "von_neumann", "absorbing", False),
+                                  (18, 14, 10, "pentagonal", "periodic", False), (32, 1, 20, "hexagonal", "periodic", True)])
+def test_device_grains_match_host_labelling(case):
+    nx, ny, nz, nb, bc, full = case
+    rng = np.random.default_rng(4)
+    mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood=nb, boundary=bc, domain_full=full, seed=9, Q=4, kT=0.2))
+    dom = None if full else (rng.random(nx * ny * nz) < 0.7).astype(np.uint8)
+    mc.set_domain(dom)
+    mob = rng.random(nx * ny * nz).astype(np.float32)
+    mc.set_mobility(mob)
+    mc.initialize()
+    for _ in range(3):
+        mc.sweep(2)
+        g = mc.grains(moore=nb != "von_neumann", threshold=0.5)
+        spins = mc.crystals()
+        per = bc == "periodic"
+        want = _grains_host(spins.tolist(), (nx, ny, nz), nb != "von_neumann",
+                            (per and nx > 1, per and ny > 1, per and full and nz > 1), mob)
+        got = (g.grains, g.cells, g.largest, g.high_cells, g.high_grains, g.high_grain_cells, g.high_largest,
+               g.low_grains, g.low_grain_cells, g.low_largest)
+        assert got == want
+    mc.close()

@@ -29,7 +29,7 @@ EXPORTS = [
     "vca_ca_timing", "vca_ca_kernel_times", "vca_ca_destroy",
     "vca_mc_create", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
-    "vca_mc_energy", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
+    "vca_mc_energy", "vca_mc_grains", "vca_mc_set_mobility_values", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
     "vca_mc_energy_noalloc",
     "vca_last_error", "vca_version",
 ]
@@ -67,6 +67,11 @@ class McDesc(ctypes.Structure):
                 ("device", ctypes.c_int)]
 
 
+class GrainStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("grains", "cells", "largest", "high_cells", "high_grains", "high_grain_cells",
+                                              "high_largest", "low_grains", "low_grain_cells", "low_largest")]
+
+
 class McInfo(ctypes.Structure):
     _fields_ = [("sweeps", ctypes.c_int), ("colors", ctypes.c_int), ("domain_cells", ctypes.c_uint64),
                 ("attempts", ctypes.c_uint64), ("accepted", ctypes.c_uint64), ("uphill", ctypes.c_uint64),
@@ -97,7 +102,8 @@ def lib() -> ctypes.CDLL:
         "vca_mc_create": [p, p], "vca_mc_set_domain": [p, p], "vca_mc_set_mobility": [p, p],
         "vca_mc_set_domain_from_ca": [p, p], "vca_mc_set_mobility_from_ca": [p, p, f64, i32],
         "vca_mc_mobility": [p, p], "vca_mc_initialize": [p], "vca_mc_sweep": [p, i32, p],
-        "vca_mc_get_info": [p, p], "vca_mc_energy": [p, p], "vca_mc_crystals": [p, p],
+        "vca_mc_get_info": [p, p], "vca_mc_energy": [p, p], "vca_mc_grains": [p, i32, f64, p],
+        "vca_mc_set_mobility_values": [p, p, i32], "vca_mc_crystals": [p, p],
         "vca_mc_set_spins": [p, p], "vca_mc_timing": [p, p, p, p],
         "vca_mc_energy_noalloc": [p, i32, i32, i32, i32, i32, i32, u64, i32, f64, p, p],
     }
@@ -328,6 +334,11 @@ class PottsMC:
         e = ctypes.c_double()
         _check(lib().vca_mc_energy(self.h, ctypes.byref(e)), "vca_mc_energy")
         return e.value
+
+    def grains(self, moore: bool = True, threshold: float = 0.5) -> GrainStats:
+        out = GrainStats()
+        _check(lib().vca_mc_grains(self.h, int(moore), threshold, ctypes.byref(out)), "vca_mc_grains")
+        return out
 
     def crystals(self) -> np.ndarray:
         out = np.empty(self.n, np.int32)

@@ -469,18 +469,14 @@ struct ClassGrains {
 
 constexpr double kMobilityThreshold = 0.5;  // McStage::kMobilityThreshold (McStage.hpp:61)
 
-// classify (McStage.cpp:47-66): a grain is "high" when at least half of its cells have mobility >= threshold.
-void classify(const GrainLabels& g, const std::vector<float>& mob, ClassGrains& hi, ClassGrains& lo) {
-    std::vector<uint32_t> high(g.root.size(), 0);
-    for (size_t i = 0; i < g.root.size(); ++i)
-        if (g.root[i] != GrainLabels::kNone && mob[i] >= kMobilityThreshold) ++high[g.root[i]];
-    for (size_t r = 0; r < g.root.size(); ++r) {
-        if (g.root[r] != r) continue;
-        ClassGrains& c = (2ULL * high[r] >= g.size[r]) ? hi : lo;
-        ++c.grains;
-        c.cells += g.size[r];
-        c.largest = std::max<uint64_t>(c.largest, g.size[r]);
-    }
+// The majority classes of McStage (McStage.cpp:47-66) as vca_mc_grains computes them on the device.
+void classes(const vca_mc_grain_stats& g, ClassGrains& hi, ClassGrains& lo) {
+    hi.grains = g.high_grains;
+    hi.cells = g.high_grain_cells;
+    hi.largest = g.high_largest;
+    lo.grains = g.low_grains;
+    lo.cells = g.low_grain_cells;
+    lo.largest = g.low_largest;
 }
 
 Json class_json(uint64_t cells, const ClassGrains& a, const ClassGrains& b) {
@@ -492,13 +488,6 @@ Json class_json(uint64_t cells, const ClassGrains& a, const ClassGrains& b) {
     j["meanGrainSizeEnd"] = round_to(b.mean(), 3);
     j["largestGrainEnd"] = (unsigned long long)b.largest;
     return j;
-}
-
-uint64_t largest(const GrainLabels& g) {
-    uint64_t m = 0;
-    for (size_t r = 0; r < g.root.size(); ++r)
-        if (g.root[r] == r) m = std::max<uint64_t>(m, g.size[r]);
-    return m;
 }
 
 // CoolingMobility on the host, for CA results read from a file (engine/src/mc/CoolingMobility.cpp).
@@ -561,26 +550,25 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     vcheck(vca_mc_create(&d, &mc.h), "vca_mc_create");
     timing.add_detail("mcCreate", ms_since(t));
     auto td = Clock::now();
-    std::vector<float> cell_mob;
+    bool have_mobility = false;  // mobility values held by the handle: the byMobility classes exist
     if (full) {
         vcheck(vca_mc_set_domain(mc.h, nullptr), "vca_mc_set_domain");
     } else if (ca) {
         vcheck(vca_mc_set_domain_from_ca(mc.h, ca), "vca_mc_set_domain_from_ca");
         vcheck(vca_mc_set_mobility_from_ca(mc.h, ca, cfg.mc.mobility_min, cfg.mc.mobility_from_cooling ? 1 : 0),
                "vca_mc_set_mobility_from_ca");
-        cell_mob.resize((size_t)dims.cells());
-        vcheck(vca_mc_mobility(mc.h, cell_mob.data()), "vca_mc_mobility");
+        have_mobility = true;
         s.mobility_used = cfg.mc.mobility_from_cooling;
     } else {
         std::vector<uint8_t> dom((size_t)dims.cells());
         for (size_t i = 0; i < dom.size(); ++i) dom[i] = (file->type[i] == kBasalt || file->type[i] == kLava) ? 1 : 0;
         vcheck(vca_mc_set_domain(mc.h, dom.data()), "vca_mc_set_domain");
         if (cooling != Cooling::None) {
-            cell_mob = mobility_host(*file, dom, cfg.mc.mobility_min);
-            if (cfg.mc.mobility_from_cooling) {
-                vcheck(vca_mc_set_mobility(mc.h, cell_mob.data()), "vca_mc_set_mobility");
-                s.mobility_used = true;
-            }
+            const std::vector<float> cell_mob = mobility_host(*file, dom, cfg.mc.mobility_min);
+            vcheck(vca_mc_set_mobility_values(mc.h, cell_mob.data(), cfg.mc.mobility_from_cooling ? 1 : 0),
+                   "vca_mc_set_mobility_values");
+            have_mobility = true;
+            s.mobility_used = cfg.mc.mobility_from_cooling;
         }
         if (cooling == Cooling::None && cfg.mc.mobility_from_cooling)
             s.warnings.push_back("the CA result has no solidStep/arrivalStep (txt file): cooling mobility is off, MC as "
@@ -599,19 +587,12 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
         s.warnings.push_back(full ? "the MC domain is empty" : "the MC domain is empty: the CA result holds no basalt");
     timing.add("mcInit", ms_since(t));
 
-    const bool periodic[3] = {cfg.boundary == Bc::Periodic && dims.nx > 1, cfg.boundary == Bc::Periodic && dims.ny > 1,
-                              cfg.boundary == Bc::Periodic && full && dims.nz > 1};
     const bool moore = cfg.neighborhood != Nb::VonNeumann;
-    CrystalMap cmap;
-    cmap.dims = dims;
-    cmap.crystal.resize((size_t)dims.cells());
-    double grains_ms = 0.0, crystals_ms = 0.0;
-    auto measure = [&](GrainLabels* keep) {
-        auto tm = Clock::now();
-        vcheck(vca_mc_crystals(mc.h, cmap.crystal.data()), "vca_mc_crystals");
-        crystals_ms += ms_since(tm);
-        tm = Clock::now();
-        GrainLabels g = label_grains(cmap, moore, periodic);
+    double grains_ms = 0.0;
+    auto measure = [&](vca_mc_grain_stats* keep) {
+        const auto tm = Clock::now();
+        vca_mc_grain_stats g{};
+        vcheck(vca_mc_grains(mc.h, moore ? 1 : 0, kMobilityThreshold, &g), "vca_mc_grains");
         grains_ms += ms_since(tm);
         McStats st;
         vca_mc_info mi{};
@@ -620,7 +601,7 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
         st.grains = g.grains;
         st.mean = g.grains ? double(g.cells) / double(g.grains) : 0.0;
         vcheck(vca_mc_energy(mc.h, &st.energy), "vca_mc_energy");
-        if (keep) *keep = std::move(g);
+        if (keep) *keep = g;
         return st;
     };
     const int snap_every = out_dir.empty() ? 0 : cfg.mc.snapshots_every;
@@ -642,7 +623,7 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
         snapshot(0);
     }
     double sim_ms = 0.0, stats_ms = 0.0;
-    GrainLabels start_labels, end_labels;
+    vca_mc_grain_stats start_labels{}, end_labels{};
     t = Clock::now();
     s.history.push_back(measure(&start_labels));
     stats_ms += ms_since(t);
@@ -683,7 +664,6 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     uint64_t color_n = 0;
     vca_mc_timing(mc.h, &dev_ms, &color_ms, &color_n);
     timing.add_detail("mcDevice", dev_ms);
-    timing.add_detail("mcStatsCrystals", crystals_ms);
     timing.add_detail("mcStatsGrains", grains_ms);
 
     // stats.json "mc" (McStage::statsJson, McStage.cpp:326-383)
@@ -714,19 +694,17 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     j["grainsEnd"] = (unsigned long long)last.grains;
     j["meanGrainSizeStart"] = round_to(first.mean, 3);
     j["meanGrainSizeEnd"] = round_to(last.mean, 3);
-    j["largestGrainEnd"] = (unsigned long long)largest(end_labels);
+    j["largestGrainEnd"] = (unsigned long long)end_labels.largest;
     j["energyStart"] = first.energy;
     j["energyEnd"] = last.energy;
     j["attempts"] = (unsigned long long)info.attempts;
     j["accepted"] = (unsigned long long)info.accepted;
     j["acceptedUphill"] = (unsigned long long)info.uphill;
-    if (!cell_mob.empty()) {
+    if (have_mobility) {
         ClassGrains hs, ls, he, le;
-        classify(start_labels, cell_mob, hs, ls);
-        classify(end_labels, cell_mob, he, le);
-        uint64_t hi_cells = 0;
-        for (size_t i = 0; i < cell_mob.size(); ++i)
-            hi_cells += (start_labels.root[i] != GrainLabels::kNone && cell_mob[i] >= kMobilityThreshold) ? 1 : 0;
+        classes(start_labels, hs, ls);
+        classes(end_labels, he, le);
+        const uint64_t hi_cells = start_labels.high_cells;
         Json bm = Json::object();
         bm["threshold"] = kMobilityThreshold;
         bm["mobilityMin"] = cfg.mc.mobility_min;

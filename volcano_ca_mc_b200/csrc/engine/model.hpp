@@ -161,14 +161,4 @@ struct ResultSource {
 };
 Microstructure read_ca_folder(const std::string& folder, ResultSource* src);
 
-// grains.cpp -- union-find labelling (engine/src/mc/Grains.cpp:33-150)
-struct GrainLabels {
-    static constexpr uint32_t kNone = 0xFFFFFFFFu;
-    std::vector<uint32_t> root;
-    std::vector<uint32_t> size;
-    uint64_t grains = 0;
-    uint64_t cells = 0;
-};
-GrainLabels label_grains(const CrystalMap& m, bool moore, const bool periodic[3]);
-
 }  // namespace eng

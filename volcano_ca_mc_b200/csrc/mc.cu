@@ -113,6 +113,22 @@ __global__ void mc_init_kernel(McArgs a, const uint8_t* domain, uint64_t n) {
     }
 }
 
+// Cells of each colour in the domain (buildColors' class sizes, PottsMC.cpp:194-223).
+__global__ void mc_color_count_kernel(McArgs a, const uint8_t* domain, uint64_t n, int colors, unsigned long long* counts) {
+    __shared__ unsigned int s_cnt[28];
+    for (int c = threadIdx.x; c < 28; c += blockDim.x) s_cnt[c] = 0;
+    __syncthreads();
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
+        if (!domain[g]) continue;
+        int x, y, z;
+        decode(a, (uint32_t)g, x, y, z);
+        atomicAdd(&s_cnt[color_of(a, x, y, z)], 1u);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < colors; c += blockDim.x)
+        if (s_cnt[c]) atomicAdd(&counts[c], (unsigned long long)s_cnt[c]);
+}
+
 struct ColorPred {
     McArgs a;
     const uint8_t* domain;
@@ -381,6 +397,133 @@ __global__ __launch_bounds__(kMcThreads) void mc_energy_kernel(McArgs a, const u
     if (threadIdx.x == 0 && s_sum) atomicAdd(&a.ctrl->energy_acc, s_sum);
 }
 
+// ------------------------------------------------------------------------------------------
+// Grain statistics on the device (labelGrains, engine/src/mc/Grains.cpp:33-150; the majority
+// classes by mobility of McStage, engine/src/app/McStage.cpp:38-66).  A grain is a connected set
+// of domain cells of one orientation (von Neumann or Moore connectivity, periodic axes joined).
+// Lock-free union-find over the domain list: a root is only ever linked to a smaller root by
+// compare-and-swap, so parents only decrease and every loop ends; the components do not depend on
+// the order of the unions.  Loops are bounded anyway; running out sets an error flag.
+// ------------------------------------------------------------------------------------------
+struct GrainAcc {
+    unsigned long long grains, cells, largest, high_cells;
+    unsigned long long high_grains, high_in, high_largest, low_grains, low_in, low_largest;
+    unsigned int error;
+};
+
+__device__ __forceinline__ uint32_t gr_find(uint32_t* parent, uint32_t x, unsigned* err) {
+    for (int i = 0; i < (1 << 24); ++i) {
+        const uint32_t p = parent[x];
+        if (p == x) return x;
+        const uint32_t gp = parent[p];
+        if (gp != p) parent[x] = gp;  // path halving: gp is an ancestor of x, so the write is benign
+        x = gp;
+    }
+    atomicOr(err, 1u);
+    return x;
+}
+
+__device__ __forceinline__ void gr_union(uint32_t* parent, uint32_t a, uint32_t b, unsigned* err) {
+    for (int i = 0; i < (1 << 20); ++i) {
+        uint32_t ra = gr_find(parent, a, err), rb = gr_find(parent, b, err);
+        if (ra == rb) return;
+        if (ra > rb) {
+            const uint32_t t = ra;
+            ra = rb;
+            rb = t;
+        }
+        if (atomicCAS(&parent[rb], rb, ra) == rb) return;  // rb was still a root: linked under ra
+        a = ra;
+        b = rb;
+    }
+    atomicOr(err, 1u);
+}
+
+__global__ void mc_grain_init_kernel(const uint32_t* list, uint64_t count, uint32_t* parent, uint32_t* gsize, uint32_t* ghigh) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = list[j];
+        parent[g] = g;
+        gsize[g] = 0;
+        ghigh[g] = 0;
+    }
+}
+
+// Forward offsets of the connectivity (dz, dy, dx order, forward half) on the axes of size > 1.
+__global__ void mc_grain_union_kernel(McArgs a, const uint32_t* list, uint64_t count, int moore, uint32_t* parent, GrainAcc* acc) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = list[j];
+        const int32_t sg = a.spin[g];
+        if (sg <= 0) continue;
+        int x, y, z;
+        decode(a, g, x, y, z);
+        for (int dz = 0; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!(dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0))))) continue;
+                    if ((a.nx == 1 && dx) || (a.ny == 1 && dy) || (a.nz == 1 && dz)) continue;
+                    if (!moore && abs(dx) + abs(dy) + abs(dz) != 1) continue;
+                    int qx = x + dx, qy = y + dy, qz = z + dz;
+                    if (!mc_wrap(qx, a.nx, a.per[0]) || !mc_wrap(qy, a.ny, a.per[1]) || !mc_wrap(qz, a.nz, a.per[2])) continue;
+                    const uint32_t q = (uint32_t)qx + (uint32_t)a.nx * ((uint32_t)qy + (uint32_t)a.ny * (uint32_t)qz);
+                    if (a.spin[q] == sg) gr_union(parent, g, q, &acc->error);
+                }
+    }
+}
+
+__global__ void mc_grain_count_kernel(McArgs a, const uint32_t* list, uint64_t count, const float* mob, double threshold,
+                                      uint32_t* parent, uint32_t* gsize, uint32_t* ghigh, GrainAcc* acc) {
+    unsigned long long cells = 0, high = 0;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = list[j];
+        if (a.spin[g] <= 0) continue;
+        const uint32_t r = gr_find(parent, g, &acc->error);
+        parent[g] = r;
+        atomicAdd(&gsize[r], 1u);
+        ++cells;
+        if (mob != nullptr && (double)mob[g] >= threshold) {
+            atomicAdd(&ghigh[r], 1u);
+            ++high;
+        }
+    }
+    cells = __reduce_add_sync(0xFFFFFFFFu, (unsigned)cells);
+    high = __reduce_add_sync(0xFFFFFFFFu, (unsigned)high);
+    if ((threadIdx.x & 31) == 0) {
+        if (cells) atomicAdd(&acc->cells, cells);
+        if (high) atomicAdd(&acc->high_cells, high);
+    }
+}
+
+__global__ void mc_grain_reduce_kernel(McArgs a, const uint32_t* list, uint64_t count, const uint32_t* parent,
+                                       const uint32_t* gsize, const uint32_t* ghigh, GrainAcc* acc) {
+    unsigned long long grains = 0, largest = 0, hg = 0, hin = 0, hl = 0, lg = 0, lin = 0, ll = 0;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = list[j];
+        if (a.spin[g] <= 0 || parent[g] != g) continue;
+        const unsigned long long sz = gsize[g];
+        ++grains;
+        largest = max(largest, sz);
+        if (2ull * ghigh[g] >= sz) {  // the class of the majority of its cells (ties: high)
+            ++hg;
+            hin += sz;
+            hl = max(hl, sz);
+        } else {
+            ++lg;
+            lin += sz;
+            ll = max(ll, sz);
+        }
+    }
+    if (grains) {
+        atomicAdd(&acc->grains, grains);
+        atomicMax(&acc->largest, largest);
+        atomicAdd(&acc->high_grains, hg);
+        atomicAdd(&acc->high_in, hin);
+        atomicMax(&acc->high_largest, hl);
+        atomicAdd(&acc->low_grains, lg);
+        atomicAdd(&acc->low_in, lin);
+        atomicMax(&acc->low_largest, ll);
+    }
+}
+
 // CoolingMobility (engine/src/mc/CoolingMobility.cpp) on the device.
 __global__ void mc_domain_from_ca_kernel(const uint8_t* type, int nx, int P, uint64_t rows, uint8_t* domain) {
     const uint64_t n = (uint64_t)nx * rows;
@@ -483,6 +626,16 @@ struct vca_mc {
     bool domain_set = false;
     bool initialized = false;
     int sms = 148;
+    // set-up buffers, allocated on first use and kept (no cudaMalloc / cudaFree per call)
+    size_t list_cap = 0;                 // cells that list / list_mob can hold
+    unsigned int* scratch = nullptr;     // mobility: [end, min, max] + time[n]
+    void* cub_temp = nullptr;
+    size_t cub_temp_bytes = 0;
+    unsigned long long* d_count = nullptr;  // 28 colour counts
+    uint32_t* gparent = nullptr;         // grain statistics: parent, size, high count per cell (n each)
+    uint32_t* gsize = nullptr;
+    uint32_t* ghigh = nullptr;
+    void* gacc = nullptr;                // GrainAcc
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     double total_ms = 0.0;
     double color_ms = 0.0;
@@ -550,6 +703,13 @@ void mc_free(vca_mc* h) {
     cudaFree(h->list_mob);
     cudaFree(h->table);
     cudaFree(h->ctrl);
+    cudaFree(h->scratch);
+    cudaFree(h->cub_temp);
+    cudaFree(h->d_count);
+    cudaFree(h->gparent);
+    cudaFree(h->gsize);
+    cudaFree(h->ghigh);
+    cudaFree(h->gacc);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
@@ -751,8 +911,8 @@ vca_status vca_mc_set_mobility_from_ca(vca_mc* h, vca_ca* ca, double mobility_mi
     VCA_CUDA(cudaSetDevice(h->device));
     VCA_CUDA(cudaStreamSynchronize(v.stream));
     if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->n));
-    unsigned int* scratch = nullptr;  // [end, min, max] + time[n]
-    VCA_CUDA(cudaMalloc(&scratch, 4 * (3 + h->n)));
+    if (!h->scratch) VCA_CUDA(cudaMalloc(&h->scratch, 4 * (3 + h->n)));
+    unsigned int* scratch = h->scratch;  // [end, min, max] + time[n]
     const unsigned int init[3] = {0u, 0xFFFFFFFFu, 0u};
     VCA_CUDA(cudaMemcpyAsync(scratch, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
     const uint64_t rows = (uint64_t)v.ny * v.nz;
@@ -763,7 +923,6 @@ vca_status vca_mc_set_mobility_from_ca(vca_mc* h, vca_ca* ca, double mobility_mi
     mc_normalize_kernel<<<blocks, 256, 0, h->stream>>>(scratch + 3, h->domain, scratch + 1, mobility_min, h->n, h->mobility);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamSynchronize(h->stream);
-    cudaFree(scratch);
     if (e != cudaSuccess) return cuda_fail(e, "mobility kernels");
     if (e2 != cudaSuccess) return cuda_fail(e2, "mobility kernels");
     h->mobility_set = true;
@@ -794,47 +953,51 @@ vca_status vca_mc_initialize(vca_mc* h) {
     McArgs a = mc_args(h);
     mc_init_kernel<<<h->sms * 8, 256, 0, h->stream>>>(a, h->domain, h->n);
     VCA_CUDA(cudaGetLastError());
-    // Colour lists, colour by colour, globalIndex ascending inside a colour (PottsMC.cpp:194-223).
-    cudaFree(h->list);
-    h->list = nullptr;
-    cudaFree(h->list_mob);
-    h->list_mob = nullptr;
-    unsigned long long* d_count = nullptr;
-    VCA_CUDA(cudaMalloc(&d_count, 8 * (size_t)h->colors));
-    VCA_CUDA(cudaMemsetAsync(d_count, 0, 8 * (size_t)h->colors, h->stream));
-    size_t temp_bytes = 0;
-    ColorPred pred{a, h->domain, 0};
-    thrust::counting_iterator<uint32_t> it(0);
-    // A domain bound for the list: count of domain cells.
-    std::vector<uint8_t> dummy;
-    uint32_t* all = nullptr;
-    VCA_CUDA(cudaMalloc(&all, 4 * h->n));
-    VCA_CUDA(cub::DeviceSelect::If(nullptr, temp_bytes, it, all, d_count, (int64_t)h->n, pred, h->stream));
-    void* temp = nullptr;
-    VCA_CUDA(cudaMalloc(&temp, temp_bytes));
+    // Colour lists, colour by colour, globalIndex ascending inside a colour (PottsMC.cpp:194-223):
+    // count the cells of each colour, then select each colour into its place of one list.
+    if (!h->d_count) VCA_CUDA(cudaMalloc(&h->d_count, 8 * 28));
+    VCA_CUDA(cudaMemsetAsync(h->d_count, 0, 8 * 28, h->stream));
+    mc_color_count_kernel<<<h->sms * 8, 256, 0, h->stream>>>(a, h->domain, h->n, h->colors, h->d_count);
+    VCA_CUDA(cudaGetLastError());
     std::vector<unsigned long long> counts((size_t)h->colors, 0);
+    VCA_CUDA(cudaMemcpyAsync(counts.data(), h->d_count, 8 * (size_t)h->colors, cudaMemcpyDeviceToHost, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->color_off.assign((size_t)h->colors + 1, 0);
     uint64_t total = 0;
     for (int c = 0; c < h->colors; ++c) {
-        pred.color = c;
-        VCA_CUDA(cub::DeviceSelect::If(temp, temp_bytes, it, all + total, d_count + c, (int64_t)h->n, pred, h->stream));
-        VCA_CUDA(cudaMemcpyAsync(&counts[c], d_count + c, 8, cudaMemcpyDeviceToHost, h->stream));
-        VCA_CUDA(cudaStreamSynchronize(h->stream));
         h->color_off[c] = total;
         total += counts[c];
     }
     h->color_off[h->colors] = total;
-    cudaFree(temp);
-    cudaFree(d_count);
-    VCA_CUDA(cudaMalloc(&h->list, 4 * std::max<uint64_t>(total, 1)));
-    if (total) VCA_CUDA(cudaMemcpyAsync(h->list, all, 4 * total, cudaMemcpyDeviceToDevice, h->stream));
-    if (h->mobility_on) {
-        VCA_CUDA(cudaMalloc(&h->list_mob, 4 * std::max<uint64_t>(total, 1)));
-        if (total) mc_gather_mob_kernel<<<grid_for(total, h->sms), 256, 0, h->stream>>>(h->list, h->mobility, h->list_mob, total);
+    if (total > h->list_cap || (h->mobility_on && !h->list_mob)) {
+        cudaFree(h->list);
+        cudaFree(h->list_mob);
+        h->list = nullptr;
+        h->list_mob = nullptr;
+        h->list_cap = std::max<uint64_t>(total, 1);
+        VCA_CUDA(cudaMalloc(&h->list, 4 * h->list_cap));
+        VCA_CUDA(cudaMalloc(&h->list_mob, 4 * h->list_cap));
+    }
+    ColorPred pred{a, h->domain, 0};
+    thrust::counting_iterator<uint32_t> it(0);
+    size_t temp_bytes = 0;
+    VCA_CUDA(cub::DeviceSelect::If(nullptr, temp_bytes, it, h->list, h->d_count, (int64_t)h->n, pred, h->stream));
+    if (temp_bytes > h->cub_temp_bytes) {
+        cudaFree(h->cub_temp);
+        h->cub_temp = nullptr;
+        VCA_CUDA(cudaMalloc(&h->cub_temp, temp_bytes));
+        h->cub_temp_bytes = temp_bytes;
+    }
+    for (int c = 0; c < h->colors; ++c) {
+        if (counts[c] == 0) continue;
+        pred.color = c;
+        VCA_CUDA(cub::DeviceSelect::If(h->cub_temp, temp_bytes, it, h->list + h->color_off[c], h->d_count + c, (int64_t)h->n, pred,
+                                       h->stream));
+    }
+    if (h->mobility_on && total) {
+        mc_gather_mob_kernel<<<grid_for(total, h->sms), 256, 0, h->stream>>>(h->list, h->mobility, h->list_mob, total);
         VCA_CUDA(cudaGetLastError());
     }
-    VCA_CUDA(cudaStreamSynchronize(h->stream));
-    cudaFree(all);
     VCA_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream));
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->initialized = true;
@@ -956,6 +1119,64 @@ vca_status vca_mc_get_info(vca_mc* h, vca_mc_info* out) {
     out->accepted = h->ctrl_host->accepted;
     out->uphill = h->ctrl_host->uphill;
     out->kernel_launches = h->launches;
+    return VCA_OK;
+}
+
+vca_status vca_mc_grains(vca_mc* h, int moore, double mobility_threshold, vca_mc_grain_stats* out) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!out) {
+        set_error("vca_mc_grains: null output");
+        return VCA_ERR_ARG;
+    }
+    if (!h->initialized) {
+        set_error("vca_mc_grains: initialize first");
+        return VCA_ERR_STATE;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (!h->gparent) {
+        VCA_CUDA(cudaMalloc(&h->gparent, 4 * h->n));
+        VCA_CUDA(cudaMalloc(&h->gsize, 4 * h->n));
+        VCA_CUDA(cudaMalloc(&h->ghigh, 4 * h->n));
+        VCA_CUDA(cudaMalloc(&h->gacc, sizeof(GrainAcc)));
+    }
+    GrainAcc* acc = static_cast<GrainAcc*>(h->gacc);
+    VCA_CUDA(cudaMemsetAsync(acc, 0, sizeof(GrainAcc), h->stream));
+    const uint64_t total = h->color_off.back();
+    const McArgs a = mc_args(h);
+    const float* mob = h->mobility_set ? h->mobility : nullptr;
+    if (total) {
+        const int grid = grid_for(total, h->sms);
+        mc_grain_init_kernel<<<grid, kMcThreads, 0, h->stream>>>(h->list, total, h->gparent, h->gsize, h->ghigh);
+        mc_grain_union_kernel<<<grid, kMcThreads, 0, h->stream>>>(a, h->list, total, moore, h->gparent, acc);
+        mc_grain_count_kernel<<<grid, kMcThreads, 0, h->stream>>>(a, h->list, total, mob, mobility_threshold, h->gparent, h->gsize,
+                                                                  h->ghigh, acc);
+        mc_grain_reduce_kernel<<<grid, kMcThreads, 0, h->stream>>>(a, h->list, total, h->gparent, h->gsize, h->ghigh, acc);
+        VCA_CUDA(cudaGetLastError());
+        h->launches += 4;
+    }
+    GrainAcc r;
+    VCA_CUDA(cudaMemcpyAsync(&r, acc, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    if (r.error) {
+        set_error("vca_mc_grains: a bounded union-find loop ran out");
+        return VCA_ERR_TIMEOUT;
+    }
+    out->grains = r.grains;
+    out->cells = r.cells;
+    out->largest = r.largest;
+    out->high_cells = r.high_cells;
+    out->high_grains = r.high_grains;
+    out->high_grain_cells = r.high_in;
+    out->high_largest = r.high_largest;
+    out->low_grains = r.low_grains;
+    out->low_grain_cells = r.low_in;
+    out->low_largest = r.low_largest;
+    return VCA_OK;
+}
+
+vca_status vca_mc_set_mobility_values(vca_mc* h, const float* mobility, int use_in_dynamics) {
+    if (vca_status s = vca_mc_set_mobility(h, mobility)) return s;
+    if (mobility) h->mobility_on = use_in_dynamics != 0;
     return VCA_OK;
 }
 
