@@ -100,6 +100,14 @@ typedef struct {
 
 /* LavaCA ctor (LavaCA.hpp:84-144): all cells AIR, buffers on the device. */
 vca_status vca_ca_create(const vca_ca_desc* desc, vca_ca** out);
+/* Device bytes a handle of this description allocates (the admission figure of a job server).
+ * No counterpart in the reference. */
+vca_status vca_ca_footprint(const vca_ca_desc* desc, uint64_t* bytes);
+/* Give a handle another space and parameters (any description whose sizes fit the handle's device
+ * memory: vca_ca_footprint of it <= that of the creating one, same device), in the state of a new
+ * handle.  Allocates nothing; lets a server keep resident handles for jobs of varying size.
+ * VCA_ERR_ARG when it does not fit.  No counterpart in the reference. */
+vca_status vca_ca_reconfigure(vca_ca* ca, const vca_ca_desc* desc);
 /* Back to the state of a new handle (all cells AIR, no terrain, no vents, step 0) without
  * freeing or allocating device memory, so that one resident handle can run job after job of the
  * same dimensions.  No counterpart in the reference (it builds a new LavaCA per run). */
@@ -174,6 +182,13 @@ typedef struct {
 } vca_mc_info;
 
 vca_status vca_mc_create(const vca_mc_desc* desc, vca_mc** out);
+/* Device bytes an MC handle of this description can come to hold (all per-cell buffers).
+ * No counterpart in the reference. */
+vca_status vca_mc_footprint(const vca_mc_desc* desc, uint64_t* bytes);
+/* Another space / parameters on this handle (no more cells than it was created for, same device):
+ * orientations cleared, domain and mobility unset.  Allocates nothing.  No counterpart in the
+ * reference. */
+vca_status vca_mc_reconfigure(vca_mc* mc, const vca_mc_desc* desc);
 /* setDomain / setDomainAll (PottsMC.cpp:61-83): in_domain is N bytes, or NULL for all cells. */
 vca_status vca_mc_set_domain(vca_mc* mc, const uint8_t* in_domain);
 /* setMobility (PottsMC.cpp:85-102): N floats, or NULL to switch mobility off. */

@@ -176,3 +176,36 @@ def test_reset_reuses_handle():
         for a, b in zip(got[3], fresh[k][3]):
             assert np.array_equal(a, b)
     ca.close()
+
+
+def test_reconfigure_runs_other_spaces_exactly():
+    """vca_ca_reconfigure: a resident handle created for a large space runs smaller spaces with other
+    parameters (2D and 3D, other neighbourhoods and boundaries) exactly like new handles, and refuses
+    a space that does not fit."""
+    big = _params(64, 40, 32, "moore", "absorbing", 400, capi.SWEEP_ACTIVE, 1)
+    jobs = [(40, 24, 20, "pentagonal", "periodic", 7), (96, 1, 40, "hexagonal", "absorbing", 8),
+            (33, 17, 14, "von_neumann", "periodic", 9)]
+    ca = capi.LavaCA(big)
+    for nx, ny, nz, nb, bc, seed in jobs:
+        p = _params(nx, ny, nz, nb, bc, 300, capi.SWEEP_ACTIVE, seed)
+        p.eruption_steps = 30
+        heights = C.terrain(nx, ny, nz, seed)
+        vents = C.pick_vents(heights, nx, ny, nz, 2, seed)
+        fresh = capi.LavaCA(p)
+        fresh.apply_terrain(heights)
+        fresh.place_seeds(vents)
+        fresh.run()
+        want = (fresh.info().steps, fresh.info().stop_reason, fresh.history(), fresh.download())
+        fresh.close()
+        ca.reconfigure(p)
+        ca.apply_terrain(heights)
+        ca.place_seeds(vents)
+        ca.run()
+        got = (ca.info().steps, ca.info().stop_reason, ca.history(), ca.download())
+        assert got[:3] == want[:3]
+        for a, b in zip(got[3], want[3]):
+            assert np.array_equal(a, b)
+    assert capi.ca_footprint(big) >= capi.ca_footprint(_params(40, 24, 20, "moore", "absorbing", 300, 0, 1))
+    with pytest.raises(capi.VcaError, match="does not fit"):
+        ca.reconfigure(_params(128, 40, 32, "moore", "absorbing", 300, capi.SWEEP_ACTIVE, 1))
+    ca.close()

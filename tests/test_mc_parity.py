@@ -195,3 +195,30 @@ def test_device_grains_match_host_labelling(case):
                g.low_grains, g.low_grain_cells, g.low_largest)
         assert got == want
     mc.close()
+
+
+def test_mc_reconfigure_runs_other_spaces_exactly():
+    """vca_mc_reconfigure: one handle, spaces of fewer cells and other parameters, same results as
+    new handles; a larger space is refused."""
+    mc = capi.PottsMC(capi.McParams(40, 30, 20, neighborhood="moore", boundary="periodic", domain_full=True, seed=1, Q=8))
+    rng = np.random.default_rng(3)
+    for nx, ny, nz, nb, bc, full, Q, kT in [(20, 16, 12, "pentagonal", "periodic", False, 16, 0.4),
+                                            (48, 1, 30, "hexagonal", "absorbing", True, 5, 0.0),
+                                            (17, 13, 9, "von_neumann", "periodic", True, 32, 1.0)]:
+        p = capi.McParams(nx, ny, nz, neighborhood=nb, boundary=bc, domain_full=full, seed=5, Q=Q, kT=kT)
+        dom = None if full else (rng.random(nx * ny * nz) < 0.6).astype(np.uint8)
+        fresh = capi.PottsMC(p)
+        fresh.set_domain(dom)
+        fresh.initialize()
+        fresh.sweep(4)
+        want = (fresh.crystals(), fresh.energy(), fresh.info().attempts)
+        fresh.close()
+        mc.reconfigure(p)
+        mc.set_domain(dom)
+        mc.initialize()
+        mc.sweep(4)
+        got = (mc.crystals(), mc.energy(), mc.info().attempts)
+        assert np.array_equal(got[0], want[0]) and got[1:] == want[1:]
+    with pytest.raises(capi.VcaError, match="does not fit"):
+        mc.reconfigure(capi.McParams(41, 30, 20, neighborhood="moore", boundary="periodic", domain_full=True, Q=8))
+    mc.close()

@@ -24,10 +24,10 @@ STOP_NAMES = {0: "running", 1: "no lava", 2: "no air", 3: "no change", 4: "max s
 
 # Every entry point declared in include/vca.h.
 EXPORTS = [
-    "vca_ca_create", "vca_ca_reset", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
+    "vca_ca_create", "vca_ca_footprint", "vca_ca_reconfigure", "vca_ca_reset", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
     "vca_ca_get_info", "vca_ca_history", "vca_ca_download", "vca_ca_set_state", "vca_ca_get_spill",
     "vca_ca_timing", "vca_ca_kernel_times", "vca_ca_destroy",
-    "vca_mc_create", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
+    "vca_mc_create", "vca_mc_footprint", "vca_mc_reconfigure", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
     "vca_mc_energy", "vca_mc_grains", "vca_mc_set_mobility_values", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
     "vca_mc_energy_noalloc",
@@ -94,12 +94,12 @@ def lib() -> ctypes.CDLL:
         raise VcaError(f"cannot load {LIB_PATH}: {e}") from e
     p, i32, u64, f64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_double
     sig = {
-        "vca_ca_create": [p, p], "vca_ca_reset": [p], "vca_ca_apply_terrain": [p, p], "vca_ca_place_seeds": [p, p, i32],
+        "vca_ca_create": [p, p], "vca_ca_footprint": [p, p], "vca_ca_reconfigure": [p, p], "vca_ca_reset": [p], "vca_ca_apply_terrain": [p, p], "vca_ca_place_seeds": [p, p, i32],
         "vca_ca_step": [p, p], "vca_ca_run": [p], "vca_ca_get_info": [p, p],
         "vca_ca_history": [p, p, p, i32, p], "vca_ca_download": [p, p, p, p, p, p],
         "vca_ca_set_state": [p, p, p, p, p, p, p, p, i32, i32], "vca_ca_get_spill": [p, p],
         "vca_ca_timing": [p, p, p, p], "vca_ca_kernel_times": [p, p, p, p, p],
-        "vca_mc_create": [p, p], "vca_mc_set_domain": [p, p], "vca_mc_set_mobility": [p, p],
+        "vca_mc_create": [p, p], "vca_mc_footprint": [p, p], "vca_mc_reconfigure": [p, p], "vca_mc_set_domain": [p, p], "vca_mc_set_mobility": [p, p],
         "vca_mc_set_domain_from_ca": [p, p], "vca_mc_set_mobility_from_ca": [p, p, f64, i32],
         "vca_mc_mobility": [p, p], "vca_mc_initialize": [p], "vca_mc_sweep": [p, i32, p],
         "vca_mc_get_info": [p, p], "vca_mc_energy": [p, p], "vca_mc_grains": [p, i32, f64, p],
@@ -162,6 +162,14 @@ class CaParams:
                       self.sweep, self.device)
 
 
+def ca_footprint(params: "CaParams") -> int:
+    """Device bytes of a CA handle for these parameters."""
+    d = params.desc()
+    b = ctypes.c_uint64()
+    _check(lib().vca_ca_footprint(ctypes.byref(d), ctypes.byref(b)), "vca_ca_footprint")
+    return b.value
+
+
 class LavaCA:
     """Python face of the vca_ca_* handle (the reference's LavaCA, engine/src/ca/LavaCA.hpp)."""
 
@@ -183,6 +191,13 @@ class LavaCA:
             self.close()
         except Exception:
             pass
+
+    def reconfigure(self, params: "CaParams") -> None:
+        """Another space / parameters on this handle's device memory (must fit), state of a new handle."""
+        d = params.desc()
+        _check(lib().vca_ca_reconfigure(self.h, ctypes.byref(d)), "vca_ca_reconfigure")
+        self.params = params
+        self.n = params.nx * params.ny * params.nz
 
     def reset(self) -> None:
         """All cells AIR, no terrain, no vents, step 0 (device memory kept)."""
@@ -276,6 +291,14 @@ class McParams:
                       self.seed, self.Q, self.J, self.kT, self.device)
 
 
+def mc_footprint(params: "McParams") -> int:
+    """Device bytes an MC handle for these parameters can come to hold."""
+    d = params.desc()
+    b = ctypes.c_uint64()
+    _check(lib().vca_mc_footprint(ctypes.byref(d), ctypes.byref(b)), "vca_mc_footprint")
+    return b.value
+
+
 class PottsMC:
     """Python face of the vca_mc_* handle (the reference's PottsMC with mc.update = checkerboard)."""
 
@@ -297,6 +320,13 @@ class PottsMC:
             self.close()
         except Exception:
             pass
+
+    def reconfigure(self, params: "McParams") -> None:
+        """Another space / parameters on this handle (no more cells than at creation)."""
+        d = params.desc()
+        _check(lib().vca_mc_reconfigure(self.h, ctypes.byref(d)), "vca_mc_reconfigure")
+        self.params = params
+        self.n = params.nx * params.ny * params.nz
 
     def set_domain(self, domain: np.ndarray | None) -> None:
         d = None if domain is None else np.ascontiguousarray(domain, np.uint8)

@@ -1621,9 +1621,13 @@ vca_status upload_vents(vca_ca* h, const vca_vent* vents, int count) {
     std::vector<int4> table((size_t)slots, make_int4(-1, -1, -1, 0));
     for (int i = 0; i < count; ++i)
         if (vents[i].flow_id > 0) table[(size_t)vents[i].flow_id] = make_int4(vents[i].x, vents[i].y, vents[i].z, 0);
-    cudaFree(h->vents);
-    h->vents = nullptr;
-    VCA_CUDA(cudaMalloc(&h->vents, sizeof(int4) * table.size()));
+    if ((size_t)slots > h->vent_cap) {  // grows only: a resident handle keeps its buffer
+        cudaFree(h->vents);
+        h->vents = nullptr;
+        const size_t cap = std::max<size_t>((size_t)slots, 64);
+        VCA_CUDA(cudaMalloc(&h->vents, sizeof(int4) * cap));
+        h->vent_cap = cap;
+    }
     VCA_CUDA(cudaMemcpyAsync(h->vents, table.data(), sizeof(int4) * table.size(), cudaMemcpyHostToDevice, h->stream));
     // bit 1 of the tile flags: the tiles that hold a vent (the only ones whose LAVA can be reheated)
     const auto& g = h->geom;
@@ -1657,46 +1661,78 @@ vca_status get_plane(vca_ca* h, T* dst, const T* src) {
 
 }  // namespace
 
-extern "C" {
+namespace vca {
 
-vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
-    if (d == nullptr || out == nullptr) {
-        set_error("vca_ca_create: null argument");
-        return VCA_ERR_ARG;
-    }
-    *out = nullptr;
+vca_status validate_desc(const vca_ca_desc* d, const char* who) {
     const int nx = d->nx, ny = d->ny, nz = d->nz;
-    if (nx < 1 || ny < 1 || nz < 1 || (nx > 1) + (ny > 1) + (nz > 1) < 2) {
-        set_error("vca_ca_create: the space must be 2D (exactly one size equal to 1) or 3D");
+    auto bad = [&](const std::string& m) {
+        set_error(std::string(who) + ": " + m);
         return VCA_ERR_ARG;
-    }
-    if ((uint64_t)nx * ny * nz > 2000000000ULL) {
-        set_error("vca_ca_create: more than 2 000 000 000 cells");
-        return VCA_ERR_ARG;
-    }
-    if (d->mode == VCA_MODE_LAVA && (nx > 1) + (ny > 1) + (nz > 1) == 2 && ny != 1) {
-        set_error("vca_ca_create: a 2D lava space is the x-z cross-section (ny = 1)");
-        return VCA_ERR_ARG;
-    }
-    if (d->max_steps < 0 || d->max_steps > 65535) {
-        set_error("vca_ca_create: max_steps must be in 0..65535");
-        return VCA_ERR_ARG;
-    }
+    };
+    if (nx < 1 || ny < 1 || nz < 1 || (nx > 1) + (ny > 1) + (nz > 1) < 2)
+        return bad("the space must be 2D (exactly one size equal to 1) or 3D");
+    if ((uint64_t)nx * ny * nz > 2000000000ULL) return bad("more than 2 000 000 000 cells");
+    if (d->mode == VCA_MODE_LAVA && (nx > 1) + (ny > 1) + (nz > 1) == 2 && ny != 1)
+        return bad("a 2D lava space is the x-z cross-section (ny = 1)");
+    if (d->max_steps < 0 || d->max_steps > 65535) return bad("max_steps must be in 0..65535");
     if (d->neighborhood < 0 || d->neighborhood > 3 || d->boundary < 0 || d->boundary > 1 || d->mode < 0 || d->mode > 1 ||
-        d->sweep < 0 || d->sweep > 1) {
-        set_error("vca_ca_create: unknown neighborhood, boundary, mode or sweep");
-        return VCA_ERR_ARG;
+        d->sweep < 0 || d->sweep > 1)
+        return bad("unknown neighborhood, boundary, mode or sweep");
+    NbTable nb;
+    if (!build_nb(d->neighborhood, nx, ny, nz, nb)) return bad("the hexagonal neighbourhood is defined in 2D only");
+    return VCA_OK;
+}
+
+// Pitched geometry and tile shape of a space (tiles 64 x TY x TZ, TY * TZ = 16).
+CaGeom geometry_of(const vca_ca_desc* d) {
+    CaGeom g{};
+    g.nx = d->nx;
+    g.ny = d->ny;
+    g.nz = d->nz;
+    g.P = (d->nx + kTileX - 1) / kTileX * kTileX;
+    const bool periodic = d->boundary == VCA_BC_PERIODIC;
+    g.per[0] = periodic && d->nx > 1;
+    g.per[1] = periodic && d->ny > 1;
+    g.per[2] = periodic && d->mode == VCA_MODE_CLASSIC && d->nz > 1;
+    if (d->ny > 1 && d->nz > 1) {
+        g.TY = 4;
+        g.TZ = 4;
+    } else if (d->ny == 1) {
+        g.TY = 1;
+        g.TZ = 16;
+    } else {
+        g.TY = 16;
+        g.TZ = 1;
     }
-    vca_ca* h = new vca_ca();
+    g.tiles_x = g.P / kTileX;
+    g.tiles_y = (d->ny + g.TY - 1) / g.TY;
+    g.tiles_z = (d->nz + g.TZ - 1) / g.TZ;
+    return g;
+}
+
+CaSizes sizes_of(const vca_ca_desc* d) {
+    const CaGeom g = geometry_of(d);
+    CaSizes z;
+    z.plane_cells = (size_t)g.P * d->ny * d->nz;
+    z.ntiles = (uint64_t)g.tiles_x * g.tiles_y * g.tiles_z;
+    z.chg_cap = (uint32_t)std::min<uint64_t>((uint64_t)d->nx * d->ny * d->nz, 1u << 22);
+    z.cols = (size_t)d->nx * d->ny;
+    z.hist = std::max(1, d->max_steps);
+    return z;
+}
+
+// Everything of a handle that depends on the space and the parameters: geometry, neighbourhood
+// tables, TMA descriptors, grids, all cells AIR, no vents, step 0.  Allocates nothing.
+vca_status configure(vca_ca* h, const vca_ca_desc* d) {
     h->desc = *d;
-    h->device = d->device;
-    if (!build_nb(d->neighborhood, nx, ny, nz, h->tables_host.nb)) {
-        delete h;
-        set_error("vca_ca_create: the hexagonal neighbourhood is defined in 2D only");
-        return VCA_ERR_ARG;
-    }
+    h->geom = geometry_of(d);
+    const CaGeom& g = h->geom;
+    h->ntiles = (uint64_t)g.tiles_x * g.tiles_y * g.tiles_z;
+    h->plane_cells = (size_t)g.P * g.ny * g.nz;
+    h->chg_cap = h->cap.chg_cap;
+    std::memset(&h->tables_host, 0, sizeof(h->tables_host));
+    build_nb(d->neighborhood, d->nx, d->ny, d->nz, h->tables_host.nb);
     // side offsets: union of dz == 0 offsets over all variants (LavaCA.hpp:104-112)
-    h->tables_host.nside = 0;
     for (int v = 0; v < h->tables_host.nb.variants; ++v)
         for (int i = 0; i < h->tables_host.nb.count[v]; ++i) {
             const int8_t* o = h->tables_host.nb.off[v][i];
@@ -1709,6 +1745,37 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
                 ++h->tables_host.nside;
             }
         }
+    h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)h->sms * std::max(1, h->rules_per_sm));
+    // one wave, and no more blocks than the grid could ever list candidates for (small grids share the GPU)
+    h->cand_blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->sms * std::max(1, h->cand_per_sm),
+                                                                  (h->ntiles * kTileCells + kCandThreads - 1) / kCandThreads));
+    if (vca_status s = encode_maps(h)) return s;
+    drop_graph(h);
+    if (vca_status s = clear_planes(h)) return s;
+    vca_vent none{0, 0, 0, 0};
+    if (vca_status s = upload_vents(h, &none, 0)) return s;  // synchronizes the stream
+    h->has_terrain = false;
+    h->seeded = false;
+    h->steps = 0;
+    h->stop = VCA_STOP_RUNNING;
+    return VCA_OK;
+}
+
+}  // namespace vca
+
+extern "C" {
+
+vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
+    if (d == nullptr || out == nullptr) {
+        set_error("vca_ca_create: null argument");
+        return VCA_ERR_ARG;
+    }
+    *out = nullptr;
+    if (vca_status s = validate_desc(d, "vca_ca_create")) return s;
+    const CaSizes need = sizes_of(d);
+    vca_ca* h = new vca_ca();
+    h->desc = *d;
+    h->device = d->device;
     auto fail = [&](vca_status s) {
         free_all(h);
         delete h;
@@ -1724,31 +1791,7 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
                   std::to_string(prop.minor));
         return fail(VCA_ERR_CUDA);
     }
-    auto& g = h->geom;
-    g.nx = nx;
-    g.ny = ny;
-    g.nz = nz;
-    g.P = (nx + kTileX - 1) / kTileX * kTileX;
-    const bool periodic = d->boundary == VCA_BC_PERIODIC;
-    g.per[0] = periodic && nx > 1;
-    g.per[1] = periodic && ny > 1;
-    g.per[2] = periodic && d->mode == VCA_MODE_CLASSIC && nz > 1;
-    if (ny > 1 && nz > 1) {
-        g.TY = 4;
-        g.TZ = 4;
-    } else if (ny == 1) {
-        g.TY = 1;
-        g.TZ = 16;
-    } else {
-        g.TY = 16;
-        g.TZ = 1;
-    }
-    g.tiles_x = g.P / kTileX;
-    g.tiles_y = (ny + g.TY - 1) / g.TY;
-    g.tiles_z = (nz + g.TZ - 1) / g.TZ;
-    h->ntiles = (uint64_t)g.tiles_x * g.tiles_y * g.tiles_z;
-    h->plane_cells = (size_t)g.P * ny * nz;
-    const size_t n = h->plane_cells;
+    h->sms = prop.multiProcessorCount;
 #define ALLOC(ptr, bytes)                                                         \
     do {                                                                          \
         e = cudaMalloc(&(ptr), (bytes));                                          \
@@ -1756,42 +1799,38 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     } while (0)
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
+    const size_t n = need.plane_cells;
     for (int b = 0; b < 2; ++b) {
         ALLOC(h->type[b], n);
         ALLOC(h->flow[b], n * 4);
         ALLOC(h->temp[b], n * 4);
         ALLOC(h->solid[b], n * 2);
         ALLOC(h->arrival[b], n * 2);
-        ALLOC(h->tile_list[b], h->ntiles * 4);
+        ALLOC(h->tile_list[b], need.ntiles * 4);
     }
-    ALLOC(h->tile_flags, h->ntiles * 4);
-    ALLOC(h->tile_mark[0], h->ntiles * 4);
-    ALLOC(h->tile_mark[1], h->ntiles * 4);
+    ALLOC(h->tile_flags, need.ntiles * 4);
+    ALLOC(h->tile_mark[0], need.ntiles * 4);
+    ALLOC(h->tile_mark[1], need.ntiles * 4);
     ALLOC(h->desc_plane, n);
     ALLOC(h->drop_plane, n);
-    h->chg_cap = (uint32_t)std::min<uint64_t>((uint64_t)nx * ny * nz, 1u << 22);
-    ALLOC(h->chg_list[0], sizeof(uint32_t) * (size_t)h->chg_cap);
-    ALLOC(h->chg_list[1], sizeof(uint32_t) * (size_t)h->chg_cap);
-    ALLOC(h->cand_list, sizeof(uint32_t) * (size_t)h->ntiles * kTileCells);  // never overflows
+    ALLOC(h->chg_list[0], sizeof(uint32_t) * (size_t)need.chg_cap);
+    ALLOC(h->chg_list[1], sizeof(uint32_t) * (size_t)need.chg_cap);
+    ALLOC(h->cand_list, sizeof(uint32_t) * (size_t)need.ntiles * kTileCells);  // never overflows
     ALLOC(h->ctrl, sizeof(CaCtrl));
-    ALLOC(h->hist_active, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
-    ALLOC(h->hist_changed, sizeof(unsigned long long) * (size_t)std::max(1, d->max_steps));
+    ALLOC(h->hist_active, sizeof(unsigned long long) * (size_t)need.hist);
+    ALLOC(h->hist_changed, sizeof(unsigned long long) * (size_t)need.hist);
+    ALLOC(h->spill, sizeof(int32_t) * need.cols);
+    ALLOC(h->heights_dev, sizeof(int32_t) * need.cols);
 #undef ALLOC
-    if ((e = cudaMemsetAsync(h->drop_plane, 0xFF, n, h->stream)) != cudaSuccess) return fail(cuda_fail(e, "cudaMemsetAsync"));
-    if (vca_status st = encode_maps(h)) return fail(st);
+    h->cap = need;
     e = cudaMallocHost(&h->ctrl_host, sizeof(CaCtrl));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
-    if (vca_status st = clear_planes(h)) return fail(st);
-    int per_sm = 0;
     e = cudaFuncSetAttribute(ca_rules_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRulesDynSmem);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ca_rules_kernel, kThreads, kRulesDynSmem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->rules_per_sm, ca_rules_kernel, kThreads, kRulesDynSmem);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
-    h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)prop.multiProcessorCount * std::max(1, per_sm));
-    int cand_per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cand_per_sm, ca_cand_kernel, kCandThreads, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->cand_per_sm, ca_cand_kernel, kCandThreads, 0);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
-    h->cand_blocks = prop.multiProcessorCount * std::max(1, cand_per_sm);  // one wave
     if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&h->ring_ev[0], cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&h->ring_ev[1], cudaEventDisableTiming)) != cudaSuccess)
@@ -1799,11 +1838,43 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     if ((e = cudaMallocHost(&h->ctrl_ring, 2 * sizeof(CaCtrl))) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
     const char* prof = std::getenv("VCA_PROFILE_KERNELS");
     h->profile_kernels = prof != nullptr && prof[0] == '1';
-    vca_vent none{0, 0, 0, 0};
-    if (vca_status s = upload_vents(h, &none, 0)) return fail(s);
-    e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamSynchronize"));
+    if (vca_status s = configure(h, d)) return fail(s);
     *out = h;
+    return VCA_OK;
+}
+
+vca_status vca_ca_reconfigure(vca_ca* h, const vca_ca_desc* d) {
+    if (vca_status s = check(h)) return s;
+    if (d == nullptr) {
+        set_error("vca_ca_reconfigure: null desc");
+        return VCA_ERR_ARG;
+    }
+    if (vca_status s = validate_desc(d, "vca_ca_reconfigure")) return s;
+    if (d->device != h->device) {
+        set_error("vca_ca_reconfigure: the handle lives on another device");
+        return VCA_ERR_ARG;
+    }
+    const CaSizes need = sizes_of(d);
+    if (need.plane_cells > h->cap.plane_cells || need.ntiles > h->cap.ntiles || need.chg_cap > h->cap.chg_cap ||
+        need.cols > h->cap.cols || need.hist > h->cap.hist) {
+        set_error("vca_ca_reconfigure: the grid does not fit the handle's device memory (vca_ca_footprint)");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    return configure(h, d);
+}
+
+vca_status vca_ca_footprint(const vca_ca_desc* d, uint64_t* bytes) {
+    if (d == nullptr || bytes == nullptr) {
+        set_error("vca_ca_footprint: null argument");
+        return VCA_ERR_ARG;
+    }
+    if (vca_status s = validate_desc(d, "vca_ca_footprint")) return s;
+    const CaSizes z = sizes_of(d);
+    *bytes = 2 * 13 * (uint64_t)z.plane_cells + 2 * (uint64_t)z.plane_cells  // state x 2, desc, drop
+             + 4 * 5 * (uint64_t)z.ntiles                                     // tile lists, flags, marks
+             + 4 * (uint64_t)z.ntiles * kTileCells                            // candidate list
+             + 2 * 4 * (uint64_t)z.chg_cap + 2 * 8 * (uint64_t)z.hist + 2 * 4 * (uint64_t)z.cols + sizeof(CaCtrl);
     return VCA_OK;
 }
 
@@ -1842,8 +1913,6 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
         }
     }
     const std::vector<int32_t> spill = fill_depressions(hv, g.nx, g.ny, g.per[0] != 0, g.per[1] != 0);
-    if (h->spill == nullptr) VCA_CUDA(cudaMalloc(&h->spill, sizeof(int32_t) * cols));
-    if (h->heights_dev == nullptr) VCA_CUDA(cudaMalloc(&h->heights_dev, sizeof(int32_t) * cols));
     VCA_CUDA(cudaMemcpyAsync(h->heights_dev, hv.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->spill, spill.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
     const int cur = h->steps & 1;

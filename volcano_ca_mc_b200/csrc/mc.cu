@@ -612,6 +612,7 @@ struct vca_mc {
     int parity_colors = 0;
     int classes[3] = {1, 1, 1};
     uint64_t n = 0;
+    uint64_t cap_n = 0;                  // cells the per-cell buffers hold (a resident handle runs smaller spaces)
     int32_t* spin = nullptr;
     uint8_t* domain = nullptr;
     float* mobility = nullptr;     // N floats when set
@@ -738,54 +739,29 @@ vca_status sweeps_grid(vca_mc* h, int* grid) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-vca_status vca_mc_create(const vca_mc_desc* d, vca_mc** out) {
-    if (!d || !out) {
-        set_error("vca_mc_create: null argument");
+vca_status mc_validate(const vca_mc_desc* d, const char* who) {
+    auto bad = [&](const std::string& m) {
+        set_error(std::string(who) + ": " + m);
         return VCA_ERR_ARG;
-    }
-    *out = nullptr;
-    if (d->nx < 1 || d->ny < 1 || d->nz < 1 || (d->nx > 1) + (d->ny > 1) + (d->nz > 1) < 2) {
-        set_error("vca_mc_create: the space must be 2D or 3D");
-        return VCA_ERR_ARG;
-    }
-    const uint64_t n = (uint64_t)d->nx * d->ny * d->nz;
-    if (n > 2000000000ULL) {
-        set_error("vca_mc_create: more than 2 000 000 000 cells");
-        return VCA_ERR_ARG;
-    }
-    if (d->Q < 2) {
-        set_error("vca_mc_create: Q must be at least 2 (PottsMC needs two orientations)");
-        return VCA_ERR_ARG;
-    }
-    if (!(d->J > 0.0) || !(d->kT >= 0.0)) {
-        set_error("vca_mc_create: J must be > 0 and kT >= 0");
-        return VCA_ERR_ARG;
-    }
-    vca_mc* h = new vca_mc();
-    h->desc = *d;
-    h->device = d->device;
-    h->n = n;
-    if (!build_nb(d->neighborhood, d->nx, d->ny, d->nz, h->nb_host)) {
-        delete h;
-        set_error("vca_mc_create: the hexagonal neighbourhood is defined in 2D only");
-        return VCA_ERR_ARG;
-    }
-    auto fail = [&](vca_status s) {
-        mc_free(h);
-        delete h;
-        return s;
     };
-    cudaError_t e = cudaSetDevice(d->device);
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
-    cudaDeviceProp prop;
-    if ((e = cudaGetDeviceProperties(&prop, d->device)) != cudaSuccess) return fail(cuda_fail(e, "cudaGetDeviceProperties"));
-    if (prop.major < 10) {
-        set_error("vca_mc_create: needs an sm_100 (Blackwell) device");
-        return fail(VCA_ERR_CUDA);
-    }
-    h->sms = prop.multiProcessorCount;
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1 || (d->nx > 1) + (d->ny > 1) + (d->nz > 1) < 2)
+        return bad("the space must be 2D or 3D");
+    if ((uint64_t)d->nx * d->ny * d->nz > 2000000000ULL) return bad("more than 2 000 000 000 cells");
+    if (d->Q < 2) return bad("Q must be at least 2 (PottsMC needs two orientations)");
+    if (!(d->J > 0.0) || !(d->kT >= 0.0)) return bad("J must be > 0 and kT >= 0");
+    NbTable nb;
+    if (!build_nb(d->neighborhood, d->nx, d->ny, d->nz, nb)) return bad("the hexagonal neighbourhood is defined in 2D only");
+    return VCA_OK;
+}
+
+// The space and parameters of an MC handle: neighbourhood, periodic axes, colours, acceptance
+// table; orientations and domain cleared.  Allocates nothing.
+vca_status mc_configure(vca_mc* h, const vca_mc_desc* d) {
+    h->desc = *d;
+    h->n = (uint64_t)d->nx * d->ny * d->nz;
+    build_nb(d->neighborhood, d->nx, d->ny, d->nz, h->nb_host);
     // Periodic axes: PottsMC ctor (PottsMC.cpp:18) with the Boundary of McStage::run (McStage.cpp:106).
     const bool periodic = d->boundary == VCA_BC_PERIODIC;
     h->per[0] = periodic && d->nx > 1;
@@ -796,6 +772,7 @@ vca_status vca_mc_create(const vca_mc_desc* d, vca_mc** out) {
     bool odd = false;
     for (int a = 0; a < 3; ++a) odd = odd || (h->per[a] && dims[a] % 2 == 1);
     h->parity_colors = d->neighborhood == VCA_NB_VON_NEUMANN && !odd;
+    for (int a = 0; a < 3; ++a) h->classes[a] = 1;
     if (h->parity_colors) {
         h->colors = 2;
     } else {
@@ -820,25 +797,91 @@ vca_status vca_mc_create(const vca_mc_desc* d, vca_mc** out) {
             }
             table[b * kTableSide + a] = v;
         }
+    VCA_CUDA(cudaMemcpyAsync(h->nb, &h->nb_host, sizeof(NbTable), cudaMemcpyHostToDevice, h->stream));
+    VCA_CUDA(cudaMemcpyAsync(h->table, table.data(), 8 * table.size(), cudaMemcpyHostToDevice, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->spin, 0, 4 * h->n, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->domain, 0, h->n, h->stream));
+    VCA_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    h->domain_set = false;
+    h->mobility_set = false;
+    h->mobility_on = false;
+    h->initialized = false;
+    h->color_off.assign(1, 0);
+    return VCA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vca_status vca_mc_create(const vca_mc_desc* d, vca_mc** out) {
+    if (!d || !out) {
+        set_error("vca_mc_create: null argument");
+        return VCA_ERR_ARG;
+    }
+    *out = nullptr;
+    if (vca_status s = mc_validate(d, "vca_mc_create")) return s;
+    const uint64_t n = (uint64_t)d->nx * d->ny * d->nz;
+    vca_mc* h = new vca_mc();
+    h->device = d->device;
+    h->cap_n = n;
+    auto fail = [&](vca_status s) {
+        mc_free(h);
+        delete h;
+        return s;
+    };
+    cudaError_t e = cudaSetDevice(d->device);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, d->device)) != cudaSuccess) return fail(cuda_fail(e, "cudaGetDeviceProperties"));
+    if (prop.major < 10) {
+        set_error("vca_mc_create: needs an sm_100 (Blackwell) device");
+        return fail(VCA_ERR_CUDA);
+    }
+    h->sms = prop.multiProcessorCount;
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
     if ((e = cudaMalloc(&h->nb, sizeof(NbTable))) != cudaSuccess || (e = cudaMalloc(&h->spin, 4 * n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->domain, n)) != cudaSuccess || (e = cudaMalloc(&h->table, 8 * table.size())) != cudaSuccess ||
+        (e = cudaMalloc(&h->domain, n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->table, 8 * kTableSide * kTableSide)) != cudaSuccess ||
         (e = cudaMalloc(&h->ctrl, sizeof(McCtrl))) != cudaSuccess)
         return fail(cuda_fail(e, "cudaMalloc"));
     if ((e = cudaMallocHost(&h->ctrl_host, sizeof(McCtrl))) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
-    if ((e = cudaMemcpyAsync(h->nb, &h->nb_host, sizeof(NbTable), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(h->table, table.data(), 8 * table.size(), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->spin, 0, 4 * n, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->domain, 0, n, h->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(h->ctrl, 0, sizeof(McCtrl), h->stream)) != cudaSuccess)
-        return fail(cuda_fail(e, "upload"));
     if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaEventCreate"));
     const char* prof = std::getenv("VCA_PROFILE_KERNELS");
     h->profile_kernels = prof != nullptr && prof[0] == '1';
-    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return fail(cuda_fail(e, "cudaStreamSynchronize"));
+    if (vca_status s = mc_configure(h, d)) return fail(s);
     *out = h;
+    return VCA_OK;
+}
+
+vca_status vca_mc_reconfigure(vca_mc* h, const vca_mc_desc* d) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!d) {
+        set_error("vca_mc_reconfigure: null desc");
+        return VCA_ERR_ARG;
+    }
+    if (vca_status s = mc_validate(d, "vca_mc_reconfigure")) return s;
+    if (d->device != h->device || (uint64_t)d->nx * d->ny * d->nz > h->cap_n) {
+        set_error("vca_mc_reconfigure: the space does not fit the handle (more cells, or another device)");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    return mc_configure(h, d);
+}
+
+vca_status vca_mc_footprint(const vca_mc_desc* d, uint64_t* bytes) {
+    if (!d || !bytes) {
+        set_error("vca_mc_footprint: null argument");
+        return VCA_ERR_ARG;
+    }
+    if (vca_status s = mc_validate(d, "vca_mc_footprint")) return s;
+    const uint64_t n = (uint64_t)d->nx * d->ny * d->nz;
+    // spin 4 + domain 1 + mobility 4 + mobility scratch 4 + colour lists 8 + grain labels 12 bytes per cell,
+    // the list-selection scratch (bounded by 4 bytes per cell), tables and counters
+    *bytes = 37 * n + 8 * kTableSide * kTableSide + sizeof(McCtrl) + 8 * 28 + sizeof(NbTable) + 4096;
     return VCA_OK;
 }
 
@@ -865,7 +908,7 @@ vca_status vca_mc_set_mobility(vca_mc* h, const float* mobility) {
         h->mobility_on = false;
         return VCA_OK;
     }
-    if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->n));
+    if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->cap_n));
     VCA_CUDA(cudaMemcpyAsync(h->mobility, mobility, 4 * h->n, cudaMemcpyHostToDevice, h->stream));
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->mobility_set = true;
@@ -910,8 +953,8 @@ vca_status vca_mc_set_mobility_from_ca(vca_mc* h, vca_ca* ca, double mobility_mi
     }
     VCA_CUDA(cudaSetDevice(h->device));
     VCA_CUDA(cudaStreamSynchronize(v.stream));
-    if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->n));
-    if (!h->scratch) VCA_CUDA(cudaMalloc(&h->scratch, 4 * (3 + h->n)));
+    if (!h->mobility) VCA_CUDA(cudaMalloc(&h->mobility, 4 * h->cap_n));
+    if (!h->scratch) VCA_CUDA(cudaMalloc(&h->scratch, 4 * (3 + h->cap_n)));
     unsigned int* scratch = h->scratch;  // [end, min, max] + time[n]
     const unsigned int init[3] = {0u, 0xFFFFFFFFu, 0u};
     VCA_CUDA(cudaMemcpyAsync(scratch, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
@@ -1134,9 +1177,9 @@ vca_status vca_mc_grains(vca_mc* h, int moore, double mobility_threshold, vca_mc
     }
     VCA_CUDA(cudaSetDevice(h->device));
     if (!h->gparent) {
-        VCA_CUDA(cudaMalloc(&h->gparent, 4 * h->n));
-        VCA_CUDA(cudaMalloc(&h->gsize, 4 * h->n));
-        VCA_CUDA(cudaMalloc(&h->ghigh, 4 * h->n));
+        VCA_CUDA(cudaMalloc(&h->gparent, 4 * h->cap_n));
+        VCA_CUDA(cudaMalloc(&h->gsize, 4 * h->cap_n));
+        VCA_CUDA(cudaMalloc(&h->ghigh, 4 * h->cap_n));
         VCA_CUDA(cudaMalloc(&h->gacc, sizeof(GrainAcc)));
     }
     GrainAcc* acc = static_cast<GrainAcc*>(h->gacc);

@@ -119,8 +119,22 @@ vca_status ca_view(vca_ca* h, CaView* v);
 
 }  // namespace vca
 
+namespace vca {
+// Device allocation sizes of a CA handle (a resident handle runs any space that fits them).
+struct CaSizes {
+    size_t plane_cells = 0;   // P * ny * nz
+    uint64_t ntiles = 0;
+    uint32_t chg_cap = 0;
+    size_t cols = 0;          // nx * ny
+    int hist = 0;             // steps of history
+};
+}  // namespace vca
+
 struct vca_ca {
     vca::CaTensorMaps tmaps;  // first member: CUtensorMap needs 64-byte alignment
+    vca::CaSizes cap;         // what the device buffers can hold
+    int sms = 0, rules_per_sm = 0, cand_per_sm = 0;
+    size_t vent_cap = 0;
     vca_ca_desc desc;
     vca::CaGeom geom;
     vca::CaTables tables_host;
