@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large", action="store_true", help="skip the full-size 1024x1024x256 sub-benchmark")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched job-mix sub-benchmark")
+    ap.add_argument("--no-served", action="store_true", help="skip the served (Poisson arrivals) sub-benchmark")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served arrival trace")
+    ap.add_argument("--slots", type=int, default=16, help="worker slots of the batched and served runs")
     ap.add_argument("--profile-job", choices=["active", "dense"], default=None,
                     help="run exactly one CA job with this schedule (no warm-up, no MC) and exit: the case "
                          "ncu captures")
@@ -259,6 +263,36 @@ class E2E:
         self.ca.close()
 
 
+def job_mixes(args, device):
+    """Many small independent jobs on one GPU through the job server (resident handles, footprint
+    admission): a batch of 96 jobs drawn from master seed 2026, run on `slots` workers and one at a
+    time, and a Poisson trace (20 jobs/s, master seed 77) replayed in real time the same two ways.
+    Every job's result hash must agree between the two runs."""
+    from volcano_ca_mc_b200 import serve
+
+    keys = ("slots", "jobs", "makespan_s", "jobs_per_s", "cell_updates_per_s", "p50_s", "p99_s", "mean_concurrency")
+    out = {}
+    if not args.no_batched:
+        jobs = serve.make_mix(96, 2026)
+        many = serve.run(jobs, slots=args.slots, device=device)
+        one = serve.run(jobs, slots=1, device=device)
+        out["batched"] = {"mix": "96 jobs, master seed 2026: 2D sides 128-2048, 3D sides 64-256 (z = side/2), "
+                                 "200-600 CA steps, 20-100 MCS",
+                          "cells": sum(j.cells for j in jobs), **{k: many[k] for k in keys},
+                          "phase_ms_total": many["phase_ms_total"],
+                          "one_at_a_time": {k: one[k] for k in keys}, "mismatches": serve.compare(many, one)}
+    if not args.no_served:
+        rate = 20.0
+        trace = serve.make_mix(max(1, int(rate * args.serve_seconds)), 77, rate_hz=rate)
+        many = serve.run(trace, slots=args.slots, realtime=True, device=device)
+        one = serve.run(trace, slots=1, realtime=True, device=device)
+        out["served"] = {"trace": f"{len(trace)} jobs, Poisson arrivals at {rate:g} jobs/s, master seed 77, "
+                                  "replayed in real time; latency = completion - arrival",
+                         **{k: many[k] for k in keys}, "phase_ms_total": many["phase_ms_total"],
+                         "one_at_a_time": {k: one[k] for k in keys}, "mismatches": serve.compare(many, one)}
+    return out
+
+
 def cpu_baseline(w):
     """The reference engine on one job of the workload, all host threads."""
     from oracle import oracle as O
@@ -390,7 +424,9 @@ def ours(args):
                                                              f"cuda:{local}", world)
     cpu = None
     eng = None
+    mixes = {}
     if rank == 0 and world == 1:
+        mixes = job_mixes(args, local)
         eng = engine_cli(w)
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(w)
@@ -431,6 +467,7 @@ def ours(args):
     }
     if large is not None:
         line["large"] = large
+    line.update(mixes)
     if eng is not None:
         line["engine_cli"] = eng
     if cpu is not None:

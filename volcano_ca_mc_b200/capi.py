@@ -370,8 +370,10 @@ class PottsMC:
         _check(lib().vca_mc_grains(self.h, int(moore), threshold, ctypes.byref(out)), "vca_mc_grains")
         return out
 
-    def crystals(self) -> np.ndarray:
-        out = np.empty(self.n, np.int32)
+    def crystals(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Orientations (N int32), into a new array or into ``out`` (e.g. a view of pinned memory)."""
+        if out is None:
+            out = np.empty(self.n, np.int32)
         _check(lib().vca_mc_crystals(self.h, _ptr(out)), "vca_mc_crystals")
         return out
 

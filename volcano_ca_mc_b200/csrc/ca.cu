@@ -1521,6 +1521,7 @@ void free_all(vca_ca* h) {
     cudaFree(h->spill);
     cudaFree(h->heights_dev);
     cudaFree(h->vents);
+    cudaFree(h->seeds_dev);
     cudaFree(h->ctrl);
     cudaFree(h->hist_active);
     cudaFree(h->hist_changed);
@@ -1958,13 +1959,22 @@ vca_status vca_ca_place_seeds(vca_ca* h, const vca_vent* vents, int count) {
         for (size_t i = 0; i < keyed.size(); ++i)
             if (i + 1 == keyed.size() || keyed[i + 1].first != keyed[i].first) uniq.push_back(seeds[(size_t)keyed[i].second]);
         const int nu = (int)uniq.size();
-        int4* ds = nullptr;
-        VCA_CUDA(cudaMalloc(&ds, sizeof(int4) * (size_t)nu));
-        VCA_CUDA(cudaMemcpyAsync(ds, uniq.data(), sizeof(int4) * (size_t)nu, cudaMemcpyHostToDevice, h->stream));
-        ca_seed_kernel<<<std::min(1184, (nu + 255) / 256), 256, 0, h->stream>>>(make_args(h), ds, nu, cur, temp);
+        // a grow-only buffer: a cudaFree per call would wait for every stream of the device
+        if ((size_t)nu > h->seed_cap) {
+            VCA_CUDA(cudaStreamSynchronize(h->stream));
+            cudaFree(h->seeds_dev);
+            h->seeds_dev = nullptr;
+            h->seed_cap = 0;
+            const size_t cap = std::max<size_t>((size_t)nu, 1024);
+            VCA_CUDA(cudaMalloc(&h->seeds_dev, sizeof(int4) * cap));
+            h->seed_cap = cap;
+        }
+        VCA_CUDA(cudaMemcpyAsync(h->seeds_dev, uniq.data(), sizeof(int4) * (size_t)nu, cudaMemcpyHostToDevice,
+                                 h->stream));
+        ca_seed_kernel<<<std::min(1184, (nu + 255) / 256), 256, 0, h->stream>>>(make_args(h), h->seeds_dev, nu, cur,
+                                                                                 temp);
         VCA_CUDA(cudaGetLastError());
         VCA_CUDA(cudaStreamSynchronize(h->stream));
-        cudaFree(ds);
         h->launches += 1;
     }
     if (vca_status s = upload_vents(h, vents, count)) return s;

@@ -1017,14 +1017,15 @@ vca_status vca_mc_initialize(vca_mc* h) {
         cudaFree(h->list_mob);
         h->list = nullptr;
         h->list_mob = nullptr;
-        h->list_cap = std::max<uint64_t>(total, 1);
+        h->list_cap = std::max<uint64_t>(std::max<uint64_t>(total, h->cap_n), 1);  // once per handle
         VCA_CUDA(cudaMalloc(&h->list, 4 * h->list_cap));
         VCA_CUDA(cudaMalloc(&h->list_mob, 4 * h->list_cap));
     }
     ColorPred pred{a, h->domain, 0};
     thrust::counting_iterator<uint32_t> it(0);
     size_t temp_bytes = 0;
-    VCA_CUDA(cub::DeviceSelect::If(nullptr, temp_bytes, it, h->list, h->d_count, (int64_t)h->n, pred, h->stream));
+    // sized for the capacity, so that later, larger spaces on a resident handle allocate nothing
+    VCA_CUDA(cub::DeviceSelect::If(nullptr, temp_bytes, it, h->list, h->d_count, (int64_t)h->cap_n, pred, h->stream));
     if (temp_bytes > h->cub_temp_bytes) {
         cudaFree(h->cub_temp);
         h->cub_temp = nullptr;

@@ -134,7 +134,7 @@ struct vca_ca {
     vca::CaTensorMaps tmaps;  // first member: CUtensorMap needs 64-byte alignment
     vca::CaSizes cap;         // what the device buffers can hold
     int sms = 0, rules_per_sm = 0, cand_per_sm = 0;
-    size_t vent_cap = 0;
+    size_t vent_cap = 0, seed_cap = 0;
     vca_ca_desc desc;
     vca::CaGeom geom;
     vca::CaTables tables_host;
@@ -156,6 +156,7 @@ struct vca_ca {
     int cand_blocks = 0;      // grid of the candidate pass
     int32_t* spill = nullptr;
     int4* vents = nullptr;
+    int4* seeds_dev = nullptr;  // unique seed cells of place_seeds (grows only)
     int vent_slots = 0;
     vca::CaCtrl* ctrl = nullptr;
     vca::CaCtrl* ctrl_host = nullptr;   // pinned mirror

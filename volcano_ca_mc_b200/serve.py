@@ -131,41 +131,82 @@ def make_mix(n: int, master_seed: int, share_3d: float = 0.3, rate_hz: float | N
     return jobs
 
 
+class ResultBuffers:
+    """Pinned host buffers that jobs' results are downloaded into and handed to the consumer in.
+    A slot takes a free buffer set for each job and is released as soon as the result is in it; the
+    consumer (here the result hash) returns the set when it is done, so a slow consumer holds back
+    new jobs only when every set is taken."""
+
+    def __init__(self, cap_cells: int, count: int):
+        import torch
+        pin = lambda dt: torch.empty(cap_cells, dtype=dt, pin_memory=True).numpy()
+        self.free: queue.Queue = queue.Queue()
+        for _ in range(count):
+            self.free.put((pin(torch.uint8), pin(torch.int32), pin(torch.float32), pin(torch.int16).view("uint16"),
+                           pin(torch.int16).view("uint16"), pin(torch.int32)))
+
+    def get(self):
+        return self.free.get()
+
+    def put(self, bufs):
+        self.free.put(bufs)
+
+
 class Slot:
-    """A worker's resident handles, sized for the largest job it may get."""
+    """A worker's resident CA and MC handles, sized for the largest job it may get."""
 
     def __init__(self, cap: JobSpec, device: int):
         self.device = device
         self.ca = capi.LavaCA(cap.ca_params(device))
         self.mc = capi.PottsMC(cap.mc_params(device))
+        # one small job first: the handles' set-up buffers are allocated on first use, sized for the
+        # capacity, so no job of the trace waits on a device-wide allocation
+        three_d = cap.ny > 1
+        self.run(JobSpec(job_id=-2, nx=32 if three_d else 64, ny=32 if three_d else 1, nz=16 if three_d else 64,
+                         neighborhood="moore", boundary="absorbing", seed=1, max_steps=8, n_vents=1, Q=32, kT=0.0,
+                         mcs=1))
 
-    def run(self, job: JobSpec) -> dict:
+    def run(self, job: JobSpec, bufs=None) -> tuple[dict, tuple]:
+        """Runs the job; returns its record and its result arrays (the five CA planes and the crystal
+        orientations, views of ``bufs`` when given)."""
+        t = [time.perf_counter()]
         heights, vents = job.terrain()
         self.ca.reconfigure(job.ca_params(self.device))
         self.ca.apply_terrain(heights)
         self.ca.place_seeds(vents)
+        t.append(time.perf_counter())
         self.ca.run()
         info = self.ca.info()
-        planes = self.ca.download()
+        t.append(time.perf_counter())
+        n = job.cells
+        planes = self.ca.download(None if bufs is None else tuple(a[:n] for a in bufs[:5]))
+        t.append(time.perf_counter())
         self.mc.reconfigure(job.mc_params(self.device))
         self.mc.set_domain_from_ca(self.ca)
         self.mc.set_mobility_from_ca(self.ca, 0.05, True)
         self.mc.initialize()
         self.mc.sweep(job.mcs)
         g = self.mc.grains(moore=job.neighborhood != "von_neumann")
-        crystals = self.mc.crystals()
-        h = hashlib.sha256()
-        for a in planes:
-            h.update(memoryview(a).cast("B"))
-        h.update(memoryview(crystals).cast("B"))
+        crystals = self.mc.crystals(None if bufs is None else bufs[5][:n])
         mi = self.mc.info()
-        return {"job": job.job_id, "steps": info.steps, "stop": info.stop_reason, "sha": h.hexdigest()[:24],
-                "energy": self.mc.energy(), "grains": g.grains, "attempts": mi.attempts,
-                "cell_updates": job.cells * info.steps}
+        energy = self.mc.energy()
+        t.append(time.perf_counter())
+        rec = {"job": job.job_id, "steps": info.steps, "stop": info.stop_reason, "energy": energy, "grains": g.grains,
+               "attempts": mi.attempts, "cell_updates": job.cells * info.steps, "done": t[-1],
+               "phases_ms": {k: round((t[i + 1] - t[i]) * 1e3, 3)
+                             for i, k in enumerate(("setup", "ca", "download", "mc"))}}
+        return rec, (*planes, crystals)
 
     def close(self):
         self.mc.close()
         self.ca.close()
+
+
+def result_hash(arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(memoryview(np.ascontiguousarray(a)).cast("B"))
+    return h.hexdigest()[:24]
 
 
 def capacity(jobs: list[JobSpec]) -> JobSpec:
@@ -186,6 +227,7 @@ def run(jobs: list[JobSpec], slots: int = 8, budget_bytes: int = 120 << 30, real
     pool: queue.Queue = queue.Queue()
     for _ in range(slots):
         pool.put({k: Slot(c, device) for k, c in caps.items()})
+    results = {k: ResultBuffers(c.cells, slots + 4) for k, c in caps.items()}
     lock = threading.Condition()
     in_use = [0]
     records: dict[int, dict] = {}
@@ -196,16 +238,26 @@ def run(jobs: list[JobSpec], slots: int = 8, budget_bytes: int = 120 << 30, real
     t0 = time.perf_counter()
 
     def worker(job: JobSpec, slot_set: dict, start: float, fp: int):
+        dim = "3d" if job.ny > 1 else "2d"
+        bufs = results[dim].get()
+        rec = None
         try:
-            res = slot_set["3d" if job.ny > 1 else "2d"].run(job)
-            records[job.job_id] = {"arrival": job.arrival_s, "start": start, "end": time.perf_counter() - t0, **res}
+            rec, arrays = slot_set[dim].run(job, bufs)
         except BaseException as e:  # reported after the run
             errors.append(e)
-        finally:
+        finally:  # the slot is free once the result is in host memory
             pool.put(slot_set)
             with lock:
                 in_use[0] -= fp
                 lock.notify_all()
+        try:  # the consumer: checks the result, then gives the buffers back
+            if rec is not None:
+                rec["sha"] = result_hash(arrays)
+                records[job.job_id] = {"arrival": job.arrival_s, "start": start, "end": rec.pop("done") - t0, **rec}
+        except BaseException as e:
+            errors.append(e)
+        finally:
+            results[dim].put(bufs)
 
     threads = []
     for job in order:
@@ -224,14 +276,21 @@ def run(jobs: list[JobSpec], slots: int = 8, budget_bytes: int = 120 << 30, real
         threads.append(th)
     for th in threads:
         th.join()
-    makespan = time.perf_counter() - t0
     while not pool.empty():
         for s in pool.get().values():
             s.close()
     if errors:
         raise errors[0]
+    makespan = max((r["end"] for r in records.values()), default=0.0)  # the last result in host memory
     lat = np.array([r["end"] - (r["arrival"] if realtime else 0.0) for r in records.values()])
+    busy = sum(r["end"] - r["start"] for r in records.values())
+    phases = {}
+    for r in records.values():
+        for k, v in r["phases_ms"].items():
+            phases[k] = phases.get(k, 0.0) + v
     return {"records": records, "slots": slots, "makespan_s": makespan, "jobs": len(records),
+            "mean_concurrency": busy / makespan if makespan > 0 else 0.0,
+            "phase_ms_total": {k: round(v, 1) for k, v in phases.items()},
             "jobs_per_s": len(records) / makespan if makespan > 0 else 0.0,
             "cell_updates_per_s": sum(r["cell_updates"] for r in records.values()) / makespan if makespan > 0 else 0.0,
             "p50_s": float(np.percentile(lat, 50)) if len(lat) else 0.0,
