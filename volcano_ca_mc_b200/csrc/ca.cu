@@ -72,6 +72,18 @@ __device__ __forceinline__ bool halo_axis(int& v, int n, int periodic) {
     return wrap_axis(v, n, periodic);
 }
 __device__ __forceinline__ bool solid_ground(int t) { return t == kRock || t == kBasalt; }
+// resolve() for a neighbour one cell away, as selects instead of branches, so that the loads of
+// all neighbours of a cell can be issued together.  v is only meaningful when the result is true.
+__device__ __forceinline__ bool wrap1_sel(int& v, int n, int periodic) {
+    const bool in = (unsigned)v < (unsigned)n;
+    const int w = v < 0 ? v + n : v - n;
+    v = in ? v : w;
+    return in | ((periodic != 0) & (n > 1));
+}
+__device__ __forceinline__ bool resolve1_sel(const CaGeom& g, int& x, int& y, int& z) {
+    const bool a = wrap1_sel(x, g.nx, g.per[0]), b = wrap1_sel(y, g.ny, g.per[1]), c = wrap1_sel(z, g.nz, g.per[2]);
+    return a & b & c;
+}
 
 // CandidateVote (engine/src/ca/CaRules.hpp:127-183).
 struct Vote {
@@ -247,15 +259,13 @@ __device__ void drop_rescan18(const CaKernelArgs& k, const uint8_t* T, int x, in
     uint64_t air = 0, solid = 0, lava = 0;
 #pragma unroll
     for (int i = 0; i < kWin; ++i) {
+        // clamped loads without branches, so that all 35 are in flight together
         const int z = b + i;
-        if (z < 0) {
-            solid |= 1ull << i;
-        } else if (z < g.nz) {
-            const int t = T[col + zs * z];
-            air |= (uint64_t)(t == kAir) << i;
-            solid |= (uint64_t)(t == kRock || t == kBasalt) << i;
-            lava |= (uint64_t)(t == kLava) << i;
-        }
+        const bool in = z >= 0 && z < g.nz;
+        const int t = __ldg(T + col + zs * min(max(z, 0), g.nz - 1));
+        air |= (uint64_t)(in && t == kAir) << i;
+        solid |= (uint64_t)(z < 0 || (in && (t == kRock || t == kBasalt))) << i;
+        lava |= (uint64_t)(in && t == kLava) << i;
     }
     const int hi = min(g.nz, zc + kMaxDrop + 2);
     for (int z = zc; z < hi; ++z) {
@@ -330,14 +340,17 @@ __device__ __forceinline__ bool gather_vote(const CaKernelArgs& k, const uint8_t
     const NbTable& nb = k.tables.nb;
     const int var = nb.variants == 1 ? 0 : (int)fast_mod(hash_salt(hash_index(prefix, gidx), kSaltNeighborhood), k.var_mod);
     const int cnt = nb.count[var];
-    const int c_drop = k.classic ? 0 : (int)k.drop[pidx(g, x, y, z)];
+    const int64_t self = pidx(g, x, y, z);
+    const int c_drop = k.classic ? 0 : (int)k.drop[self];
+    // one round of independent loads: a neighbour outside the grid (or past the variant's count)
+    // reads the cell itself, which is AIR
     uint32_t lava_mask = 0;
 #pragma unroll
     for (int i = 0; i < 26; ++i) {
-        if (i < cnt) {
-            int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
-            if (resolve(g, sx, sy, sz) && __ldg(T + pidx(g, sx, sy, sz)) == kLava) lava_mask |= 1u << i;
-        }
+        int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
+        const bool ok = (i < cnt) & resolve1_sel(g, sx, sy, sz);
+        const int tv = __ldg(T + (ok ? pidx(g, sx, sy, sz) : self));
+        lava_mask |= (uint32_t)(tv == kLava) << i;
     }
     if (!lava_mask) return false;
     v.n = 0;
@@ -361,17 +374,17 @@ __device__ __forceinline__ bool gather_vote(const CaKernelArgs& k, const uint8_t
                 src[q] = i;
             }
         }
+        // the sources' flowId, temperature and D(n), again in one round (unused slots read the cell)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            if (src[q] < 0 || src[q] == 26) continue;
-            int sx = x + nb.off[var][src[q]][0], sy = y + nb.off[var][src[q]][1], sz = z + nb.off[var][src[q]][2];
-            resolve(g, sx, sy, sz);
-            const int64_t sp = pidx(g, sx, sy, sz);
+            const bool use = src[q] >= 0 && src[q] != 26;
+            const int i = use ? src[q] : 0;
+            int sx = x + nb.off[var][i][0], sy = y + nb.off[var][i][1], sz = z + nb.off[var][i][2];
+            resolve1_sel(g, sx, sy, sz);
+            const int64_t sp = use ? pidx(g, sx, sy, sz) : self;
             fl[q] = __ldg(F + sp);
-            if (!k.classic) {
-                te[q] = __ldg(Te + sp);
-                dsc[q] = k.desc[sp];
-            }
+            te[q] = __ldg(Te + sp);
+            dsc[q] = __ldg(k.desc + sp);
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -873,13 +886,35 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                 // or below its column's spill level (gatherLavaCandidates, LavaCA.hpp:462-519); in classic
                 // mode from any LAVA neighbour.
                 uint32_t near = 0;
-                const int dz_lo = lava_mode ? 0 : -hz_on;
-                for (int dz = dz_lo; dz <= hz_on; ++dz)
+                if (lava_mode) {
+                    // A same-level source needs dropDepth(c) == D(n) >= 0, a diagonal one above needs
+                    // dropDepth(c) == 0; a LAVA cell straight above always feeds (a fall).  Most AIR
+                    // cells next to LAVA lie over it (dropDepth -1) and are left out here.
+                    const uint32_t dc = win_mid(reinterpret_cast<const uint8_t*>(sl.drop) +
+                                                ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq);
+                    const uint32_t lands = __vcmpges4(dc, 0u), flat = __vcmpeq4(dc, 0u);
+                    uint32_t level = 0, above = 0, fall = 0;
                     for (int dy = -hy_on; dy <= hy_on; ++dy) {
-                        const uint8_t* rp = sl.type + (hr + dy + HY * dz) * kSmemRowBytes + kRowOff + 4 * xq;
-                        near |= __vcmpeq4(win_left(rp), 0x02020202u) | __vcmpeq4(win_mid(rp), 0x02020202u) |
-                                __vcmpeq4(win_right(rp), 0x02020202u);
+                        const uint8_t* rp = sl.type + (hr + dy) * kSmemRowBytes + kRowOff + 4 * xq;
+                        level |= __vcmpeq4(win_left(rp), 0x02020202u) | __vcmpeq4(win_mid(rp), 0x02020202u) |
+                                 __vcmpeq4(win_right(rp), 0x02020202u);
+                        if (hz_on) {
+                            const uint8_t* ap = rp + HY * kSmemRowBytes;
+                            const uint32_t mid = __vcmpeq4(win_mid(ap), 0x02020202u);
+                            above |= __vcmpeq4(win_left(ap), 0x02020202u) | __vcmpeq4(win_right(ap), 0x02020202u) |
+                                     (dy != 0 ? mid : 0u);
+                            if (dy == 0) fall = mid;
+                        }
                     }
+                    near = (level & lands) | (above & flat) | fall;
+                } else {
+                    for (int dz = -hz_on; dz <= hz_on; ++dz)
+                        for (int dy = -hy_on; dy <= hy_on; ++dy) {
+                            const uint8_t* rp = sl.type + (hr + dy + HY * dz) * kSmemRowBytes + kRowOff + 4 * xq;
+                            near |= __vcmpeq4(win_left(rp), 0x02020202u) | __vcmpeq4(win_mid(rp), 0x02020202u) |
+                                    __vcmpeq4(win_right(rp), 0x02020202u);
+                        }
+                }
                 if (stage_spill && k.ponding) {
                     uint32_t m = __vcmpeq4(win_mid(rowp - HY * kSmemRowBytes), 0x02020202u);
 #pragma unroll
@@ -1043,7 +1078,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
 // finishes the step (finishStep, LavaCA.hpp:1206-1229).
 // ------------------------------------------------------------------------------------------
 constexpr int kCandThreads = 128;
-__global__ __launch_bounds__(kCandThreads, 6) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
+__global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
     __shared__ unsigned long long s_red[kCandThreads / 32];
     __shared__ bool s_last;
     CaCtrl* ctrl = k.ctrl;
@@ -1057,6 +1092,10 @@ __global__ __launch_bounds__(kCandThreads, 6) void ca_cand_kernel(const __grid_c
     const uint32_t stamp = min(t, 65535u);
     const uint64_t prefix = hash_prefix(k.seed, t);
     const unsigned n = ctrl->cand_count;
+    // the blocks that hold listed cells take part (at least one, which finishes the step); the others
+    // leave at once, so a short list costs a few blocks instead of the whole grid
+    const unsigned parts = max(1u, min(gridDim.x, (n + kCandThreads - 1) / kCandThreads));
+    if (blockIdx.x >= parts) return;
     const int lane = threadIdx.x & 31;
     unsigned born = 0;
     const uint64_t stride = (uint64_t)gridDim.x * kCandThreads;
@@ -1109,7 +1148,7 @@ __global__ __launch_bounds__(kCandThreads, 6) void ca_cand_kernel(const __grid_c
             atomicAdd(&ctrl->acc_born, sb);
         }
         __threadfence();
-        s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
+        s_last = atomicAdd(&ctrl->ticket, 1u) == parts - 1;
     }
     __syncthreads();
     if (s_last && threadIdx.x == 0) {
