@@ -25,6 +25,10 @@ CASES = [
     (30, 30, 18, "von_neumann", "periodic", 60, 2),
     (40, 24, 20, "pentagonal", "absorbing", 60, 3),
     (65, 9, 21, "pentagonal", "periodic", 50, 2),
+    # periodic x with nx a multiple of 16: the wrapped frame columns come with the tile's TMA boxes
+    (64, 1, 40, "moore", "periodic", 100, 2),         # one tile in x: both ends wrap
+    (48, 20, 16, "pentagonal", "periodic", 50, 2),    # padded rows: the copy of x = 0 sits at x = nx
+    (128, 12, 12, "moore", "periodic", 50, 3),        # two tiles in x
 ]
 
 

@@ -601,6 +601,9 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 // Tiles at the grid edge get their frame cells (VOID, or the periodic copy) patched after the load.
 // ------------------------------------------------------------------------------------------
 constexpr int kSpillCols = kTileX * 4;  // columns of a tile with nz > 1 (TY <= 4)
+// a wrapped-x column buffer: 16 bytes per halo row (or drop row), each buffer 128-byte aligned
+constexpr int kXSideBytes = (kMaxHaloRows * 16 + 127) / 128 * 128;
+constexpr int kXSideDropBytes = (kMaxDropRows * 16 + 127) / 128 * 128;
 
 struct __align__(128) RulesSlot {
     int32_t flow[kTileCells];
@@ -611,9 +614,15 @@ struct __align__(128) RulesSlot {
     uint8_t type[kMaxHaloRows * kSmemRowBytes];
     int8_t drop[kMaxDropRows * kSmemRowBytes];
     int32_t spill[kSpillCols];
+    // wrapped x columns (periodic x): [0] the 16 cells ending at x = nx - 1 (left frame, byte 15 of
+    // each row), [1] the 16 cells from x = 0 (right frame or padded-row copy, byte 0)
+    __align__(128) uint8_t xside[2][kXSideBytes];
+    __align__(128) int8_t xside_drop[2][kXSideDropBytes];
 };
 static_assert(offsetof(RulesSlot, type) % 128 == 0 && offsetof(RulesSlot, drop) % 128 == 0 &&
-                  offsetof(RulesSlot, own_type) % 128 == 0 && offsetof(RulesSlot, solid) % 128 == 0,
+                  offsetof(RulesSlot, own_type) % 128 == 0 && offsetof(RulesSlot, solid) % 128 == 0 &&
+                  offsetof(RulesSlot, xside) % 128 == 0 && offsetof(RulesSlot, xside_drop) % 128 == 0 &&
+                  kXSideBytes % 128 == 0 && kXSideDropBytes % 128 == 0,
               "TMA destinations are 128-byte aligned");
 constexpr size_t kRulesDynSmem = 2 * sizeof(RulesSlot) + 128;
 
@@ -663,6 +672,8 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     // transaction bytes of one slot fill
     const uint32_t tx_copy = kTileCells * (1 + 4 + 4 + 2 + 2);
     const uint32_t tx_rules = kTileCells * (4 + 4 + 2 + 2) + kSmemRowBytes * halo_rows + (lava_mode ? kSmemRowBytes * drop_rows : 0);
+    const bool xwrap = g.per[0] && (g.nx & 15) == 0;  // the wrapped x columns come by TMA (16-cell aligned)
+    const uint32_t tx_xside = 16u * halo_rows + (lava_mode ? 16u * drop_rows : 0u);
     if (tid == 0) {
         s_flags[0] = s_flags[1] = 0;
         mbar_init(&s_bar[0], 1);
@@ -706,7 +717,9 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         if (tid == 0) {
             bulk_wait_read_all();
             fence_proxy_async();
-            mbar_arrive_expect_tx(&s_bar[s], rules ? tx_rules : tx_copy);
+            // periodic x: an x-edge tile also loads the column that holds its wrapped frame cells
+            const bool wl = rules && xwrap && x0 == 0, wr = rules && xwrap && x0 + kTileX >= g.nx;
+            mbar_arrive_expect_tx(&s_bar[s], (rules ? tx_rules : tx_copy) + (wl ? tx_xside : 0u) + (wr ? tx_xside : 0u));
             tma_load_3d(sl.flow, &k.tm.flow[cur], x0, y0, z0, &s_bar[s]);
             tma_load_3d(sl.temp, &k.tm.temp[cur], x0, y0, z0, &s_bar[s]);
             tma_load_3d(sl.solid, &k.tm.solid[cur], x0, y0, z0, &s_bar[s]);
@@ -714,6 +727,14 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             if (rules) {
                 tma_load_3d(sl.type, &k.tm.halo_type[cur], x0 - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
                 if (lava_mode) tma_load_3d(sl.drop, &k.tm.drop, x0 - 16, y0 - hy_on, z0, &s_bar[s]);
+                if (wl) {
+                    tma_load_3d(sl.xside[0], &k.tm.xside_type[cur], g.nx - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
+                    if (lava_mode) tma_load_3d(sl.xside_drop[0], &k.tm.xside_drop, g.nx - 16, y0 - hy_on, z0, &s_bar[s]);
+                }
+                if (wr) {
+                    tma_load_3d(sl.xside[1], &k.tm.xside_type[cur], 0, y0 - hy_on, z0 - hz_on, &s_bar[s]);
+                    if (lava_mode) tma_load_3d(sl.xside_drop[1], &k.tm.xside_drop, 0, y0 - hy_on, z0, &s_bar[s]);
+                }
             } else {
                 tma_load_3d(sl.own_type, &k.tm.own_type[cur], x0, y0, z0, &s_bar[s]);
             }
@@ -824,7 +845,10 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                     if (!(which == 2 && xpad < 0) &&
                         !(xx >= 0 && xx < g.nx && yy >= 0 && yy < g.ny && zz >= 0 && zz < g.nz)) {
                         frame_at = r * kSmemRowBytes + kRowOff + (xx - x0);
-                        if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
+                        const bool yz_in = yy >= 0 && yy < g.ny && zz >= 0 && zz < g.nz;
+                        if (xwrap && yz_in && (xx == -1 || xx == g.nx))
+                            frame_v = xx < 0 ? sl.xside[0][r * 16 + 15] : sl.xside[1][r * 16];  // loaded with the boxes
+                        else if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1]) && halo_axis(zz, g.nz, g.per[2]))
                             frame_v = T[pidx(g, xx, yy, zz)];
                     }
                 }
@@ -847,10 +871,14 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                         int yy = y0 - hy_on + r % HY;
                         const int zz = z0 + r / HY;
                         const int at = r * kSmemRowBytes + kRowOff + (xx - x0);
-                        if (!(which == 2 && xpad < 0) && zz < g.nz && !(xx >= 0 && xx < g.nx && yy >= 0 && yy < g.ny) &&
-                            halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) {
-                            dframe_at = at;
-                            dframe_v = k.drop[pidx(g, xx, yy, zz)];
+                        if (!(which == 2 && xpad < 0) && zz < g.nz && !(xx >= 0 && xx < g.nx && yy >= 0 && yy < g.ny)) {
+                            if (xwrap && yy >= 0 && yy < g.ny && (xx == -1 || xx == g.nx)) {
+                                dframe_at = at;
+                                dframe_v = sl.xside_drop[xx < 0 ? 0 : 1][r * 16 + (xx < 0 ? 15 : 0)];
+                            } else if (halo_axis(xx, g.nx, g.per[0]) && halo_axis(yy, g.ny, g.per[1])) {
+                                dframe_at = at;
+                                dframe_v = k.drop[pidx(g, xx, yy, zz)];
+                            }
                         }
                     }
                 }
@@ -1652,6 +1680,11 @@ vca_status encode_maps(vca_ca* h) {
         if (vca_status s = encode_plane(&m.arrival[b], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->arrival[b], g, kTileX, TY, TZ, "arrivalStep"))
             return s;
     }
+    for (int b = 0; b < 2; ++b)
+        if (vca_status s = encode_plane(&m.xside_type[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->type[b], g, 16, HY, HZ, "type column"))
+            return s;
+    if (vca_status s = encode_plane(&m.xside_drop, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->drop_plane, g, 16, HY, TZ, "drop column"))
+        return s;
     return encode_plane(&m.drop, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->drop_plane, g, kTileX + 32, HY, TZ, "drop depth");
 }
 

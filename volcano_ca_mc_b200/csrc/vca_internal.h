@@ -68,6 +68,10 @@ struct CaTables {
 // z0 - 1), and the drop-depth rows {96, TY + 2, TZ} from (x0 - 16, y0 - 1, z0).
 struct CaTensorMaps {
     CUtensorMap own_type[2], halo_type[2], flow[2], temp[2], solid[2], arrival[2], drop;
+    // 16-cell-wide columns of the type halo rows {16, TY + 2, TZ + 2} and of the drop rows
+    // {16, TY + 2, TZ}: with periodic x (nx a multiple of 16) an x-edge tile loads the column at the
+    // other end of its rows, which holds its wrapped frame cell
+    CUtensorMap xside_type[2], xside_drop;
 };
 
 struct CaKernelArgs {
