@@ -140,6 +140,13 @@ vca_status vca_ca_set_state(vca_ca* ca, const uint8_t* type, const int32_t* flow
                             const vca_vent* vents, int vent_count, int steps_done);
 /* Spill levels in use (nx*ny, x fastest); returns VCA_ERR_STATE when there is no terrain. */
 vca_status vca_ca_get_spill(vca_ca* ca, int32_t* spill);
+/* The per-flow sums of Simulation::flowSums (engine/src/app/Simulation.cpp:408-466) over the current
+ * state, on the device: for flowId f in 1..flows, lava[f] and basalt[f] count the LAVA and BASALT
+ * cells of flow f and reach2[f] is the largest (x - vx)^2 + (y - vy)^2 over them, (vx, vy) the
+ * vent of flow f as given to vca_ca_place_seeds (0 for a flow without cells).  Each array holds
+ * flows + 1 entries; entry 0 is set to 0.  The reference's maxReach is the largest hypot over the
+ * cells rounded to 0.01, which equals sqrt(reach2[f]) rounded to 0.01. */
+vca_status vca_ca_flow_stats(vca_ca* ca, int flows, uint64_t* lava, uint64_t* basalt, uint64_t* reach2);
 /* Device time of the CA steps so far [ms] (CUDA events around the step launches) and the average
  * duration of one launch of the rules kernel [ms] over the last vca_ca_run / vca_ca_step calls. */
 vca_status vca_ca_timing(vca_ca* ca, double* total_ms, double* rules_kernel_ms, uint64_t* rules_launches);

@@ -25,7 +25,7 @@ STOP_NAMES = {0: "running", 1: "no lava", 2: "no air", 3: "no change", 4: "max s
 # Every entry point declared in include/vca.h.
 EXPORTS = [
     "vca_ca_create", "vca_ca_footprint", "vca_ca_reconfigure", "vca_ca_reset", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
-    "vca_ca_get_info", "vca_ca_history", "vca_ca_download", "vca_ca_set_state", "vca_ca_get_spill",
+    "vca_ca_get_info", "vca_ca_history", "vca_ca_download", "vca_ca_set_state", "vca_ca_get_spill", "vca_ca_flow_stats",
     "vca_ca_timing", "vca_ca_kernel_times", "vca_ca_destroy",
     "vca_mc_create", "vca_mc_footprint", "vca_mc_reconfigure", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
@@ -97,7 +97,7 @@ def lib() -> ctypes.CDLL:
         "vca_ca_create": [p, p], "vca_ca_footprint": [p, p], "vca_ca_reconfigure": [p, p], "vca_ca_reset": [p], "vca_ca_apply_terrain": [p, p], "vca_ca_place_seeds": [p, p, i32],
         "vca_ca_step": [p, p], "vca_ca_run": [p], "vca_ca_get_info": [p, p],
         "vca_ca_history": [p, p, p, i32, p], "vca_ca_download": [p, p, p, p, p, p],
-        "vca_ca_set_state": [p, p, p, p, p, p, p, p, i32, i32], "vca_ca_get_spill": [p, p],
+        "vca_ca_set_state": [p, p, p, p, p, p, p, p, i32, i32], "vca_ca_get_spill": [p, p], "vca_ca_flow_stats": [p, i32, p, p, p],
         "vca_ca_timing": [p, p, p, p], "vca_ca_kernel_times": [p, p, p, p, p],
         "vca_mc_create": [p, p], "vca_mc_footprint": [p, p], "vca_mc_reconfigure": [p, p], "vca_mc_set_domain": [p, p], "vca_mc_set_mobility": [p, p],
         "vca_mc_set_domain_from_ca": [p, p], "vca_mc_set_mobility_from_ca": [p, p, f64, i32],
@@ -258,6 +258,13 @@ class LavaCA:
         out = np.empty(self.params.nx * self.params.ny, np.int32)
         _check(lib().vca_ca_get_spill(self.h, _ptr(out)), "vca_ca_get_spill")
         return out
+
+    def flow_stats(self, flows: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Simulation::flowSums on the device: per flowId 0..flows the LAVA cells, the BASALT cells and
+        the largest squared horizontal distance from the flow's vent (entry 0 is 0)."""
+        lava, basalt, reach2 = (np.zeros(flows + 1, np.uint64) for _ in range(3))
+        _check(lib().vca_ca_flow_stats(self.h, flows, _ptr(lava), _ptr(basalt), _ptr(reach2)), "vca_ca_flow_stats")
+        return lava, basalt, reach2
 
     def timing(self) -> tuple[float, float, int]:
         tot, ker, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()

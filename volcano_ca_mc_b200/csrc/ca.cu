@@ -1206,6 +1206,51 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
 }
 
 // ------------------------------------------------------------------------------------------
+// Simulation::flowSums (Simulation.cpp:408-466) over the current state: per flowId f in 1..flows
+// the LAVA and BASALT cells and the largest squared horizontal distance from the vent of f.  With
+// few flows each block sums into shared memory first (one global atomic per flow and block).
+// ------------------------------------------------------------------------------------------
+constexpr int kFlowPrivMax = 1024;  // flows summed in shared memory (3 * 8 B each)
+__global__ void ca_flow_stats_kernel(const uint8_t* T, const int32_t* F, CaGeom g, const int4* vents, int vent_slots,
+                                     int flows, unsigned long long* out) {
+    extern __shared__ unsigned long long s_sum[];  // [3][flows + 1] when flows <= kFlowPrivMax
+    const bool priv = flows <= kFlowPrivMax;
+    const int m = flows + 1;
+    unsigned long long* acc = priv ? s_sum : out;
+    if (priv) {
+        for (int i = threadIdx.x; i < 3 * m; i += blockDim.x) s_sum[i] = 0ull;
+        __syncthreads();
+    }
+    const uint64_t cells = (uint64_t)g.nx * g.ny * g.nz;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cells; i += stride) {
+        const uint64_t r = i / (uint64_t)g.nx;
+        const int x = (int)(i - r * (uint64_t)g.nx);
+        const int64_t p = (int64_t)x + (int64_t)g.P * (int64_t)r;
+        const int t = T[p];
+        if (t != kLava && t != kBasalt) continue;
+        const int32_t f = F[p];
+        if (f <= 0 || f > flows) continue;
+        const int y = (int)(r % (uint64_t)g.ny);
+        atomicAdd(&acc[(t == kLava ? 0 : m) + f], 1ull);
+        if (f < vent_slots) {
+            const int4 v = vents[f];
+            const long long dx = x - v.x, dy = y - v.y;
+            atomicMax(&acc[2 * m + f], (unsigned long long)(dx * dx + dy * dy));
+        }
+    }
+    if (priv) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 3 * m; i += blockDim.x) {
+            const unsigned long long v = s_sum[i];
+            if (v == 0ull) continue;
+            if (i < 2 * m) atomicAdd(&out[i], v);
+            else atomicMax(&out[i], v);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // Set-up kernels.
 // ------------------------------------------------------------------------------------------
 // Per-tile LAVA flag of the current state and the LAVA / AIR totals (countInitialState,
@@ -1589,6 +1634,7 @@ void free_all(vca_ca* h) {
     cudaFree(h->heights_dev);
     cudaFree(h->vents);
     cudaFree(h->seeds_dev);
+    cudaFree(h->flow_sums);
     cudaFree(h->ctrl);
     cudaFree(h->hist_active);
     cudaFree(h->hist_changed);
@@ -2153,6 +2199,45 @@ vca_status vca_ca_get_spill(vca_ca* h, int32_t* spill) {
     }
     VCA_CUDA(cudaSetDevice(h->device));
     VCA_CUDA(cudaMemcpy(spill, h->spill, sizeof(int32_t) * (size_t)h->geom.nx * h->geom.ny, cudaMemcpyDeviceToHost));
+    return VCA_OK;
+}
+
+vca_status vca_ca_flow_stats(vca_ca* h, int flows, uint64_t* lava, uint64_t* basalt, uint64_t* reach2) {
+    if (vca_status s = check(h)) return s;
+    if (flows < 0 || (flows > 0 && (lava == nullptr || basalt == nullptr || reach2 == nullptr))) {
+        set_error("vca_ca_flow_stats: bad flow count or null array");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (vca_status s = sync_ctrl(h)) return s;
+    const size_t m = (size_t)flows + 1;
+    if (3 * m > h->flow_sums_cap) {  // grows only
+        VCA_CUDA(cudaStreamSynchronize(h->stream));
+        cudaFree(h->flow_sums);
+        h->flow_sums = nullptr;
+        h->flow_sums_cap = 0;
+        VCA_CUDA(cudaMalloc(&h->flow_sums, sizeof(unsigned long long) * 3 * m));
+        h->flow_sums_cap = 3 * m;
+    }
+    VCA_CUDA(cudaMemsetAsync(h->flow_sums, 0, sizeof(unsigned long long) * 3 * m, h->stream));
+    const int cur = h->steps & 1;
+    const auto& g = h->geom;
+    const size_t smem = flows <= kFlowPrivMax ? sizeof(unsigned long long) * 3 * m : 0;
+    const uint64_t cells = (uint64_t)g.nx * g.ny * g.nz;
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->sms * 8, (cells + 255) / 256));
+    ca_flow_stats_kernel<<<blocks, 256, smem, h->stream>>>(h->type[cur], h->flow[cur], g, h->vents, h->vent_slots, flows,
+                                                            h->flow_sums);
+    VCA_CUDA(cudaGetLastError());
+    h->launches += 1;
+    std::vector<unsigned long long> host(3 * m);
+    VCA_CUDA(cudaMemcpyAsync(host.data(), h->flow_sums, sizeof(unsigned long long) * 3 * m, cudaMemcpyDeviceToHost,
+                             h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t f = 0; f < m; ++f) {
+        lava[f] = f ? host[f] : 0;
+        basalt[f] = f ? host[m + f] : 0;
+        reach2[f] = f ? host[2 * m + f] : 0;
+    }
     return VCA_OK;
 }
 

@@ -26,36 +26,71 @@ vca_status cuda_fail(cudaError_t e, const char* what) {
 }
 
 // TerrainGenerator::fillDepressions (engine/src/terrain/TerrainGenerator.cpp:86-161): priority
-// flood from the outlets (non-periodic edges; on a fully wrapped map, the lowest columns).  The
-// filled surface is unique, so the visiting order of equal levels does not change the result.
+// flood from the outlets (non-periodic edges; on a fully wrapped map, the lowest columns).  A column
+// is closed by the first open neighbour taken from the queue, at level max(own height, that
+// neighbour's level); levels are taken in nondecreasing order, so the filled surface (the lowest
+// level over all paths to an outlet of the highest column on the path) does not depend on the order
+// inside one level.  Heights are small integers, so the queue is a bucket per level (a stack of
+// columns linked through `next`): linear time.  A height range too wide for buckets uses a heap.
 std::vector<int32_t> fill_depressions(const std::vector<int32_t>& h, int nx, int ny, bool px, bool py) {
     const size_t n = h.size();
     std::vector<int32_t> filled = h;
+    if (n == 0) return filled;
     std::vector<char> closed(n, 0);
+    const auto mm = std::minmax_element(h.begin(), h.end());
+    const int32_t lo = *mm.first;
+    const uint64_t range = (uint64_t)((int64_t)*mm.second - lo) + 1;
+    const bool buckets = range <= (uint64_t)std::max<size_t>(n, 1u << 16);
+    std::vector<int64_t> head(buckets ? range : 0, -1);
+    std::vector<int64_t> next(buckets ? n : 0, -1);
     using Item = std::pair<int32_t, size_t>;
     std::priority_queue<Item, std::vector<Item>, std::greater<Item>> open;
+    auto push = [&](size_t i, int32_t level) {
+        if (buckets) {
+            const size_t b = (size_t)((int64_t)level - lo);
+            next[i] = head[b];
+            head[b] = (int64_t)i;
+        } else {
+            open.push({level, i});
+        }
+    };
     auto seed = [&](size_t i) {
         if (!closed[i]) {
             closed[i] = 1;
-            open.push({h[i], i});
+            push(i, h[i]);
         }
     };
+    bool any = false;
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x) {
             const bool ex = !px && nx > 1 && (x == 0 || x == nx - 1);
             const bool ey = !py && ny > 1 && (y == 0 || y == ny - 1);
-            if (ex || ey) seed((size_t)x + (size_t)nx * y);
+            if (ex || ey) {
+                seed((size_t)x + (size_t)nx * y);
+                any = true;
+            }
         }
-    if (open.empty() && n > 0) {
-        const int32_t lowest = *std::min_element(h.begin(), h.end());
+    if (!any)
         for (size_t i = 0; i < n; ++i)
-            if (h[i] == lowest) seed(i);
-    }
+            if (h[i] == lo) seed(i);
     const int dx[4] = {-1, 1, 0, 0}, dy[4] = {0, 0, -1, 1};
-    while (!open.empty()) {
-        const Item it = open.top();
-        open.pop();
-        const int x = (int)(it.second % (size_t)nx), y = (int)(it.second / (size_t)nx);
+    size_t cur = 0;  // lowest bucket that may hold columns
+    for (;;) {
+        size_t i;
+        int32_t level;
+        if (buckets) {
+            while (cur < range && head[cur] < 0) ++cur;
+            if (cur == range) break;
+            i = (size_t)head[cur];
+            head[cur] = next[i];
+            level = (int32_t)((int64_t)cur + lo);
+        } else {
+            if (open.empty()) break;
+            i = open.top().second;
+            level = open.top().first;
+            open.pop();
+        }
+        const int x = (int)(i % (size_t)nx), y = (int)(i / (size_t)nx);
         for (int d = 0; d < 4; ++d) {
             int sx = x + dx[d], sy = y + dy[d];
             if (sx < 0 || sx >= nx) {
@@ -69,8 +104,8 @@ std::vector<int32_t> fill_depressions(const std::vector<int32_t>& h, int nx, int
             const size_t j = (size_t)sx + (size_t)nx * sy;
             if (closed[j]) continue;
             closed[j] = 1;
-            filled[j] = std::max(h[j], it.first);
-            open.push({filled[j], j});
+            filled[j] = std::max(h[j], level);
+            push(j, filled[j]);
         }
     }
     return filled;

@@ -365,23 +365,17 @@ RunSummary run_ca(const Config& cfg, const std::string& out_dir, Timing& timing,
     return s;
 }
 
-// Simulation::flowSums / statsFromSums (Simulation.cpp:404-524).
-Json ca_stats(const Config& c, const RunSummary& s) {
+// Simulation::flowSums / statsFromSums (Simulation.cpp:404-524).  The sums come from the device
+// (vca_ca_flow_stats).  The reference's reach is the largest hypot(x - vx, y - vy) over a flow's
+// cells and is written rounded to 0.01; the device gives the largest squared distance D, and
+// sqrt(D) rounds to the same 0.01 step: hypot and sqrt(D) differ by at most one ulp, while
+// 100 sqrt(D) of an integer D never lies within 1e-8 of a rounding boundary k + 0.5.
+Json ca_stats(const Config& c, const RunSummary& s, vca_ca* ca) {
     const size_t flows = s.vents.size();
-    std::vector<uint64_t> lava(flows + 1, 0), basalt(flows + 1, 0);
+    std::vector<uint64_t> lava(flows + 1, 0), basalt(flows + 1, 0), reach2(flows + 1, 0);
+    vcheck(vca_ca_flow_stats(ca, (int)flows, lava.data(), basalt.data(), reach2.data()), "vca_ca_flow_stats");
     std::vector<double> reach(flows + 1, 0.0);
-    const Microstructure& m = s.result;
-    size_t i = 0;
-    for (int z = 0; z < m.dims.nz; ++z)
-        for (int y = 0; y < m.dims.ny; ++y)
-            for (int x = 0; x < m.dims.nx; ++x, ++i) {
-                const uint8_t t = m.type[i];
-                const int32_t f = m.flow[i];
-                if ((t != kLava && t != kBasalt) || f <= 0 || (size_t)f > flows) continue;
-                (t == kLava ? lava : basalt)[(size_t)f] += 1;
-                const Vent& v = s.vents[(size_t)f - 1];
-                reach[(size_t)f] = std::max(reach[(size_t)f], std::hypot(double(x - v.x), double(y - v.y)));
-            }
+    for (size_t f = 1; f <= flows; ++f) reach[f] = std::sqrt((double)reach2[f]);
     Json j = Json::object();
     j["mode"] = mode_name(c.ca.mode);
     j["steps"] = s.steps;
@@ -918,7 +912,7 @@ int run_from_cli(const CliOptions& opt, Clock::time_point start) {
         s = run_ca(cfg, out_dir, timing, progress, ca);
         s.ca_ran = true;
         t = Clock::now();
-        stats = ca_stats(cfg, s);
+        stats = ca_stats(cfg, s, ca.h);
         timing.add("caStats", ms_since(t));
     }
     stats["parallel"] = parallel_json(cfg);

@@ -161,6 +161,8 @@ struct vca_ca {
     int32_t* spill = nullptr;
     int4* vents = nullptr;
     int4* seeds_dev = nullptr;  // unique seed cells of place_seeds (grows only)
+    unsigned long long* flow_sums = nullptr;  // 3 * (flows + 1) sums of vca_ca_flow_stats (grows only)
+    size_t flow_sums_cap = 0;
     int vent_slots = 0;
     vca::CaCtrl* ctrl = nullptr;
     vca::CaCtrl* ctrl_host = nullptr;   // pinned mirror

@@ -177,6 +177,7 @@ class Slot:
         t.append(time.perf_counter())
         self.ca.run()
         info = self.ca.info()
+        lava, basalt, reach2 = self.ca.flow_stats(len(vents))
         t.append(time.perf_counter())
         n = job.cells
         planes = self.ca.download(None if bufs is None else tuple(a[:n] for a in bufs[:5]))
@@ -192,6 +193,7 @@ class Slot:
         energy = self.mc.energy()
         t.append(time.perf_counter())
         rec = {"job": job.job_id, "steps": info.steps, "stop": info.stop_reason, "energy": energy, "grains": g.grains,
+               "lava_volume": int(lava.sum() + basalt.sum()), "max_reach": round(float(np.sqrt(reach2.max())), 2),
                "attempts": mi.attempts, "cell_updates": job.cells * info.steps, "done": t[-1],
                "phases_ms": {k: round((t[i + 1] - t[i]) * 1e3, 3)
                              for i, k in enumerate(("setup", "ca", "download", "mc"))}}
