@@ -191,11 +191,12 @@ struct SmallVote {
 };
 
 __device__ __forceinline__ void tile_origin(const CaGeom& g, uint32_t tile, int& x0, int& y0, int& z0) {
-    const int tx = (int)(tile % (uint32_t)g.tiles_x);
-    const uint32_t r = tile / (uint32_t)g.tiles_x;
-    x0 = tx * kTileX;
-    y0 = (int)(r % (uint32_t)g.tiles_y) * g.TY;
-    z0 = (int)(r / (uint32_t)g.tiles_y) * g.TZ;
+    uint32_t tx, ty;
+    const uint32_t r = fast_divmod(tile, g.div_tx, tx);
+    const uint32_t tz = fast_divmod(r, g.div_ty, ty);
+    x0 = (int)tx * kTileX;
+    y0 = (int)ty * g.TY;
+    z0 = (int)tz * g.TZ;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -478,10 +479,10 @@ __device__ __forceinline__ void schedule_around(const CaKernelArgs& k, uint32_t 
     uint32_t target = 0;
     if (want && lane < 27) {
         const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
-        int tx = (int)(tile % (uint32_t)g.tiles_x) + dx;
-        const uint32_t r = tile / (uint32_t)g.tiles_x;
-        int ty = (int)(r % (uint32_t)g.tiles_y) + dy;
-        int tz = (int)(r / (uint32_t)g.tiles_y) + dz;
+        uint32_t ux, uy;
+        const uint32_t r = fast_divmod(tile, g.div_tx, ux);
+        const uint32_t uz = fast_divmod(r, g.div_ty, uy);
+        int tx = (int)ux + dx, ty = (int)uy + dy, tz = (int)uz + dz;
         if (wrap_axis(tx, g.tiles_x, g.per[0]) && wrap_axis(ty, g.tiles_y, g.per[1]) && wrap_axis(tz, g.tiles_z, g.per[2])) {
             target = (uint32_t)tx + (uint32_t)g.tiles_x * ((uint32_t)ty + (uint32_t)g.tiles_y * tz);
             const uint32_t m = 2u * (t + 2u);
@@ -1826,6 +1827,8 @@ CaGeom geometry_of(const vca_ca_desc* d) {
     g.tiles_x = g.P / kTileX;
     g.tiles_y = (d->ny + g.TY - 1) / g.TY;
     g.tiles_z = (d->nz + g.TZ - 1) / g.TZ;
+    g.div_tx = make_fastdiv32((uint32_t)g.tiles_x);
+    g.div_ty = make_fastdiv32((uint32_t)g.tiles_y);
     return g;
 }
 

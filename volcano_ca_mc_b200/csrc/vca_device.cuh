@@ -48,6 +48,24 @@ __device__ __forceinline__ uint64_t fast_mod(uint64_t x, FastMod f) {
     return r;
 }
 
+// n / d and n % d for 32-bit n and a divisor d >= 1 fixed at set-up: q = umulhi(n, m) with
+// m = floor((2^32 - 1) / d) is floor(n / d) or one less, one correction step finishes it.
+struct FastDiv32 {
+    uint32_t d;
+    uint32_t m;
+};
+inline FastDiv32 make_fastdiv32(uint32_t d) { return FastDiv32{d, d ? 0xFFFFFFFFu / d : 0u}; }
+__device__ __forceinline__ uint32_t fast_divmod(uint32_t n, FastDiv32 f, uint32_t& rem) {
+    uint32_t q = __umulhi(n, f.m);
+    uint32_t r = n - q * f.d;
+    if (r >= f.d) {
+        ++q;
+        r -= f.d;
+    }
+    rem = r;
+    return q;
+}
+
 // Offsets of the neighbourhood variants (engine/src/core/Neighborhood.cpp:55-119).
 struct NbTable {
     int variants;

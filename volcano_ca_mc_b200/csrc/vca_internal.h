@@ -55,6 +55,7 @@ struct CaGeom {
     int per[3];               // periodic axes (Boundary, engine/src/core/Boundary.cpp:5-11)
     int TY, TZ;               // tile rows: TY * TZ = 16, tile = 64 x TY x TZ cells
     int tiles_x, tiles_y, tiles_z;
+    FastDiv32 div_tx, div_ty;  // / tiles_x and / tiles_y (tile id -> tile coordinates)
 };
 
 struct CaTables {
