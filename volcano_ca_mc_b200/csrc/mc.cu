@@ -85,6 +85,61 @@ __device__ __forceinline__ int32_t spin_at(const McArgs& a, int x, int y, int z)
     return a.spin[(uint64_t)x + (uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z)];
 }
 
+// mc_wrap for a neighbour one cell away, as selects (no branch), so that the loads of all
+// neighbours of a cell can be issued together.  v is only meaningful when the result is true.
+__device__ __forceinline__ bool mc_wrap1_sel(int& v, int n, int periodic) {
+    const bool in = (unsigned)v < (unsigned)n;
+    const int w = v < 0 ? v + n : v - n;
+    v = in ? v : w;
+    return in | ((periodic != 0) & (n > 1));
+}
+
+// unlikeBeforeAfter's neighbour counts (PottsMC.cpp:394-430, PottsMC.hpp:191-204) for the cell
+// (x, y, z) = globalIndex g and variant var: neighbours in the domain (spin != 0) and those equal to
+// cur / prop.  The offsets come from the block's copy of the table and the loads go out together;
+// a neighbour outside the frame reads the cell itself and counts as spin 0.
+__device__ __forceinline__ void nb_counts(const McArgs& a, const NbTable& nb, int var, int x, int y, int z, uint32_t g,
+                                          int32_t cur, int32_t prop, int& in_dom, int& same_a, int& same_b) {
+    const int cnt = nb.count[var];
+    int32_t sv[26];
+#pragma unroll
+    for (int k = 0; k < 26; ++k) {
+        int sx = x + nb.off[var][k][0], sy = y + nb.off[var][k][1], sz = z + nb.off[var][k][2];
+        const bool ok = (k < cnt) & mc_wrap1_sel(sx, a.nx, a.per[0]) & mc_wrap1_sel(sy, a.ny, a.per[1]) &
+                        mc_wrap1_sel(sz, a.nz, a.per[2]);
+        // globalIndex fits 32 bits (at most 2e9 cells)
+        const uint32_t idx = ok ? (uint32_t)sx + (uint32_t)a.nx * ((uint32_t)sy + (uint32_t)a.ny * (uint32_t)sz) : g;
+        const int32_t v = a.spin[idx];
+        sv[k] = ok ? v : 0;
+    }
+    in_dom = same_a = same_b = 0;
+#pragma unroll
+    for (int k = 0; k < 26; ++k) {
+        in_dom += sv[k] != 0;
+        same_a += sv[k] == cur;
+        same_b += sv[k] == prop;
+    }
+}
+// The same counts one neighbour after another: fewer registers, for grids where each thread has
+// several cells and the SM hides the latency with more resident warps.
+__device__ __forceinline__ void nb_counts_loop(const McArgs& a, const NbTable& nb, int var, int x, int y, int z,
+                                               int32_t cur, int32_t prop, int& in_dom, int& same_a, int& same_b) {
+    in_dom = same_a = same_b = 0;
+    const int cnt = nb.count[var];
+    for (int k = 0; k < cnt; ++k) {
+        const int32_t sj = spin_at(a, x + nb.off[var][k][0], y + nb.off[var][k][1], z + nb.off[var][k][2]);
+        in_dom += sj != 0;
+        same_a += sj == cur;
+        same_b += sj == prop;
+    }
+}
+__device__ __forceinline__ void stage_nb(const McArgs& a, NbTable& s_nb) {
+    const int* src = reinterpret_cast<const int*>(a.nb);
+    int* dst = reinterpret_cast<int*>(&s_nb);
+    for (int i = threadIdx.x; i < (int)(sizeof(NbTable) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+}
+static_assert(sizeof(NbTable) % sizeof(int) == 0, "NbTable is copied as ints");
+
 // PottsMC::axisClass / colorOf (PottsMC.cpp:145-158), colour numbering of buildColors (173-193).
 __host__ __device__ inline int axis_class(int c, int n, int periodic) {
     if (periodic && (n % 2) == 1 && c == n - 1) return 2;
@@ -153,12 +208,14 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
     __shared__ unsigned long long s_table[kTableSide * kTableSide];
     __shared__ unsigned long long s_red[3][kMcThreads / 32];
     __shared__ bool s_last;
+    __shared__ NbTable s_nb;
     for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
+    stage_nb(a, s_nb);
     __syncthreads();
     McCtrl* ctrl = a.ctrl;
     const uint32_t t = ctrl->sweeps;
     const uint64_t prefix = hash_prefix(a.seed, t);
-    const NbTable& nb = *a.nb;
+    const NbTable& nb = s_nb;
     unsigned my_att = 0, my_acc = 0, my_up = 0;
     for (uint64_t j = blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < count; j += (uint64_t)gridDim.x * kMcThreads) {
         const uint32_t g = list[j];
@@ -175,14 +232,8 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
         const int32_t cur = a.spin[g];
         int32_t prop = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
         if (prop >= cur) ++prop;
-        int in_dom = 0, same_a = 0, same_b = 0;
-        const int cnt = nb.count[var];
-        for (int k = 0; k < cnt; ++k) {
-            const int32_t sj = spin_at(a, x + nb.off[var][k][0], y + nb.off[var][k][1], z + nb.off[var][k][2]);
-            in_dom += sj != 0;
-            same_a += sj == cur;
-            same_b += sj == prop;
-        }
+        int in_dom, same_a, same_b;
+        nb_counts_loop(a, nb, var, x, y, z, cur, prop, in_dom, same_a, same_b);
         const int before = in_dom - same_a, after = in_dom - same_b;
         const unsigned long long e = s_table[before * kTableSide + after];
         bool accept;
@@ -279,15 +330,17 @@ __device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks) {
 // (sweepColors, PottsMC.cpp:495-514), a grid barrier after each, the same trial as mc_color_kernel
 // (colorTrials, PottsMC.cpp:394-493).  Replaces `sweeps` x `colors` launches; for domains of a few
 // hundred thousand cells the launches, not the trials, were the cost.
-template <bool kMobility, bool kRandomNb>
-__global__ __launch_bounds__(kMcThreads) void mc_sweeps_kernel(McArgs a, McColors col, int sweeps) {
+template <bool kMobility, bool kRandomNb, bool kBatched>
+__global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel(McArgs a, McColors col, int sweeps) {
     __shared__ unsigned long long s_table[kTableSide * kTableSide];
     __shared__ unsigned long long s_red[3][kMcThreads / 32];
+    __shared__ NbTable s_nb;
     for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
+    stage_nb(a, s_nb);
     __syncthreads();
     McCtrl* ctrl = a.ctrl;
     const uint32_t t0 = ctrl->sweeps;
-    const NbTable& nb = *a.nb;
+    const NbTable& nb = s_nb;
     unsigned long long my_att = 0, my_acc = 0, my_up = 0;
     bool ok = true;
     for (int s = 0; s < sweeps && ok; ++s) {
@@ -309,14 +362,11 @@ __global__ __launch_bounds__(kMcThreads) void mc_sweeps_kernel(McArgs a, McColor
                 const int32_t cur = a.spin[g];
                 int32_t prop = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
                 if (prop >= cur) ++prop;
-                int in_dom = 0, same_a = 0, same_b = 0;
-                const int cnt = nb.count[var];
-                for (int k = 0; k < cnt; ++k) {
-                    const int32_t sj = spin_at(a, x + nb.off[var][k][0], y + nb.off[var][k][1], z + nb.off[var][k][2]);
-                    in_dom += sj != 0;
-                    same_a += sj == cur;
-                    same_b += sj == prop;
-                }
+                int in_dom, same_a, same_b;
+                if (kBatched)
+                    nb_counts(a, nb, var, x, y, z, g, cur, prop, in_dom, same_a, same_b);
+                else
+                    nb_counts_loop(a, nb, var, x, y, z, cur, prop, in_dom, same_a, same_b);
                 const unsigned long long th = s_table[(in_dom - same_a) * kTableSide + (in_dom - same_b)];
                 bool accept;
                 if (th >> 63) {
@@ -720,19 +770,30 @@ void mc_free(vca_mc* h) {
 
 using SweepsKernel = void (*)(McArgs, McColors, int);
 
-SweepsKernel sweeps_kernel_for(const vca_mc* h) {
+template <bool kBatched>
+SweepsKernel sweeps_kernel_of(const vca_mc* h) {
     const bool random_nb = h->nb_host.variants > 1;
-    if (h->mobility_on) return random_nb ? mc_sweeps_kernel<true, true> : mc_sweeps_kernel<true, false>;
-    return random_nb ? mc_sweeps_kernel<false, true> : mc_sweeps_kernel<false, false>;
+    if (h->mobility_on) return random_nb ? mc_sweeps_kernel<true, true, kBatched> : mc_sweeps_kernel<true, false, kBatched>;
+    return random_nb ? mc_sweeps_kernel<false, true, kBatched> : mc_sweeps_kernel<false, false, kBatched>;
 }
 
-// Blocks of the cooperative sweep launch: all resident at once, no more than the largest colour needs.
-vca_status sweeps_grid(vca_mc* h, int* grid) {
-    int per_sm = 0;
-    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweeps_kernel_for(h), kMcThreads, 0));
+// The sweep kernel and its cooperative grid (all blocks resident at once, no more than the largest
+// colour needs).  When every cell of the largest colour gets a thread of its own in the batched
+// form, a colour pass is one trial's latency: batched neighbour loads.  Otherwise each thread has
+// several cells and the loop form, with more resident warps per SM, hides the latency better.
+vca_status sweeps_launch_shape(vca_mc* h, SweepsKernel* kernel, int* grid) {
     uint64_t widest = 0;
     for (int c = 0; c < h->colors; ++c) widest = std::max<uint64_t>(widest, h->color_off[c + 1] - h->color_off[c]);
-    const uint64_t need = (widest + kMcThreads - 1) / kMcThreads;
+    const uint64_t need = std::max<uint64_t>(1, (widest + kMcThreads - 1) / kMcThreads);
+    int per_sm = 0;
+    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweeps_kernel_of<true>(h), kMcThreads, 0));
+    if (need <= (uint64_t)h->sms * std::max(1, per_sm)) {
+        *kernel = sweeps_kernel_of<true>(h);
+        *grid = (int)need;
+        return VCA_OK;
+    }
+    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweeps_kernel_of<false>(h), kMcThreads, 0));
+    *kernel = sweeps_kernel_of<false>(h);
     *grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * std::max(1, per_sm)));
     return VCA_OK;
 }
@@ -1068,12 +1129,13 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
         col.colors = h->colors;
         for (int c = 0; c <= h->colors; ++c) col.off[c] = h->color_off[c];
         int grid = 1;
-        if (vca_status s = sweeps_grid(h, &grid)) return s;
+        SweepsKernel kernel = nullptr;
+        if (vca_status s = sweeps_launch_shape(h, &kernel, &grid)) return s;
         VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
         if (count > 0 && h->color_off.back() > 0) {
             int n = count;
             void* args[] = {&a, &col, &n};
-            VCA_CUDA(cudaLaunchCooperativeKernel((const void*)sweeps_kernel_for(h), grid, kMcThreads, args, 0, h->stream));
+            VCA_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, grid, kMcThreads, args, 0, h->stream));
             h->launches += 1;
         } else if (count > 0) {
             // empty domain: the sweeps still count (sweepsDone)
