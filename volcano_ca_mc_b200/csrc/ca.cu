@@ -574,6 +574,20 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int 
                  "r"(y), "r"(z), "r"(smem_u32(src))
                  : "memory");
 }
+// 4D boxes {x, y, z, plane}: two planes of one allocation (flowId + temperature, solidStep +
+// arrivalStep) move in one copy
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];\n" ::"l"(map),
+                 "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_u32(src))
+                 : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
 // the shared-memory sources of all committed bulk stores have been read
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
@@ -620,6 +634,9 @@ struct __align__(128) RulesSlot {
     __align__(128) uint8_t xside[2][kXSideBytes];
     __align__(128) int8_t xside_drop[2][kXSideDropBytes];
 };
+static_assert(offsetof(RulesSlot, temp) == offsetof(RulesSlot, flow) + 4 * kTileCells &&
+                  offsetof(RulesSlot, arrival) == offsetof(RulesSlot, solid) + 2 * kTileCells,
+              "the planes of a pair follow each other in a slot, as a 4D box lands them");
 static_assert(offsetof(RulesSlot, type) % 128 == 0 && offsetof(RulesSlot, drop) % 128 == 0 &&
                   offsetof(RulesSlot, own_type) % 128 == 0 && offsetof(RulesSlot, solid) % 128 == 0 &&
                   offsetof(RulesSlot, xside) % 128 == 0 && offsetof(RulesSlot, xside_drop) % 128 == 0 &&
@@ -721,10 +738,8 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             // periodic x: an x-edge tile also loads the column that holds its wrapped frame cells
             const bool wl = rules && xwrap && x0 == 0, wr = rules && xwrap && x0 + kTileX >= g.nx;
             mbar_arrive_expect_tx(&s_bar[s], (rules ? tx_rules : tx_copy) + (wl ? tx_xside : 0u) + (wr ? tx_xside : 0u));
-            tma_load_3d(sl.flow, &k.tm.flow[cur], x0, y0, z0, &s_bar[s]);
-            tma_load_3d(sl.temp, &k.tm.temp[cur], x0, y0, z0, &s_bar[s]);
-            tma_load_3d(sl.solid, &k.tm.solid[cur], x0, y0, z0, &s_bar[s]);
-            tma_load_3d(sl.arrival, &k.tm.arrival[cur], x0, y0, z0, &s_bar[s]);
+            tma_load_4d(sl.flow, &k.tm.ft[cur], x0, y0, z0, &s_bar[s]);   // flowId and temperature
+            tma_load_4d(sl.solid, &k.tm.sa[cur], x0, y0, z0, &s_bar[s]);  // solidStep and arrivalStep
             if (rules) {
                 tma_load_3d(sl.type, &k.tm.halo_type[cur], x0 - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
                 if (lava_mode) tma_load_3d(sl.drop, &k.tm.drop, x0 - 16, y0 - hy_on, z0, &s_bar[s]);
@@ -751,10 +766,8 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
     auto store_tile = [&](int s, int x0, int y0, int z0) {  // thread 0
         RulesSlot& sl = slots[s];
         tma_store_3d(&k.tm.own_type[nxt], x0, y0, z0, sl.own_type);
-        tma_store_3d(&k.tm.flow[nxt], x0, y0, z0, sl.flow);
-        tma_store_3d(&k.tm.temp[nxt], x0, y0, z0, sl.temp);
-        tma_store_3d(&k.tm.solid[nxt], x0, y0, z0, sl.solid);
-        tma_store_3d(&k.tm.arrival[nxt], x0, y0, z0, sl.arrival);
+        tma_store_4d(&k.tm.ft[nxt], x0, y0, z0, sl.flow);
+        tma_store_4d(&k.tm.sa[nxt], x0, y0, z0, sl.solid);
         bulk_commit();
     };
 
@@ -1617,10 +1630,8 @@ void free_all(vca_ca* h) {
     if (h->device >= 0) cudaSetDevice(h->device);
     for (int b = 0; b < 2; ++b) {
         cudaFree(h->type[b]);
-        cudaFree(h->flow[b]);
-        cudaFree(h->temp[b]);
-        cudaFree(h->solid[b]);
-        cudaFree(h->arrival[b]);
+        cudaFree(h->flow[b]);   // temp[b] lies in the same allocation
+        cudaFree(h->solid[b]);  // and arrival[b]
         cudaFree(h->tile_list[b]);
     }
     cudaFree(h->tile_flags);
@@ -1710,6 +1721,27 @@ vca_status encode_plane(CUtensorMap* m, CUtensorMapDataType type, size_t elem, v
     return VCA_OK;
 }
 
+// Two planes of one allocation as a 4D tensor (P, ny, nz, 2), the plane stride given in elements.
+vca_status encode_pair(CUtensorMap* m, CUtensorMapDataType type, size_t elem, void* base, const CaGeom& g, size_t plane_stride,
+                       uint32_t bx, uint32_t by, uint32_t bz, const char* what) {
+    const EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("vca_ca_create: cuTensorMapEncodeTiled is not available from the driver");
+        return VCA_ERR_CUDA;
+    }
+    const cuuint64_t dims[4] = {(cuuint64_t)g.P, (cuuint64_t)g.ny, (cuuint64_t)g.nz, 2};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.P * elem, (cuuint64_t)g.P * g.ny * elem, (cuuint64_t)plane_stride * elem};
+    const cuuint32_t box[4] = {bx, by, bz, 2};
+    const cuuint32_t step[4] = {1, 1, 1, 1};
+    const CUresult r = fn(m, type, 4, base, dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error(std::string("vca_ca_create: cuTensorMapEncodeTiled failed for ") + what + " (CUresult " + std::to_string((int)r) + ")");
+        return VCA_ERR_CUDA;
+    }
+    return VCA_OK;
+}
+
 // Tensor maps of the rules pass (boxes of one 64 x TY x TZ tile, halo rows 96 bytes from x0 - 16).
 vca_status encode_maps(vca_ca* h) {
     const CaGeom& g = h->geom;
@@ -1720,11 +1752,12 @@ vca_status encode_maps(vca_ca* h) {
         if (vca_status s = encode_plane(&m.own_type[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->type[b], g, kTileX, TY, TZ, "type")) return s;
         if (vca_status s = encode_plane(&m.halo_type[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, h->type[b], g, kTileX + 32, HY, HZ, "type halo"))
             return s;
-        if (vca_status s = encode_plane(&m.flow[b], CU_TENSOR_MAP_DATA_TYPE_INT32, 4, h->flow[b], g, kTileX, TY, TZ, "flowId")) return s;
-        if (vca_status s = encode_plane(&m.temp[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->temp[b], g, kTileX, TY, TZ, "temp")) return s;
-        if (vca_status s = encode_plane(&m.solid[b], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->solid[b], g, kTileX, TY, TZ, "solidStep"))
+        const size_t stride = h->cap.plane_cells;  // temp[b] - flow[b], arrival[b] - solid[b]
+        if (vca_status s = encode_pair(&m.ft[b], CU_TENSOR_MAP_DATA_TYPE_INT32, 4, h->flow[b], g, stride, kTileX, TY, TZ,
+                                       "flowId + temp"))
             return s;
-        if (vca_status s = encode_plane(&m.arrival[b], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->arrival[b], g, kTileX, TY, TZ, "arrivalStep"))
+        if (vca_status s = encode_pair(&m.sa[b], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->solid[b], g, stride, kTileX, TY, TZ,
+                                       "solidStep + arrivalStep"))
             return s;
     }
     for (int b = 0; b < 2; ++b)
@@ -1924,10 +1957,12 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     const size_t n = need.plane_cells;
     for (int b = 0; b < 2; ++b) {
         ALLOC(h->type[b], n);
-        ALLOC(h->flow[b], n * 4);
-        ALLOC(h->temp[b], n * 4);
-        ALLOC(h->solid[b], n * 2);
-        ALLOC(h->arrival[b], n * 2);
+        // flowId then temperature, solidStep then arrivalStep: one allocation each, so that one 4D
+        // TMA box moves both planes of a pair (the plane stride is the capacity's plane size)
+        ALLOC(h->flow[b], n * 8);
+        h->temp[b] = reinterpret_cast<float*>(h->flow[b] + n);
+        ALLOC(h->solid[b], n * 4);
+        h->arrival[b] = h->solid[b] + n;
         ALLOC(h->tile_list[b], need.ntiles * 4);
     }
     ALLOC(h->tile_flags, need.ntiles * 4);

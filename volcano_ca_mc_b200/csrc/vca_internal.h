@@ -68,7 +68,9 @@ struct CaTables {
 // box {64, TY, TZ} of each plane, the type halo box {96, TY + 2, TZ + 2} from (x0 - 16, y0 - 1,
 // z0 - 1), and the drop-depth rows {96, TY + 2, TZ} from (x0 - 16, y0 - 1, z0).
 struct CaTensorMaps {
-    CUtensorMap own_type[2], halo_type[2], flow[2], temp[2], solid[2], arrival[2], drop;
+    CUtensorMap own_type[2], halo_type[2], drop;
+    // 4D (x, y, z, plane): flowId + temperature, solidStep + arrivalStep (pairs allocated together)
+    CUtensorMap ft[2], sa[2];
     // 16-cell-wide columns of the type halo rows {16, TY + 2, TZ + 2} and of the drop rows
     // {16, TY + 2, TZ}: with periodic x (nx a multiple of 16) an x-edge tile loads the column at the
     // other end of its rows, which holds its wrapped frame cell
