@@ -59,9 +59,9 @@ def parse():
     ap.add_argument("--no-served", action="store_true", help="skip the served (Poisson arrivals) sub-benchmark")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served arrival trace")
     ap.add_argument("--slots", type=int, default=16, help="worker slots of the batched and served runs")
-    ap.add_argument("--profile-job", choices=["active", "dense"], default=None,
-                    help="run exactly one CA job with this schedule (no warm-up, no MC) and exit: the case "
-                         "ncu captures")
+    ap.add_argument("--profile-job", choices=["active", "dense", "mc"], default=None,
+                    help="run exactly one CA job with this schedule (no warm-up, no MC), or with mc one ACTIVE "
+                         "CA job and its MC stage, and exit: the case ncu captures")
     return ap.parse_args()
 
 
@@ -532,8 +532,18 @@ def profile_job(args):
     ca.run()
     info = ca.info()
     ms, _, _ = ca.timing()
-    print(json.dumps({"profile_job": args.profile_job, "workload": w.name, "steps": info.steps,
-                      "tiles_processed": info.tiles_processed, "ms": ms}))
+    out = {"profile_job": args.profile_job, "workload": w.name, "steps": info.steps,
+           "tiles_processed": info.tiles_processed, "ms": ms}
+    if args.profile_job == "mc":
+        mc = capi.PottsMC(mc_params(w, 0))
+        mc.set_domain_from_ca(ca)
+        mc.set_mobility_from_ca(ca, 0.05, True)
+        mc.initialize()
+        mc.sweep(w.mcs)
+        mi = mc.info()
+        out["mc"] = {"sweeps": mi.sweeps, "domain_cells": mi.domain_cells, "ms": mc.timing()[0]}
+        mc.close()
+    print(json.dumps(out))
     ca.close()
 
 
