@@ -323,10 +323,6 @@ __global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force
 // ------------------------------------------------------------------------------------------
 // Rules, candidate pass: an AIR cell with LAVA within one cell (listed by the streaming pass).
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ int type_at(const CaGeom& g, const uint8_t* T, int x, int y, int z) {
-    if (!resolve(g, x, y, z)) return kVoid;
-    return __ldg(T + pidx(g, x, y, z));
-}
 
 // gatherLavaCandidates + tryPonding (LavaCA.hpp:443-519) or updateClassic's vote (1176-1182), the
 // winner (CaRules.hpp:152-173) and the solidus test.  Returns true when the cell becomes LAVA.
@@ -352,6 +348,32 @@ __device__ __forceinline__ bool gather_vote(const CaKernelArgs& k, const uint8_t
         const bool ok = (i < cnt) & resolve1_sel(g, sx, sy, sz);
         const int tv = __ldg(T + (ok ? pidx(g, sx, sy, sz) : self));
         lava_mask |= (uint32_t)(tv == kLava) << i;
+    }
+    // tryPonding's cells (LavaCA.hpp:443-461), fetched in the same round: the spill level, the cell
+    // under the one below (its support), the cells beside the one below (4 in 3D, 2 in 2D; outside
+    // the grid they are VOID, i.e. open) and the flowId and temperature of the one below
+    const bool pond = !k.classic && k.ponding && k.spill != nullptr && z >= 1;
+    int p_spill = 0, p_under = kRock;
+    bool p_closed = true;
+    int32_t p_flow = 0;
+    float p_temp = 0.0f;
+    if (pond) {
+        const int bz = z - 1;
+        p_spill = __ldg(k.spill + x + (int64_t)g.nx * y);
+        if (bz > 0) p_under = __ldg(T + pidx(g, x, y, bz - 1));  // bz == 0 stands on the grid floor
+        const int nh = g.ny > 1 ? 4 : 2;
+        const int hx[4] = {-1, 1, 0, 0}, hy[4] = {0, 0, -1, 1};
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            int sx = x + hx[h], sy = y + hy[h], sz = bz;
+            const bool ok = (h < nh) & resolve1_sel(g, sx, sy, sz);
+            const int n = __ldg(T + (ok ? pidx(g, sx, sy, sz) : self));
+            const bool open = h < nh && (!ok || n == kAir || n == kVoid);
+            p_closed = p_closed && !open;
+        }
+        const int64_t b = pidx(g, x, y, bz);
+        p_flow = __ldg(F + b);
+        p_temp = __ldg(Te + b);
     }
     if (!lava_mask) return false;
     v.n = 0;
@@ -395,24 +417,13 @@ __device__ __forceinline__ bool gather_vote(const CaKernelArgs& k, const uint8_t
                 continue;
             }
             if (src[q] == 26) {
-                // tryPonding (LavaCA.hpp:443-461)
-                if (k.spill == nullptr || z > __ldg(k.spill + x + (int64_t)g.nx * y)) continue;
-                const int bz = z - 1;
-                if (bz > 0) {  // hasSupport(x, y, bz)
-                    const int below = __ldg(T + pidx(g, x, y, bz - 1));
-                    const bool sup = solid_ground(below) || (below == kLava && bz - 1 < __ldg(k.spill + x + (int64_t)g.nx * y));
-                    if (!sup) continue;
-                }
-                const int nh = g.ny > 1 ? 4 : 2;
-                const int hx[4] = {-1, 1, 0, 0}, hy[4] = {0, 0, -1, 1};
-                bool open_side = false;
-                for (int h = 0; h < nh; ++h) {
-                    const int n = type_at(g, T, x + hx[h], y + hy[h], bz);
-                    open_side = open_side || n == kAir || n == kVoid;
-                }
-                if (open_side) continue;
-                const int64_t b = pidx(g, x, y, bz);
-                v.add(__ldg(F + b), __fsub_rn(__ldg(Te + b), k.cool_lateral));
+                // tryPonding (LavaCA.hpp:443-461): at or below the spill level, the cell below
+                // supported (hasSupport of z - 1: the grid floor, solid ground, or LAVA below the
+                // spill level) and closed on every side
+                if (!pond || z > p_spill) continue;
+                const bool sup = solid_ground(p_under) || (p_under == kLava && z - 2 < p_spill);
+                if (!sup || !p_closed) continue;
+                v.add(p_flow, __fsub_rn(p_temp, k.cool_lateral));
                 continue;
             }
             const int i = src[q];
