@@ -48,8 +48,8 @@ struct McCtrl {
     unsigned long long uphill;
     unsigned long long energy_acc;
     unsigned long long sweep_accepted;  // accepted in the running sweep
-    unsigned int bar_count;             // grid barrier of the fused sweep kernel: arrivals
-    unsigned int bar_gen;               // and generation
+    unsigned long long bar_arrived;     // grid barrier of the fused sweep kernel: arrivals so far
+                                        // (zeroed before each launch)
     int error;                          // bit 0: a bounded barrier wait ran out
     int pad;
 };
@@ -292,34 +292,32 @@ struct McColors {
     uint64_t off[28];
 };
 
-// Grid-wide barrier of a cooperative launch (all blocks resident): arrivals counted in ctrl, the
-// last arrival opens the next generation.  The wait is bounded; a block that gives up, or sees that
-// another gave up, returns false (ctrl->error is then set).
-__device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks) {
+// Grid barrier of the cooperative sweep launch.  Thread 0 of each block adds one arrival with
+// release semantics (the block's writes, ordered before it by __syncthreads, become visible with
+// it) and polls the count with acquire loads until every block has arrived `epoch` times; the count
+// only grows during a launch and is zeroed before it.  The wait is bounded; a block that gives up,
+// or sees that another gave up, returns false (ctrl->error is then set).
+__device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks, unsigned long long epoch) {
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
-        volatile unsigned* gen = &ctrl->bar_gen;
+        unsigned long long* cnt = &ctrl->bar_arrived;
         volatile int* err = &ctrl->error;
-        const unsigned g = *gen;
-        __threadfence();
+        asm volatile("red.release.gpu.global.add.u64 [%0], 1;\n" ::"l"(cnt) : "memory");
+        const unsigned long long target = epoch * nblocks;
         int ok = 1;
-        if (atomicAdd(&ctrl->bar_count, 1u) == nblocks - 1) {
-            atomicExch(&ctrl->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&ctrl->bar_gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*gen == g) {
-                if (*err || ++spins > (1ll << 26)) {
-                    ok = 0;
-                    atomicOr(&ctrl->error, 1);
-                    break;
-                }
-                __nanosleep(32);
+        long long spins = 0;
+        for (;;) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(cnt) : "memory");
+            if (v >= target) break;
+            if (*err || ++spins > (1ll << 26)) {
+                ok = 0;
+                atomicOr(&ctrl->error, 1);
+                break;
             }
+            __nanosleep(32);
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -343,6 +341,7 @@ __global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel
     const NbTable& nb = s_nb;
     unsigned long long my_att = 0, my_acc = 0, my_up = 0;
     bool ok = true;
+    unsigned long long epoch = 0;  // grid barriers passed in this launch
     for (int s = 0; s < sweeps && ok; ++s) {
         const uint64_t prefix = hash_prefix(a.seed, t0 + (uint32_t)s);
         for (int c = 0; c < col.colors && ok; ++c) {
@@ -380,7 +379,7 @@ __global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel
                     ++my_acc;
                 }
             }
-            ok = mc_grid_barrier(ctrl, gridDim.x);
+            ok = mc_grid_barrier(ctrl, gridDim.x, ++epoch);
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1135,6 +1134,7 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
         if (count > 0 && h->color_off.back() > 0) {
             int n = count;
             void* args[] = {&a, &col, &n};
+            VCA_CUDA(cudaMemsetAsync(&h->ctrl->bar_arrived, 0, sizeof(unsigned long long), h->stream));
             VCA_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, grid, kMcThreads, args, 0, h->stream));
             h->launches += 1;
         } else if (count > 0) {
