@@ -1200,12 +1200,14 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
             atomicAdd(&ctrl->acc_changed, sb);
             atomicAdd(&ctrl->acc_born, sb);
         }
-        __threadfence();
-        s_last = atomicAdd(&ctrl->ticket, 1u) == parts - 1;
+        // the ticket with acquire-release semantics: this block's sums are visible before its ticket,
+        // and the last block sees every other block's sums after its own
+        unsigned old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;\n" : "=r"(old) : "l"(&ctrl->ticket) : "memory");
+        s_last = old == parts - 1;
     }
     __syncthreads();
     if (s_last && threadIdx.x == 0) {
-        __threadfence();
         const unsigned long long active = atomicExch(&ctrl->acc_active, 0ull);
         const unsigned long long changed = atomicExch(&ctrl->acc_changed, 0ull);
         const unsigned long long nborn = atomicExch(&ctrl->acc_born, 0ull);
@@ -1225,8 +1227,7 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
         else if (changed == 0 && !ctrl->random_nb) stop = VCA_STOP_NO_CHANGE;
         else if ((int)steps >= ctrl->max_steps) stop = VCA_STOP_MAX_STEPS;
         ctrl->stop = stop;
-        ctrl->steps = steps;
-        __threadfence();
+        ctrl->steps = steps;  // read by the next kernels, after this launch has completed
     }
 }
 
