@@ -1476,7 +1476,6 @@ vca_status sync_ctrl(vca_ca* h) {
 // Totals and initial stop state of the current buffer, the first tile list, and a copy of the
 // current buffer into the other one (both buffers equal: the ACTIVE schedule relies on it).
 vca_status init_state(vca_ca* h, int steps_done) {
-    drop_graph(h);  // the arguments (vents, spill) may have changed
     const int cur = steps_done & 1, oth = cur ^ 1;
     const size_t n = h->plane_cells;
     VCA_CUDA(cudaMemcpyAsync(h->type[oth], h->type[cur], n, cudaMemcpyDeviceToDevice, h->stream));
@@ -1529,7 +1528,13 @@ constexpr int kGraphSteps = 16;  // steps captured in one CUDA graph
 // The launches of kGraphSteps steps, captured once per state set-up (the kernel arguments only
 // change with the terrain, the vents or the state).  Launches after the stop exit at once.
 vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
-    if (h->graph_exec) return VCA_OK;
+    // A captured graph stays valid while the arguments and launch shapes it was captured with are
+    // unchanged (a resident handle running job after job on one space keeps them; make_args zeroes
+    // the padding, so a byte comparison is exact).
+    if (h->graph_exec && std::memcmp(&h->graph_args, &k, sizeof(k)) == 0 && h->graph_grid == h->grid_blocks &&
+        h->graph_cand == h->cand_blocks)
+        return VCA_OK;
+    drop_graph(h);
     VCA_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < kGraphSteps; ++s) {
         ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
@@ -1540,6 +1545,9 @@ vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
     const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
     const cudaError_t e2 = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+    h->graph_args = k;
+    h->graph_grid = h->grid_blocks;
+    h->graph_cand = h->cand_blocks;
     cudaGraphDestroy(graph);
     if (e2 != cudaSuccess) {
         h->graph_exec = nullptr;
@@ -1917,7 +1925,6 @@ vca_status configure(vca_ca* h, const vca_ca_desc* d) {
     h->cand_blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->sms * std::max(1, h->cand_per_sm),
                                                                   (h->ntiles * kTileCells + kCandThreads - 1) / kCandThreads));
     if (vca_status s = encode_maps(h)) return s;
-    drop_graph(h);
     if (vca_status s = clear_planes(h)) return s;
     vca_vent none{0, 0, 0, 0};
     if (vca_status s = upload_vents(h, &none, 0)) return s;  // synchronizes the stream
@@ -2053,7 +2060,6 @@ vca_status vca_ca_reset(vca_ca* h) {
     if (vca_status s = clear_planes(h)) return s;
     vca_vent none{0, 0, 0, 0};
     if (vca_status s = upload_vents(h, &none, 0)) return s;  // synchronizes the stream
-    drop_graph(h);
     h->has_terrain = false;
     h->seeded = false;
     h->steps = 0;
@@ -2090,7 +2096,6 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->has_terrain = true;
     h->launches += 1;
-    drop_graph(h);
     return VCA_OK;
 }
 

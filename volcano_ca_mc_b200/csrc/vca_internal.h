@@ -190,7 +190,9 @@ struct vca_ca {
     uint64_t launches = 0;    // kernel launches issued
     int profile_kernels = 0;  // bracket each rules launch with events (set by VCA_PROFILE_KERNELS=1)
     std::vector<cudaEvent_t> prof_events;
-    cudaGraphExec_t graph_exec = nullptr;   // kGraphSteps steps of launches (rebuilt after set-up calls)
+    cudaGraphExec_t graph_exec = nullptr;   // kGraphSteps steps of launches
+    vca::CaKernelArgs graph_args;            // the arguments and grids graph_exec was captured with
+    int graph_grid = 0, graph_cand = 0;
     vca::CaCtrl* ctrl_ring = nullptr;       // pinned: two in-flight copies of the control block
     cudaEvent_t ring_ev[2] = {nullptr, nullptr};
 };
