@@ -138,7 +138,8 @@ vca_status vca_ca_download(vca_ca* ca, uint8_t* type, int32_t* flow_id, float* t
 vca_status vca_ca_set_state(vca_ca* ca, const uint8_t* type, const int32_t* flow_id, const float* temp,
                             const uint16_t* solid_step, const uint16_t* arrival_step, const int32_t* spill,
                             const vca_vent* vents, int vent_count, int steps_done);
-/* Spill levels in use (nx*ny, x fastest); returns VCA_ERR_STATE when there is no terrain. */
+/* Spill levels in use (LavaCA::spill_, set by applyTerrain, LavaCA.hpp:205; read by spillAt, 383):
+ * nx*ny values, x fastest; returns VCA_ERR_STATE when there is no terrain. */
 vca_status vca_ca_get_spill(vca_ca* ca, int32_t* spill);
 /* The per-flow sums of Simulation::flowSums (engine/src/app/Simulation.cpp:408-466) over the current
  * state, on the device: for flowId f in 1..flows, lava[f] and basalt[f] count the LAVA and BASALT
@@ -154,6 +155,7 @@ vca_status vca_ca_timing(vca_ca* ca, double* total_ms, double* rules_kernel_ms, 
  * step with CUDA events around each kernel: the average device time [ms] of the drop-depth, rules
  * and candidate kernels of a step, and the steps measured.  No counterpart in the reference. */
 vca_status vca_ca_kernel_times(vca_ca* ca, double* drop_ms, double* rules_ms, double* cand_ms, uint64_t* steps);
+/* ~LavaCA: frees the handle's device memory, stream and graph. */
 void vca_ca_destroy(vca_ca* ca);
 
 /* ------------------------------------------------------------------------------------------
@@ -207,13 +209,16 @@ vca_status vca_mc_set_domain_from_ca(vca_mc* mc, vca_ca* ca);
  * If use_in_dynamics is 0 the values are kept only for vca_mc_mobility() (the reference computes
  * them for statistics even when mc.mobilityFromCooling is false). */
 vca_status vca_mc_set_mobility_from_ca(vca_mc* mc, vca_ca* ca, double mobility_min, int use_in_dynamics);
-/* Current mobility values (N floats, 0 outside the domain); VCA_ERR_STATE if none were set. */
+/* Current mobility values (PottsMC::mobility_, set by setMobility, PottsMC.cpp:85-102): N floats, 0
+ * outside the domain; VCA_ERR_STATE if none were set. */
 vca_status vca_mc_mobility(vca_mc* mc, float* out);
 /* PottsMC::initialize with setCheckerboard(true) (PottsMC.cpp:104-224). */
 vca_status vca_mc_initialize(vca_mc* mc);
 /* count x PottsMC::sweep (PottsMC.cpp:516-533); accepted (may be NULL) gets the accepted
  * changes of these sweeps. */
 vca_status vca_mc_sweep(vca_mc* mc, int count, uint64_t* accepted);
+/* domainCells(), sweepsDone(), attempts(), accepted(), acceptedUphill(), colorCount()
+ * (PottsMC.hpp:102-106, 133). */
 vca_status vca_mc_get_info(vca_mc* mc, vca_mc_info* out);
 /* PottsMC::totalEnergy (PottsMC.cpp:590-664). */
 vca_status vca_mc_energy(vca_mc* mc, double* energy);
@@ -246,6 +251,7 @@ vca_status vca_mc_crystals(vca_mc* mc, int32_t* out);
 vca_status vca_mc_set_spins(vca_mc* mc, const int32_t* spins);
 /* Device time of the sweeps so far [ms] and of one colour-pass launch on average [ms]. */
 vca_status vca_mc_timing(vca_mc* mc, double* total_ms, double* color_kernel_ms, uint64_t* color_launches);
+/* ~PottsMC: frees the handle's device memory and stream. */
 void vca_mc_destroy(vca_mc* mc);
 
 /* Potts energy (the quantity of vca_mc_energy) of an nx*ny*nz int32 spin grid that is already in
@@ -265,8 +271,10 @@ vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, i
                                  int domain_full, uint64_t seed, int mcs, double J, double* energy, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Message of the last failing call on this host thread (the reference reports errors as C++
+ * exceptions; no counterpart). */
 const char* vca_last_error(void);
-/* ABI version and build string ("vca <abi> sm_100a ..."). */
+/* ABI version and build string ("vca <abi> sm_100a ..."); no counterpart in the reference. */
 const char* vca_version(void);
 
 #ifdef __cplusplus
