@@ -1560,8 +1560,11 @@ vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
 vca_status run_graphs(vca_ca* h, const CaKernelArgs& k) {
     if (vca_status s = ensure_graph(h, k)) return s;
     VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
+    // graphs that can still do a step before max_steps (the stop rule can only end the run sooner)
+    const int left = std::max(0, h->desc.max_steps - h->steps);
+    const int needed = (left + kGraphSteps - 1) / kGraphSteps;
     int pending = -1;
-    for (int launched = 0;; ++launched) {
+    for (int launched = 0; launched < needed; ++launched) {
         const int slot = launched & 1;
         VCA_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
         VCA_CUDA(cudaMemcpyAsync(&h->ctrl_ring[slot], h->ctrl, sizeof(CaCtrl), cudaMemcpyDeviceToHost, h->stream));
@@ -1572,7 +1575,6 @@ vca_status run_graphs(vca_ca* h, const CaKernelArgs& k) {
             if (h->ctrl_ring[pending].stop != VCA_STOP_RUNNING || h->ctrl_ring[pending].error) break;
         }
         pending = slot;
-        if (launched > 65536 / kGraphSteps + 4) break;  // max_steps <= 65535: cannot be reached
     }
     VCA_CUDA(cudaEventRecord(h->ev_b, h->stream));
     VCA_CUDA(cudaEventSynchronize(h->ev_b));
