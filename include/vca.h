@@ -264,9 +264,13 @@ void vca_mc_destroy(vca_mc* mc);
  * rejected with VCA_ERR_ARG.  Spins: 0 outside the domain, 1..Q inside; neighborhood, boundary,
  * domain_full and seed as in vca_mc_desc; mcs = sweeps done (the neighbourhood variant of
  * pentagonal/hexagonal cells at that MCS).  Both pointers must be device memory of the current
- * device.  The first call on each device looks up the scratch address (make it before any stream
- * capture).  The call returns once the work is queued.  Calls that overlap on one device race on
- * the shared scratch: order them (one stream, or events). */
+ * device, and the stream must belong to that device (VCA_ERR_ARG otherwise).  Outside stream
+ * capture every call looks up the scratch's address in the device's current context (a context
+ * made again after cudaDeviceReset is followed); during a capture the address of the last call
+ * outside capture is used, so make the first call on each device before any stream capture
+ * (VCA_ERR_STATE otherwise).  The call returns once the work is queued.  Every call uses the same
+ * scratch and the ticket is cleared on the stream before each launch; calls that overlap on one
+ * device race on the shared scratch: order them (one stream, or events). */
 vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, int neighborhood, int boundary,
                                  int domain_full, uint64_t seed, int mcs, double J, double* energy, void* stream);
 

@@ -1,10 +1,12 @@
 """Generates the golden fixtures under tests/golden/ by running the reference engine.
 
-Run in a checkout that has the reference sources (the reference engine is built by
-``make -C oracle ref`` into ``oracle/_ref/engine``):
+Run where the reference sources are at hand (the reference engine is built by
+``make -C oracle ref REF=<reference checkout>`` into ``oracle/_ref/engine``):
 
-    python tests/golden/make_golden.py            # the small cases
-    python tests/golden/make_golden.py --large    # hashes of the full-size 1024 x 1024 x 256 workload
+    python tests/golden/make_golden.py                 # the small cases
+    python tests/golden/make_golden.py --large         # hashes of the full-size 1024 x 1024 x 256 workload (c3)
+    python tests/golden/make_golden.py --large c1 c2   # the same for the 512 x 1 x 256 and 256 x 256 x 128 workloads
+    python tests/golden/make_golden.py --config-errors # the reference's validation messages for bad configs
 
 For every case in CASES it writes ``cases/<name>.json`` (the config, in the reference's schema),
 runs ``engine --config cases/<name>.json --out <tmp>`` and stores under ``<name>/``:
@@ -216,9 +218,10 @@ def save_initial(path: str, s: "O.CaState") -> None:
 
 
 def large(name: str = "c3") -> None:
-    """The full-size workload (volcano_ca_mc_b200.workloads, 1024 x 1024 x 256 for c3): the reference
-    engine's outputs are too large to commit, so only their hashes, the step count, the per-step
-    histories and the MC counters are kept (``<name>_large/expect.json``).  A few minutes of CPU."""
+    """A workload of volcano_ca_mc_b200.workloads at its full size (c1 512 x 1 x 256, c2 256 x 256 x 128,
+    c3 1024 x 1024 x 256): the reference engine's outputs are too large to commit, so only their
+    hashes, the step count, the per-step histories and the MC counters are kept
+    (``<name>_large/expect.json``).  Seconds of CPU for c1 and c2, a few minutes for c3."""
     from volcano_ca_mc_b200 import workloads
     w = workloads.get(name)
     tmp = tempfile.mkdtemp(prefix="vca_golden_large_")
@@ -248,12 +251,54 @@ def large(name: str = "c3") -> None:
         shutil.rmtree(tmp)
 
 
+# --set overrides that the reference's config validation refuses or warns about, one message each
+# (engine/src/io/Config.cpp:20-437): the texts land in batch_summary.csv and in --validate output.
+CONFIG_ERRORS: list[list[str]] = [
+    ["space.nx=0"], ["space.nx=1.5"], ["space.nx=99999999999999999999"], ["space.nx=1", "space.ny=1"],
+    ["space.nx=100000", "space.ny=100000", "space.nz=100"], ["neighborhood=hexagonal", "space.ny=5"],
+    ["space.ny=5", "space.nz=1"], ["boundary=reflecting"], ["grid=tiles"], ["mc.Q=1"], ["mc.J=0"], ["mc.kT=-1"],
+    ["vents.count=0"], ["ca.maxSteps=-3"], ["ca.ponding=1"], ["unknownKey=1"], ["ca.unknown=2"], ["space=5"],
+    ["terrain.type=file"], ["terrain.file=5"], ["vents.positions=5"], ["vents.positions=[[1]]"],
+    ["vents.positions=[[500,0]]"], ["vents.placement=positions"],
+    ["vents.placement=positions", "vents.positions=[[1,0],[1,0]]", "vents.count=2"],
+    ["vents.placement=positions", "vents.positions=[[1,0]]", "vents.count=2"], ["vents.eruptTemp=700"],
+    ["ca.mode=classic", "mc.enabled=true"], ["ca.mode=classic", "vents.count=100000000", "space.nx=20", "space.nz=20"],
+    ["vents.positions=[[1,0]]"], ["ca.mode=classic", "vents.placement=positions"],
+    ["mc.enabled=true", "mc.domain=full", "mc.update=checkerboard"], ["output.format=png"], ["mc.statsEvery=0"],
+]
+
+
+def config_errors() -> None:
+    """tests/golden/config_errors.json: the reference engine's --validate errors and warnings for
+    each override set of CONFIG_ERRORS."""
+    out = []
+    for sets in CONFIG_ERRORS:
+        args = ["--validate"]
+        for kv in sets:
+            args += ["--set", kv]
+        r = subprocess.run([O.REF_ENGINE, *args], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+        res = json.loads(r.stdout)
+        out.append({"set": sets, "exit": r.returncode, "errors": res["errors"], "warnings": res["warnings"]})
+    with open(os.path.join(HERE, "config_errors.json"), "w") as f:
+        json.dump(out, f, indent=1, ensure_ascii=False)
+        f.write("\n")
+    print("config_errors ok")
+
+
 def main() -> None:
+    if "--config-errors" in sys.argv:
+        config_errors()
+        return
     if "--large" in sys.argv:
-        large()
+        names = [a for a in sys.argv[sys.argv.index("--large") + 1:] if not a.startswith("-")] or ["c3"]
+        for name in names:
+            large(name)
         return
     if not os.path.exists(O.REF_ENGINE):
-        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
+        ref = os.environ.get("VCA_REFERENCE_DIR", "")
+        if not ref:
+            sys.exit("the reference engine is not built: set VCA_REFERENCE_DIR to the reference checkout")
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={ref}"], check=True)
     os.makedirs(os.path.join(CASES_DIR, "heightmaps"), exist_ok=True)
     with open(os.path.join(CASES_DIR, "heightmaps", "ridge_48x40.csv"), "w") as f:
         f.write(ridge_heightmap(48, 40))

@@ -80,3 +80,13 @@ def test_empty_inputs():
     assert not mc.crystals().any()
     mc.close()
     ca.close()
+
+
+@pytest.mark.parametrize("dims,match", [
+    ((1024, 1024, 256), "null spins"),           # exactly 2^28 cells: within the limit
+    ((15790321, 17, 1), "exceed the fixed scratch"),  # 2^28 + 1 cells
+])
+def test_noalloc_size_limit(dims, match):
+    """The 2^28-cell limit of vca_mc_energy_noalloc is checked before the pointers, so null pointers
+    show which side of the limit a size falls on without any grid or device."""
+    _refused(lambda: capi.mc_energy_noalloc(0, *dims, 0), match)

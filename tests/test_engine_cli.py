@@ -93,3 +93,18 @@ def test_batch_empty_folder(tmp_path):
     r = run("--batch", str(tmp_path), "--out", str(tmp_path / "out"))
     assert r.returncode == 1
     assert r.stderr.startswith("Błąd konfiguracji: ")
+
+
+def test_validation_messages_equal_reference():
+    """--validate on configs the reference refuses or warns about: the same exit code and the same
+    error and warning texts, word for word (tests/golden/config_errors.json, made by make_golden.py
+    --config-errors from the reference engine; engine/src/io/Config.cpp:20-437)."""
+    with open(os.path.join(GOLDEN, "config_errors.json")) as f:
+        cases = json.load(f)
+    for case in cases:
+        args = ["--validate"]
+        for kv in case["set"]:
+            args += ["--set", kv]
+        r = run(*args)
+        out = json.loads(r.stdout)
+        assert (r.returncode, out["errors"], out["warnings"]) == (case["exit"], case["errors"], case["warnings"]), case

@@ -184,3 +184,34 @@ def test_oracle_mc_from_file_matches_reference_engine():
     spin, rows, totals = oracle_mc(used["mc"], used, (s.nx, s.ny, s.nz), dom, mob, False)
     assert sha(crystal_bytes((s.nx, s.ny, s.nz), spin)) == exp["files"]["mc_result.bin"]
     check_mc_rows(exp["mc_stats_csv"], rows)
+
+
+def test_oracle_matches_reference_engine_c1_workload():
+    """The 512 x 1 x 256 cross-section workload (volcano_ca_mc_b200.workloads.c1) at its full size:
+    the oracle's CA run from the heightmap and vents of the workload, and its 50 Potts sweeps, give the
+    reference engine's ca_result.bin / mc_result.bin hashes, histories and MC counters
+    (tests/golden/c1_large, made by make_golden.py --large c1)."""
+    from volcano_ca_mc_b200 import workloads
+    from tests import cases as C
+
+    w = workloads.get("c1")
+    with open(os.path.join(GOLDEN, "c1_large", "expect.json")) as f:
+        exp = json.load(f)
+    s0 = C.initial_state(w.nx, w.ny, w.nz, w.heights, w.vent_cells(), 1200.0)
+    p = O.CaParams(w.nx, w.ny, w.nz, O.NB[w.neighborhood], int(w.boundary == "periodic"), 0, w.seed, w.max_steps, 300,
+                   1200.0, 800.0, 0.3, 1.5, 0.1, 1)
+    spill = O.fill_depressions(w.heights, w.nx, w.ny, False, False)
+    s, steps, stop, act, chg = O.ca_run(p, s0, spill, O.vent_table(w.vent_cells()))
+    assert steps == exp["steps"] and STOP_TEXT[stop] == exp["stopReason"]
+    assert act == exp["activeCells"] and chg == exp["changedCells"]
+    assert sha(s.to_bytes()) == exp["files"]["ca_result.bin"]
+    dom = O.basalt_domain(s)
+    mob = O.mobility_from_cooling(s, dom, 0.05)
+    used = {"neighborhood": w.neighborhood, "boundary": w.boundary, "rngSeed": w.seed}
+    spin, rows, totals = oracle_mc({"Q": w.Q, "J": 1.0, "kT": w.kT, "mcs": w.mcs, "statsEvery": w.mcs}, used,
+                                   (w.nx, w.ny, w.nz), dom, mob, False)
+    assert sha(crystal_bytes((w.nx, w.ny, w.nz), spin)) == exp["files"]["mc_result.bin"]
+    check_mc_rows(exp["mc_stats_csv"], rows)
+    mc = exp["mc"]
+    assert [int(t) for t in totals] == [mc["attempts"], mc["accepted"], mc["acceptedUphill"]]
+    assert int(dom.sum()) == mc["domainCells"]

@@ -52,6 +52,25 @@ def test_noalloc_energy_matches_handle(nx, ny, nz, nb, bc, full, sweeps):
     assert got[0] == expected and got[1] == expected, (got, expected)
 
 
+def test_noalloc_large_then_small_call():
+    """A 384-block call followed by a 1-block call on the same stream: the ticket target changes
+    between them, and each result must still equal the handle's energy."""
+    import torch
+
+    big = handle_energy_and_spins(128, 128, 96, "moore", "periodic", True, 2)
+    small = handle_energy_and_spins(24, 20, 8, "von_neumann", "absorbing", True, 3)
+    dev_big = torch.from_numpy(big[1]).cuda()
+    dev_small = torch.from_numpy(small[1]).cuda()
+    out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    capi.mc_energy_noalloc(dev_big.data_ptr(), 128, 128, 96, out.data_ptr(), neighborhood="moore", boundary="periodic",
+                           domain_full=True, seed=5, mcs=2, J=1.0, stream=stream)
+    capi.mc_energy_noalloc(dev_small.data_ptr(), 24, 20, 8, out.data_ptr() + 8, neighborhood="von_neumann",
+                           boundary="absorbing", domain_full=True, seed=5, mcs=3, J=1.0, stream=stream)
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == [big[0], small[0]]
+
+
 def test_noalloc_rejects_oversized_grid():
     import torch
 

@@ -1,6 +1,8 @@
 // config.cpp -- configuration with the reference engine's keys, defaults and validation
 // (engine/src/io/Config.cpp): defaults <- JSON file <- --set overrides, unknown keys rejected,
-// '_'-prefixed keys treated as comments, the merged JSON kept for config_used.json.
+// '_'-prefixed keys treated as comments, the merged JSON kept for config_used.json.  The messages
+// are the reference's own Polish texts (the batch runner's batch_summary.csv and the GUI show them
+// verbatim), so a bad config reads the same through either engine.
 #include <cmath>
 #include <fstream>
 #include <limits>
@@ -12,7 +14,7 @@ namespace eng {
 
 namespace {
 
-std::string q(const std::string& path) { return "\"" + path + "\""; }
+std::string q(const std::string& path) { return "„" + path + "”"; }  // „path”
 
 std::vector<std::string> split_path(const std::string& path) {
     std::vector<std::string> parts;
@@ -25,7 +27,7 @@ std::vector<std::string> split_path(const std::string& path) {
 const Json& field(const Json& j, const std::string& path) {
     const Json* cur = &j;
     for (const std::string& part : split_path(path)) {
-        if (!cur->is_object() || !cur->contains(part)) throw ConfigError("Missing parameter " + q(path));
+        if (!cur->is_object() || !cur->contains(part)) throw ConfigError("Brak parametru " + q(path));
         cur = cur->find(part);
     }
     return *cur;
@@ -36,13 +38,13 @@ long long get_integer(const Json& j, const std::string& path, long long lo, long
     const Json& v = field(j, path);
     if (!v.is_integer() || (v.is_unsigned() && v.as_u64() > (uint64_t)hi)) {
         if (v.is_unsigned())
-            throw ConfigError("Parameter " + q(path) + " is too large (max " + std::to_string(hi) + "), given: " + v.dump());
-        throw ConfigError("Parameter " + q(path) + " must be an integer, given: " + v.dump());
+            throw ConfigError("Parametr " + q(path) + " jest za duży (maks. " + std::to_string(hi) + "), podano: " + v.dump());
+        throw ConfigError("Parametr " + q(path) + " musi być liczbą całkowitą, podano: " + v.dump());
     }
     const long long x = v.as_i64();
     if (x < lo || x > hi)
-        throw ConfigError("Parameter " + q(path) + " must be in " + std::to_string(lo) + ".." + std::to_string(hi) +
-                          ", given: " + std::to_string(x));
+        throw ConfigError("Parametr " + q(path) + " musi być z zakresu " + std::to_string(lo) + ".." +
+                          std::to_string(hi) + ", podano: " + std::to_string(x));
     return x;
 }
 int get_int(const Json& j, const std::string& path, int lo, int hi) { return (int)get_integer(j, path, lo, hi); }
@@ -50,11 +52,11 @@ int get_int(const Json& j, const std::string& path, int lo, int hi) { return (in
 // Config.cpp:66-78
 double get_number(const Json& j, const std::string& path, double lo, double hi) {
     const Json& v = field(j, path);
-    if (!v.is_number()) throw ConfigError("Parameter " + q(path) + " must be a number, given: " + v.dump());
+    if (!v.is_number()) throw ConfigError("Parametr " + q(path) + " musi być liczbą, podano: " + v.dump());
     const double x = v.as_double();
     if (!std::isfinite(x) || x < lo || x > hi) {
         std::ostringstream os;
-        os << "Parameter " << q(path) << " must be in " << lo << ".." << hi << ", given: " << x;
+        os << "Parametr " << q(path) << " musi być z zakresu " << lo << ".." << hi << ", podano: " << x;
         throw ConfigError(os.str());
     }
     return x;
@@ -62,7 +64,8 @@ double get_number(const Json& j, const std::string& path, double lo, double hi) 
 
 bool get_bool(const Json& j, const std::string& path) {
     const Json& v = field(j, path);
-    if (!v.is_bool()) throw ConfigError("Parameter " + q(path) + " must be true or false, given: " + v.dump());
+    if (!v.is_bool())
+        throw ConfigError("Parametr " + q(path) + " musi mieć wartość true lub false, podano: " + v.dump());
     return v.as_bool();
 }
 
@@ -74,14 +77,15 @@ E get_enum(const Json& j, const std::string& path, std::initializer_list<std::pa
     if (v.is_string())
         for (const auto& o : options)
             if (v.as_string() == o.first) return o.second;
-    throw ConfigError("Parameter " + q(path) + " has an invalid value " + v.dump() + "; allowed: " + allowed);
+    throw ConfigError("Parametr " + q(path) + " ma nieprawidłową wartość " + v.dump() +
+                      "; dozwolone: " + allowed);
 }
 
 // vents.positions (Config.cpp:111-147): pairs of integers inside the grid, no repeated column.
 std::vector<std::pair<int, int>> get_columns(const Json& j, const std::string& path, const Dims& d) {
     const Json& list = field(j, path);
     if (!list.is_array())
-        throw ConfigError("Parameter " + q(path) + " must be a list of [x, y] pairs, e.g. [[80, 75], [82, 70]], given: " +
+        throw ConfigError("Parametr " + q(path) + " musi być listą par [x, y], np. [[80, 75], [82, 70]], podano: " +
                           list.dump());
     std::vector<std::pair<int, int>> out;
     for (size_t i = 0; i < list.size(); ++i) {
@@ -89,15 +93,17 @@ std::vector<std::pair<int, int>> get_columns(const Json& j, const std::string& p
         const std::string where = path + "[" + std::to_string(i) + "]";
         auto is_int = [](const Json& v) { return v.is_integer() && (!v.is_unsigned() || v.as_u64() <= 100000ULL); };
         if (!p.is_array() || p.size() != 2 || !is_int(p[0]) || !is_int(p[1]))
-            throw ConfigError("Parameter " + q(where) + " must be an integer pair [x, y], given: " + p.dump());
+            throw ConfigError("Parametr " + q(where) + " musi być parą liczb całkowitych [x, y], podano: " + p.dump());
         const long long x = p[0].as_i64(), y = p[1].as_i64();
         if (x < 0 || x >= d.nx || y < 0 || y >= d.ny)
-            throw ConfigError("Parameter " + q(where) + " = " + p.dump() + " lies outside the grid: x must be in 0.." +
-                              std::to_string(d.nx - 1) + ", y in 0.." + std::to_string(d.ny - 1));
+            throw ConfigError("Parametr " + q(where) + " = " + p.dump() + " leży poza siatką: x musi być z zakresu 0.." +
+                              std::to_string(d.nx - 1) + ", y z zakresu 0.." + std::to_string(d.ny - 1) +
+                              " (space.nx = " + std::to_string(d.nx) + ", space.ny = " + std::to_string(d.ny) + ")");
         for (const auto& c : out)
             if (c.first == (int)x && c.second == (int)y)
-                throw ConfigError("Parameter " + q(where) + " = " + p.dump() +
-                                  " repeats an earlier column; a column holds at most one vent");
+                throw ConfigError("Parametr " + q(where) + " = " + p.dump() +
+                                  " powtarza kolumnę z wcześniejszego elementu listy; w jednej kolumnie może być "
+                                  "najwyżej jeden krater");
         out.emplace_back((int)x, (int)y);
     }
     return out;
@@ -112,11 +118,11 @@ void merge(Json& base, const Json& patch, const std::string& prefix) {
         if (!target) {
             std::string allowed;
             for (const auto& b : base.members()) allowed += (allowed.empty() ? "" : ", ") + b.first;
-            throw ConfigError("Unknown parameter " + q(path) + "; allowed in this section: " + allowed);
+            throw ConfigError("Nieznany parametr " + q(path) + "; dozwolone w tej sekcji: " + allowed);
         }
         if (target->is_object()) {
             if (!kv.second.is_object())
-                throw ConfigError("Parameter " + q(path) + " is a section: expected an object { ... }, given: " +
+                throw ConfigError("Parametr " + q(path) + " jest sekcją: oczekiwano obiektu { ... }, podano: " +
                                   kv.second.dump());
             merge(*target, kv.second, path);
         } else {
@@ -128,7 +134,7 @@ void merge(Json& base, const Json& patch, const std::string& prefix) {
 // --set a.b=value: JSON when it parses, else a plain string (Config.cpp:205-235).
 void apply_override(Json& j, const std::string& kv) {
     const size_t eq = kv.find('=');
-    if (eq == std::string::npos || eq == 0) throw ConfigError("An override must look like key=value, given: " + kv);
+    if (eq == std::string::npos || eq == 0) throw ConfigError("Nadpisanie musi mieć postać klucz=wartość, podano: " + kv);
     const std::string key = kv.substr(0, eq), text = kv.substr(eq + 1);
     Json value;
     try {
@@ -138,7 +144,7 @@ void apply_override(Json& j, const std::string& kv) {
     }
     const std::vector<std::string> parts = split_path(key);
     for (const std::string& p : parts)
-        if (p.empty()) throw ConfigError("Invalid parameter path in override: " + key);
+        if (p.empty()) throw ConfigError("Nieprawidłowa ścieżka parametru w nadpisaniu: " + key);
     Json patch = value;
     for (auto it = parts.rbegin(); it != parts.rend(); ++it) {
         Json obj = Json::object();
@@ -191,16 +197,16 @@ Config Config::load(const std::string& path, const std::vector<std::string>& ove
     bool space_given = false;
     if (!path.empty()) {
         std::ifstream in(path, std::ios::binary);
-        if (!in) throw ConfigError("Cannot open the config file: " + path);
+        if (!in) throw ConfigError("Nie można otworzyć pliku konfiguracyjnego: " + path);
         std::stringstream ss;
         ss << in.rdbuf();
         Json file;
         try {
             file = Json::parse(ss.str(), true);
         } catch (const JsonError& e) {
-            throw ConfigError("JSON syntax error in " + path + ": " + e.what());
+            throw ConfigError("Błąd składni JSON w pliku " + path + ": " + e.what());
         }
-        if (!file.is_object()) throw ConfigError("The config file " + path + " must hold a JSON object { ... }");
+        if (!file.is_object()) throw ConfigError("Plik konfiguracyjny " + path + " musi zawierać obiekt JSON { ... }");
         merge(j, file, "");
         space_given = file.contains("space");
     }
@@ -221,10 +227,11 @@ Config Config::from_json(const Json& j) {
     c.space.ny = get_int(j, "space.ny", 1, 100000);
     c.space.nz = get_int(j, "space.nz", 1, 100000);
     if (c.space.active_axes() < 2)
-        throw ConfigError("The space must be 2D (exactly one size equal to 1) or 3D; given " + std::to_string(c.space.nx) +
-                          " x " + std::to_string(c.space.ny) + " x " + std::to_string(c.space.nz));
+        throw ConfigError("Przestrzeń musi być 2D (dokładnie jeden wymiar równy 1) lub 3D; podano " +
+                          std::to_string(c.space.nx) + " x " + std::to_string(c.space.ny) + " x " + std::to_string(c.space.nz));
     if (c.space.cells() > 2000000000ULL)
-        throw ConfigError("The space has too many cells (" + std::to_string(c.space.cells()) + "); the maximum is 2 000 000 000");
+        throw ConfigError("Przestrzeń ma za dużo komórek (" + std::to_string(c.space.cells()) +
+                          "); maksimum to 2 000 000 000");
     c.grid = get_enum<std::string>(j, "grid", {{"vector", std::string("vector")}, {"matrix", std::string("matrix")}});
     c.boundary = get_enum<Bc>(j, "boundary", {{"absorbing", Bc::Absorbing}, {"periodic", Bc::Periodic}});
     c.neighborhood = get_enum<Nb>(j, "neighborhood", {{"von_neumann", Nb::VonNeumann}, {"moore", Nb::Moore},
@@ -236,7 +243,9 @@ Config Config::from_json(const Json& j) {
     c.mc.Q = get_int(j, "mc.Q", 2, 1000000000);
     c.mc.mcs = get_int(j, "mc.mcs", 0, 10000000);
     c.mc.J = get_number(j, "mc.J", 0.0, 1e6);
-    if (c.mc.J <= 0.0) throw ConfigError("Parameter \"mc.J\" (grain boundary energy) must be above 0, given: " + field(j, "mc.J").dump());
+    if (c.mc.J <= 0.0)
+        throw ConfigError("Parametr " + q("mc.J") + " (energia granicy ziarna) musi być większy od 0, podano: " +
+                          field(j, "mc.J").dump());
     c.mc.kT = get_number(j, "mc.kT", 0.0, 1e6);
     c.mc.mobility_from_cooling = get_bool(j, "mc.mobilityFromCooling");
     c.mc.mobility_min = get_number(j, "mc.mobilityMin", 0.0, 1.0);
@@ -255,12 +264,12 @@ Config Config::from_json(const Json& j) {
     c.ca.front = get_enum<bool>(j, "ca.sweep", {{"front", true}, {"full", false}});
 
     if (runs_ca && c.ca.mode == Mode::Lava && c.space.is2d() && c.space.ny != 1)
-        throw ConfigError("In lava mode a 2D space is the vertical x-z cross-section: ny = 1 is required (given nx = " +
+        throw ConfigError("W trybie lava przestrzeń 2D to przekrój pionowy x–z: wymagane ny = 1 (podano nx = " +
                           std::to_string(c.space.nx) + ", ny = " + std::to_string(c.space.ny) + ", nz = " +
                           std::to_string(c.space.nz) + ")");
     if (c.neighborhood == Nb::Hexagonal && !c.space.is2d())
-        throw ConfigError("The \"hexagonal\" neighbourhood is defined in 2D only; for a 3D space choose von_neumann, moore "
-                          "or pentagonal");
+        throw ConfigError("Sąsiedztwo " + q("hexagonal") + " jest zdefiniowane tylko w 2D; dla przestrzeni 3D "
+                          "wybierz von_neumann, moore lub pentagonal");
 
     c.terrain.type = get_enum<TerrainType>(j, "terrain.type", {{"cone", TerrainType::Cone}, {"file", TerrainType::File}});
     c.terrain.peak = get_number(j, "terrain.peakHeight", 0.0, 1e6);
@@ -270,10 +279,10 @@ Config Config::from_json(const Json& j) {
     c.terrain.noise = get_number(j, "terrain.noise", 0.0, 1.0);
     const Json file = field(j, "terrain.file");
     if (!file.is_null() && !file.is_string())
-        throw ConfigError("Parameter \"terrain.file\" must be a path (text) or null, given: " + file.dump());
+        throw ConfigError("Parametr " + q("terrain.file") + " musi być ścieżką (tekst) albo null, podano: " + file.dump());
     c.terrain.file = file.is_string() ? file.as_string() : std::string();
     if (runs_ca && c.ca.mode == Mode::Lava && c.terrain.type == TerrainType::File && c.terrain.file.empty())
-        throw ConfigError("terrain.type = \"file\" needs a path in \"terrain.file\"");
+        throw ConfigError("Dla terrain.type = \"file\" trzeba podać ścieżkę w " + q("terrain.file"));
 
     c.vents.count = get_int(j, "vents.count", 1, 100000000);
     c.vents.placement = get_enum<Placement>(j, "vents.placement", {{"crater", Placement::Crater}, {"random", Placement::Random},
@@ -282,32 +291,35 @@ Config Config::from_json(const Json& j) {
     const bool lava_ca = runs_ca && c.ca.mode == Mode::Lava;
     if (lava_ca && c.vents.placement == Placement::Positions) {
         if (listed == 0)
-            throw ConfigError("vents.placement = \"positions\" needs the vent list \"vents.positions\", e.g. [[80, 75]]");
+            throw ConfigError("vents.placement = \"positions\" wymaga listy kraterów w " + q("vents.positions") +
+                              ", np. [[80, 75]] (w GUI: kliknięcie na mapie wysokości)");
         if ((size_t)c.vents.count != listed)
-            throw ConfigError("vents.count (" + std::to_string(c.vents.count) + ") must equal the number of vents in "
-                              "\"vents.positions\" (" + std::to_string(listed) + ")");
+            throw ConfigError("vents.count (" + std::to_string(c.vents.count) + ") musi być równe liczbie kraterów w " +
+                              q("vents.positions") + " (" + std::to_string(listed) +
+                              "), bo przy placement = \"positions\" każdy krater ma podane położenie");
     } else if (lava_ca && listed > 0) {
-        c.warnings.push_back(std::string("vents.positions is ignored because vents.placement = \"") +
+        c.warnings.push_back(std::string("vents.positions jest ignorowane, bo vents.placement = \"") +
                              (c.vents.placement == Placement::Crater ? "crater" : "random") +
-                             "\" (positions are drawn); vents at given columns: placement = \"positions\"");
+                             "\" (położenia losowane); kratery w zadanych miejscach: placement = \"positions\"");
     } else if (runs_ca && c.ca.mode == Mode::Classic && c.vents.placement == Placement::Positions) {
-        c.warnings.push_back("in classic mode the seeds are drawn over the whole space, so vents.placement = \"positions\" "
-                             "and vents.positions are ignored");
+        c.warnings.push_back("w trybie classic zarodki są losowane w całej przestrzeni, więc vents.placement = "
+                             "\"positions\" i vents.positions są ignorowane");
     }
     c.vents.eruption_steps = get_int(j, "vents.eruptionSteps", 0, 65535);
     c.vents.erupt_temp = get_number(j, "vents.eruptTemp", -1e6, 1e6);
     if (runs_ca && c.ca.mode == Mode::Lava && c.vents.erupt_temp < c.ca.solidus)
-        throw ConfigError("vents.eruptTemp must not be below ca.solidusTemp, or lava would freeze in the vent at once");
+        throw ConfigError("vents.eruptTemp musi być nie mniejsze niż ca.solidusTemp, inaczej lawa "
+                          "zastygłaby od razu w kraterze");
     if (runs_ca && c.ca.mode == Mode::Classic && (uint64_t)c.vents.count > c.space.cells())
-        throw ConfigError("vents.count (" + std::to_string(c.vents.count) + ") cannot exceed the number of cells (" +
+        throw ConfigError("vents.count (" + std::to_string(c.vents.count) + ") nie może przekraczać liczby komórek (" +
                           std::to_string(c.space.cells()) + ")");
 
     if (c.mc.enabled && !c.mc.full && c.ca.mode == Mode::Classic)
-        throw ConfigError("mc.domain = \"basalt\" needs ca.mode = \"lava\" (classic mode has no basalt); classic MC grain "
-                          "growth is mc.domain = \"full\"");
+        throw ConfigError("mc.domain = \"basalt\" wymaga ca.mode = \"lava\" (w trybie classic nie ma bazaltu); "
+                          "klasyczny rozrost ziaren MC to mc.domain = \"full\"");
     if (c.mc.full_only() && c.mc.mobility_from_cooling)
-        c.warnings.push_back("mc.mobilityFromCooling applies to mc.domain = \"basalt\" only (the CA cooling time); it is "
-                             "ignored in full mode");
+        c.warnings.push_back("mc.mobilityFromCooling dotyczy tylko mc.domain = \"basalt\" (czas stygnięcia lawy z CA); "
+                             "w trybie full jest ignorowane");
 
     c.output.format = get_enum<OutputFormat>(j, "output.format", {{"txt", OutputFormat::Txt}, {"bin", OutputFormat::Bin},
                                                                   {"both", OutputFormat::Both}, {"none", OutputFormat::None}});
@@ -325,8 +337,8 @@ Config Config::from_json(const Json& j) {
     get_enum<bool>(j, "mpi.bcast", {{"json", false}, {"struct", true}});
     get_enum<bool>(j, "mpi.io", {{"gather", false}, {"mpiio", true}});
     if (c.mc.enabled && !c.mc.checkerboard)
-        throw ConfigError("mc.update = \"random\" is sequential by definition (each trial sees the previous ones) and is "
-                          "not offered by the GPU engine; use mc.update = \"checkerboard\"");
+        throw ConfigError("mc.update = \"random\" jest z natury sekwencyjne (każda próba widzi wynik poprzednich), "
+                          "więc silnik GPU go nie oferuje; równoległe MC: mc.update = \"checkerboard\"");
     c.effective = j;
     return c;
 }

@@ -3,9 +3,10 @@
 //
 // It restates the reduction of vca_mc_energy (PottsMC::totalEnergy, engine/src/mc/PottsMC.cpp:590-664)
 // for callers that own every byte of device memory: the per-block partial sums and the
-// last-block ticket live in one file-scope __device__ array of fixed size, whose address is looked
-// up once per device with cudaGetSymbolAddress.  The result is written to a device double of the
-// caller, on the caller's stream.
+// last-block ticket live in one file-scope __device__ array of fixed size, whose address host code
+// looks up with cudaGetSymbolAddress (on every call outside stream capture, so that a context that
+// was torn down and made again -- cudaDeviceReset -- never leaves a stale address behind).  The
+// result is written to a device double of the caller, on the caller's stream.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -114,18 +115,29 @@ __global__ __launch_bounds__(kNaThreads) void mc_energy_noalloc_kernel(NaGrid g,
 std::mutex g_na_mutex;
 unsigned long long* g_na_scratch[kNaMaxDevices] = {};
 
-// Address of the scratch array on the current device, looked up once per device.
-vca_status na_scratch(int device, unsigned long long** out) {
+// Address of the scratch array on the current device.  Outside stream capture it is looked up on
+// every call (the address belongs to the device's current context; a reset context gets a new one)
+// and remembered; during capture, where a lookup could load the module and break the capture, the
+// remembered address of the last call outside capture is used, and a device that never had one is
+// refused.
+vca_status na_scratch(int device, bool capturing, unsigned long long** out) {
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_scratch[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_energy_scratch);
-        if (e != cudaSuccess) {
-            set_error(std::string("vca_mc_energy_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            return VCA_ERR_CUDA;
+    if (capturing) {
+        if (!g_na_scratch[device]) {
+            set_error("vca_mc_energy_noalloc: the first call on a device must come before any stream capture "
+                      "(it looks up the address of the static scratch)");
+            return VCA_ERR_STATE;
         }
-        g_na_scratch[device] = static_cast<unsigned long long*>(p);
+        *out = g_na_scratch[device];
+        return VCA_OK;
     }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_energy_scratch);
+    if (e != cudaSuccess) {
+        set_error(std::string("vca_mc_energy_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        return VCA_ERR_CUDA;
+    }
+    g_na_scratch[device] = static_cast<unsigned long long*>(p);
     *out = g_na_scratch[device];
     return VCA_OK;
 }
@@ -155,10 +167,6 @@ extern "C" {
 
 vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, int neighborhood, int boundary,
                                  int domain_full, uint64_t seed, int mcs, double J, double* energy, void* stream) {
-    if (!spins || !energy) {
-        set_error("vca_mc_energy_noalloc: null spins or energy pointer");
-        return VCA_ERR_ARG;
-    }
     if (nx < 1 || ny < 1 || nz < 1 || mcs < 0 || (boundary != VCA_BC_ABSORBING && boundary != VCA_BC_PERIODIC)) {
         set_error("vca_mc_energy_noalloc: invalid dimensions, boundary or mcs");
         return VCA_ERR_ARG;
@@ -167,6 +175,10 @@ vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, i
     if (n > kNaMaxCells) {
         set_error("vca_mc_energy_noalloc: " + std::to_string(n) + " cells exceed the fixed scratch of this entry point (at most " +
                   std::to_string(kNaMaxCells) + " cells = 65536 blocks of 4096); use vca_mc_energy for larger grids");
+        return VCA_ERR_ARG;
+    }
+    if (!spins || !energy) {
+        set_error("vca_mc_energy_noalloc: null spins or energy pointer");
         return VCA_ERR_ARG;
     }
     NbTable nb;
@@ -183,8 +195,20 @@ vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, i
     }
     if (vca_status s = na_device_pointer(spins, device, "spins")) return s;
     if (vca_status s = na_device_pointer(energy, device, "energy")) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread) {
+        int stream_device = -1;
+        VCA_CUDA(cudaStreamGetDevice(st, &stream_device));
+        if (stream_device != device) {
+            set_error("vca_mc_energy_noalloc: the stream belongs to device " + std::to_string(stream_device) +
+                      ", not to the current device " + std::to_string(device));
+            return VCA_ERR_ARG;
+        }
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    VCA_CUDA(cudaStreamIsCapturing(st, &cap));
     unsigned long long* scratch = nullptr;
-    if (vca_status s = na_scratch(device, &scratch)) return s;
+    if (vca_status s = na_scratch(device, cap != cudaStreamCaptureStatusNone, &scratch)) return s;
 
     const bool periodic = boundary == VCA_BC_PERIODIC;
     NaGrid g{};
@@ -201,7 +225,6 @@ vca_status vca_mc_energy_noalloc(const int32_t* spins, int nx, int ny, int nz, i
     g.n = n;
     g.blocks = (int)((n + kNaCellsPerBlock - 1) / kNaCellsPerBlock);
     g.scale = g.forward ? J : 0.5 * J;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     // the ticket must start at zero: the kernel's last block puts it back, this makes every call
     // independent of an earlier one that did not finish
     VCA_CUDA(cudaMemsetAsync(scratch + kNaTicket, 0, sizeof(unsigned long long), st));
