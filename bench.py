@@ -1,37 +1,39 @@
 #!/usr/bin/env python
 """Benchmark of the lava-CA + Potts-MC hot paths on B200 (one JSON line on stdout, rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3] [--impl ours|reference]
 
 A step is one job of the workload: the lava CA run from the seeded terrain to its stop rule (for
-c2, 400 steps of a 256 x 256 x 128 grid) followed by the Potts checkerboard crystallisation of
-the basalt it left (100 MCS).  Inputs are resident in HBM when the timed region starts (each job's
-handle is set up beforehand); L2 is flushed before every job outside the job's device events.
+c3, 800 steps of a 1024 x 1024 x 256 grid, random pentagonal neighbourhood) followed by the Potts
+checkerboard crystallisation of the basalt it left (200 MCS).  The jobs run on resident handles:
+terrain and vents are in HBM when a job's timed region starts; L2 is flushed before every CA run
+and MC run, outside their device events (c3's 7 GB of state is far larger than L2 anyway).
 
-  value          CA cell-updates/s = cells x CA steps / CA device time (ACTIVE schedule, the
-                 default), whole job over all ranks.
+  value          CA cell-updates/s = cells x CA steps / CA device time (ACTIVE schedule), all ranks.
+  parity         the last timed job's ca_result.bin / mc_result.bin bytes (SHA-256) against the reference
+                 engine's run of the same config (tests/golden/<workload>_large), computed after timing.
   mc             MC trials/s and attempts/s of the same jobs (attempts exclude mobility skips).
-  dense          the same jobs with the DENSE schedule (every cell every step).
-  roofline       the rules kernel of the DENSE jobs: 26 B per cell (13 B state read + 13 B written)
-                 over its CUDA-event launch time, against the measured HBM copy bandwidth; traffic =
-                 the ncu DRAM bytes per launch recorded in profiles/.  roofline_active: the same for
-                 the ACTIVE jobs (26 B per cell of the processed tiles).
+  dense          the same job with the DENSE schedule (every cell every step).
+  roofline       the rules kernel of the DENSE job: 26 B per cell (13 B state read + 13 B written) over
+                 its CUDA-event launch time, against the measured HBM copy bandwidth; traffic = ncu DRAM
+                 bytes per cell of the same kernel on the c3q case (profiles/), times the cells of a launch.
   kernels_ms     device time per step of the drop-depth, rules and candidate kernels.
-  large          the full-size workload c3 (1024 x 1024 x 256, random pentagonal, 800 steps, 200 MCS):
-                 one ACTIVE job with its MC, one DENSE job, the DENSE rules-kernel roofline.
-  e2e            CA cell-updates/s through the C ABI on one resident handle: reset, terrain and vents
-                 from host memory, run, the five planes back into pinned host memory.
-  engine_cli     the engine command on one job of the workload, its times.json sections.
-  cpu_baseline   the reference engine (oracle/_ref/engine, --threads = host cores) on one job.
+  e2e            the same metric through the C ABI with host buffers: reset, terrain and vents from host
+                 memory, run, all five planes back into pinned host memory, host wall clock.
+  cpu_baseline   the reference engine (oracle/_ref/engine, --threads = host cores) on one full job.
+  c2             the 256 x 256 x 128 workload: ACTIVE / DENSE figures and its parity.
+  batched/served many small independent jobs through the job server (volcano_ca_mc_b200.serve).
 
 With --impl reference the reference engine itself is timed on the host cores (rank 0 only).
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
+import struct
 import subprocess
 import sys
 import tempfile
@@ -44,6 +46,9 @@ sys.path.insert(0, ROOT)
 HBM_FALLBACK_GBS = 6650.0
 BYTES_PER_CELL_UPDATE = 26   # 13 B state read + 13 B next state written
 BYTES_PER_TRIAL = 12         # spin read + spin write + mobility read
+# The reference arm's bounded sample: the first REF_SAMPLE_STEPS CA steps of the workload's job (its
+# front sweep runs from step 0 only: the reference engine has no resume), MC off.
+REF_SAMPLE_STEPS = {"c1": 300, "c2": 400, "c3": 300, "c3q": 300}
 
 
 def parse():
@@ -51,17 +56,21 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--workload", default="c3")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-large", action="store_true", help="skip the full-size 1024x1024x256 sub-benchmark")
+    ap.add_argument("--no-c2", action="store_true", help="skip the 256x256x128 sub-benchmark")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched job-mix sub-benchmark")
     ap.add_argument("--no-served", action="store_true", help="skip the served (Poisson arrivals) sub-benchmark")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the served arrival trace")
-    ap.add_argument("--slots", type=int, default=16, help="worker slots of the batched and served runs")
+    ap.add_argument("--slots", type=int, default=16, help="workers of the job server in the batched and served runs")
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[20.0, 60.0, 120.0, 240.0],
+                    help="arrival rates [jobs/s] of the served sweep")
+    ap.add_argument("--sweep-seconds", type=float, default=4.0, help="length of each trace of the served sweep")
     ap.add_argument("--profile-job", choices=["active", "dense", "mc"], default=None,
                     help="run exactly one CA job with this schedule (no warm-up, no MC), or with mc one ACTIVE "
                          "CA job and its MC stage, and exit: the case ncu captures")
+    ap.add_argument("--max-steps", type=int, default=None, help="with --profile-job: stop the CA after this many steps")
     return ap.parse_args()
 
 
@@ -84,18 +93,20 @@ def max_over_ranks(values, device, world):
     return t.tolist()
 
 
-def ncu_traffic(kernel: str, workload: str, schedule: str):
-    """DRAM bytes per launch of a kernel from the committed ncu summaries (profiles/*.md lines
-    `traffic: kernel=<k> workload=<w> schedule=<s> bytes_per_launch=<n>`), or None."""
+def ncu_traffic_per_cell(kernel: str, workload: str, schedule: str):
+    """DRAM bytes per processed cell of a kernel launch from the committed ncu summaries (profiles/*.md
+    lines `traffic: kernel=<k> workload=<w> schedule=<s> bytes_per_launch=<n> cells_per_launch=<c>`),
+    or None."""
     import glob
     import re
-    pat = re.compile(r"traffic:\s*kernel=(\S+)\s+workload=(\S+)\s+schedule=(\S+)\s+bytes_per_launch=(\d+)")
+    pat = re.compile(r"traffic:\s*kernel=(\S+)\s+workload=(\S+)\s+schedule=(\S+)\s+bytes_per_launch=(\d+)"
+                     r"\s+cells_per_launch=(\d+)")
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(path) as f:
             for line in f:
                 m = pat.search(line)
                 if m and m.group(1) == kernel and m.group(2) == workload and m.group(3) == schedule:
-                    return int(m.group(4))
+                    return int(m.group(4)) / int(m.group(5)), m.group(2)
     return None
 
 
@@ -164,6 +175,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def config_of(w) -> dict:
+    """The workload as both arms name it (identical keys and values in the two JSON lines)."""
+    return {"workload": f"{w.name}: {w.description}", "grid": [w.nx, w.ny, w.nz], "neighborhood": w.neighborhood,
+            "boundary": w.boundary, "ca_max_steps": w.max_steps,
+            "mc": f"Q={w.Q} kT={w.kT} {w.mcs} MCS checkerboard, cooling mobility",
+            "step": "one job: the CA run to its stop rule, then the MC crystallisation of its basalt",
+            "inputs": "seeded synthetic terrain written as the reference's CSV heightmap"}
+
+
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
@@ -180,7 +200,7 @@ def mc_params(w, device):
 
 
 class L2Flush:
-    """Writes a buffer larger than L2 (126 MB) between jobs."""
+    """Writes a buffer larger than L2 (126 MB) between runs."""
 
     def __init__(self, device):
         import torch
@@ -192,41 +212,90 @@ class L2Flush:
         torch.cuda.synchronize()
 
 
-def run_job(w, sweep, device, flush, profile=False, mc=True):
-    """One job with resident inputs; returns device-timed figures."""
-    from volcano_ca_mc_b200 import capi
-    if profile:
-        os.environ["VCA_PROFILE_KERNELS"] = "1"
-    try:
-        ca = capi.LavaCA(ca_params(w, sweep, device))
+class Resident:
+    """One CA handle and one MC handle of a workload, kept for job after job (vca_ca_reset /
+    vca_mc_reconfigure between jobs: nothing is allocated per job).  run() does one job and returns
+    its device-timed figures: CA time from the handle's CUDA events around its step launches, MC time
+    likewise, launch counts and trial counters as deltas."""
+
+    def __init__(self, w, sweep, device, profile=False):
+        from volcano_ca_mc_b200 import capi
+        self.w, self.device = w, device
+        if profile:
+            os.environ["VCA_PROFILE_KERNELS"] = "1"
+        try:
+            self.ca = capi.LavaCA(ca_params(w, sweep, device))
+        finally:
+            os.environ.pop("VCA_PROFILE_KERNELS", None)
+        self.mc = None
+        self.fresh = True
+
+    def run(self, flush, mc=True):
+        w, ca = self.w, self.ca
+        if not self.fresh:
+            ca.reset()
+        self.fresh = False
         ca.apply_terrain(w.heights)
         ca.place_seeds(w.vent_cells())
-    finally:
-        os.environ.pop("VCA_PROFILE_KERNELS", None)
-    flush()
-    ca.run()
-    ca_ms, rules_ms, rules_n = ca.timing()
-    info = ca.info()
-    mc_out = None
-    if not profile and mc:
-        mc = capi.PottsMC(mc_params(w, device))
-        mc.set_domain_from_ca(ca)
-        mc.set_mobility_from_ca(ca, 0.05, True)
-        mc.initialize()
+        t0, _, _ = ca.timing()
+        l0 = ca.info().kernel_launches
         flush()
-        mc.sweep(w.mcs)
-        mi = mc.info()
-        mc_ms, _, _ = mc.timing()
-        mc_out = {"ms": mc_ms, "trials": mi.domain_cells * w.mcs, "attempts": mi.attempts,
-                  "launches": mi.kernel_launches, "domain_cells": mi.domain_cells}
-        mc.close()
-    out = {"ca_ms": ca_ms, "steps": info.steps, "stop": info.stop_reason, "tiles": info.tiles_processed,
-           "cells_per_tile": info.cells_per_tile, "tiles_total": info.tiles_total, "launches": info.kernel_launches,
-           "rules_ms": rules_ms, "rules_n": rules_n, "mc": mc_out}
-    if profile:
-        out["kernels"] = ca.kernel_times()
-    ca.close()
-    return out
+        ca.run()
+        t1, rules_ms, rules_n = ca.timing()
+        info = ca.info()
+        out = {"ca_ms": t1 - t0, "steps": info.steps, "stop": info.stop_reason, "launches": info.kernel_launches - l0,
+               "tiles": info.tiles_processed, "cells_per_tile": info.cells_per_tile, "tiles_total": info.tiles_total,
+               "rules_ms": rules_ms, "rules_n": rules_n, "mc": None}
+        if mc:
+            from volcano_ca_mc_b200 import capi
+            if self.mc is None:
+                self.mc = capi.PottsMC(mc_params(w, self.device))
+            else:
+                self.mc.reconfigure(mc_params(w, self.device))
+            m = self.mc
+            m.set_domain_from_ca(ca)
+            m.set_mobility_from_ca(ca, 0.05, True)
+            m.initialize()
+            a0, l0m = m.info().attempts, m.info().kernel_launches
+            m0, _, _ = m.timing()
+            flush()
+            m.sweep(w.mcs)
+            mi = m.info()
+            m1, _, _ = m.timing()
+            out["mc"] = {"ms": m1 - m0, "trials": mi.domain_cells * w.mcs, "attempts": mi.attempts - a0,
+                         "launches": mi.kernel_launches - l0m, "domain_cells": mi.domain_cells}
+        return out
+
+    def parity(self):
+        """SHA-256 of this job's ca_result.bin and mc_result.bin bytes (ResultWriter.cpp:155-167,
+        204-213) against the reference engine's run of the same config, when a golden exists."""
+        import numpy as np
+        w = self.w
+        gold = os.path.join(ROOT, "tests", "golden", f"{w.name}_large", "expect.json")
+        if not os.path.exists(gold):
+            return {"checked": False, "reason": f"no golden for {w.name}"}
+        with open(gold) as f:
+            exp = json.load(f)
+        h = hashlib.sha256(b"VOLC" + struct.pack("<Iiii", 2, w.nx, w.ny, w.nz))
+        for plane in self.ca.download():
+            h.update(memoryview(np.ascontiguousarray(plane)).cast("B"))
+        ca_ok = h.hexdigest() == exp["files"]["ca_result.bin"]
+        act, chg = self.ca.history()
+        hist_ok = act == exp["activeCells"] and chg == exp["changedCells"]
+        mc_ok = None
+        if self.mc is not None:
+            hm = hashlib.sha256(b"VMC1" + struct.pack("<iii", w.nx, w.ny, w.nz))
+            hm.update(memoryview(self.mc.crystals()).cast("B"))
+            mc_ok = hm.hexdigest() == exp["files"]["mc_result.bin"]
+        return {"checked": True, "golden": f"tests/golden/{w.name}_large (reference engine, same config)",
+                "ca_result.bin": "match" if ca_ok else "MISMATCH", "histories": "match" if hist_ok else "MISMATCH",
+                "mc_result.bin": None if mc_ok is None else ("match" if mc_ok else "MISMATCH"),
+                "ok": bool(ca_ok and hist_ok and mc_ok is not False)}
+
+    def close(self):
+        if self.mc is not None:
+            self.mc.close()
+        self.ca.close()
 
 
 class E2E:
@@ -263,55 +332,126 @@ class E2E:
         self.ca.close()
 
 
+def roofline(p, w, schedule, peak, peak_kind):
+    """Rules-kernel roofline of a profiled job p (per-launch CUDA events): 26 B per cell of the tiles
+    a launch processed, over its average duration."""
+    cells = p["tiles"] * p["cells_per_tile"] / max(1, p["rules_n"])
+    bytes_per_launch = BYTES_PER_CELL_UPDATE * cells
+    ach = bytes_per_launch / (p["rules_ms"] * 1e-3) / 1e9 if p["rules_ms"] > 0 else 0.0
+    traffic, src = None, None
+    t = ncu_traffic_per_cell("ca_rules_kernel", "c3q" if w.name == "c3" else w.name, schedule)
+    if t is not None:
+        traffic, src = int(round(t[0] * cells)), t[1]
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "traffic": traffic, "kernel": "ca_rules_kernel", "schedule": schedule,
+            "launch_ms": round(p["rules_ms"], 5), "bytes_per_launch": int(bytes_per_launch), "launches": p["rules_n"],
+            "peak_kind": peak_kind,
+            "traffic_ratio": round(traffic / bytes_per_launch, 3) if traffic else None,
+            "note": "26 B per cell of the processed tiles (13 B state read + 13 B written); frac of the "
+                    f"{peak_kind} HBM copy bandwidth; traffic = ncu dram bytes read+write per cell of this kernel on "
+                    f"the {src or '-'} case (profiles/), times the cells of one launch"}
+
+
+def workload_block(w, device, flush, peak, peak_kind, jobs=2):
+    """ACTIVE jobs, a DENSE job, a profiled DENSE job (rules-kernel roofline) and the parity of the
+    last ACTIVE job, for a sub-benchmark."""
+    from volcano_ca_mc_b200 import capi
+    r = Resident(w, capi.SWEEP_ACTIVE, device)
+    runs = [r.run(flush) for _ in range(jobs)]
+    par = r.parity()
+    r.close()
+    d = Resident(w, capi.SWEEP_DENSE, device)
+    dj = d.run(flush, mc=False)
+    d.close()
+    pd = Resident(w, capi.SWEEP_DENSE, device, profile=True)
+    pj = pd.run(flush, mc=False)
+    pj["kernels"] = pd.ca.kernel_times()
+    pd.close()
+    ca_ms = sum(j["ca_ms"] for j in runs)
+    mc_ms = sum(j["mc"]["ms"] for j in runs)
+    return {"workload": f"{w.name}: {w.description}", "grid": [w.nx, w.ny, w.nz], "ca_steps": runs[0]["steps"],
+            "value": w.cells * sum(j["steps"] for j in runs) / (ca_ms * 1e-3), "unit": "cell-updates/s",
+            "ms_per_job": ca_ms / len(runs),
+            "dense": {"value": w.cells * dj["steps"] / (dj["ca_ms"] * 1e-3), "ms_per_job": dj["ca_ms"]},
+            "roofline": roofline(pj, w, "dense", peak, peak_kind), "kernels_dense_ms": pj["kernels"],
+            "mc": {"attempts_per_s": sum(j["mc"]["attempts"] for j in runs) / (mc_ms * 1e-3),
+                   "trials_per_s": sum(j["mc"]["trials"] for j in runs) / (mc_ms * 1e-3), "ms_per_job": mc_ms / len(runs)},
+            "parity": par}
+
+
 def job_mixes(args, device):
-    """Many small independent jobs on one GPU through the job server (resident handles, footprint
-    admission): a batch of 96 jobs drawn from master seed 2026, run on `slots` workers and one at a
-    time, and a Poisson trace (20 jobs/s, master seed 77) replayed in real time the same two ways.
-    Every job's result hash must agree between the two runs."""
+    """Many small independent jobs on one GPU through the engine's job server (engine --serve: engine
+    configs in, resident handles admitted against the HBM budget, all running CA grids stepped in one
+    batch), against the one-at-a-time plain path on the same jobs (one worker, vca_ca_run per job):
+    a batch of 96 jobs drawn from master seed 2026 sent at once, a Poisson trace at 20 jobs/s (master
+    seed 77) replayed in real time, and a sweep of arrival rates.  Every job's result digests must
+    agree between the two modes."""
     from volcano_ca_mc_b200 import serve
 
     keys = ("slots", "jobs", "makespan_s", "jobs_per_s", "cell_updates_per_s", "p50_s", "p99_s", "mean_concurrency")
+    pick = lambda r: {k: (round(r[k], 4) if isinstance(r[k], float) else r[k]) for k in keys}
     out = {}
     if not args.no_batched:
         jobs = serve.make_mix(96, 2026)
-        many = serve.run(jobs, slots=args.slots, device=device)
-        one = serve.run(jobs, slots=1, device=device)
+        many = serve.run(jobs, slots=args.slots, batched=True, device=device)
+        one = serve.run(jobs, slots=1, batched=False, device=device)
+        streams = serve.run(jobs, slots=args.slots, batched=False, device=device)
         out["batched"] = {"mix": "96 jobs, master seed 2026: 2D sides 128-2048, 3D sides 64-256 (z = side/2), "
-                                 "200-600 CA steps, 20-100 MCS",
-                          "cells": sum(j.cells for j in jobs), **{k: many[k] for k in keys},
-                          "phase_ms_total": many["phase_ms_total"],
-                          "one_at_a_time": {k: one[k] for k in keys}, "mismatches": serve.compare(many, one)}
+                                 "200-600 CA steps, 20-100 MCS, sent at once",
+                          "cells": sum(j.cells for j in jobs), **pick(many), "server": many["server"],
+                          "one_at_a_time": pick(one), "independent_streams": pick(streams),
+                          "mismatches": serve.compare(many, one) + serve.compare(streams, one)}
     if not args.no_served:
         rate = 20.0
         trace = serve.make_mix(max(1, int(rate * args.serve_seconds)), 77, rate_hz=rate)
-        many = serve.run(trace, slots=args.slots, realtime=True, device=device)
-        one = serve.run(trace, slots=1, realtime=True, device=device)
+        many = serve.run(trace, slots=args.slots, batched=True, realtime=True, device=device)
+        one = serve.run(trace, slots=1, batched=False, realtime=True, device=device)
         out["served"] = {"trace": f"{len(trace)} jobs, Poisson arrivals at {rate:g} jobs/s, master seed 77, "
                                   "replayed in real time; latency = completion - arrival",
-                         **{k: many[k] for k in keys}, "phase_ms_total": many["phase_ms_total"],
-                         "one_at_a_time": {k: one[k] for k in keys}, "mismatches": serve.compare(many, one)}
+                         **pick(many), "server": many["server"], "one_at_a_time": pick(one),
+                         "mismatches": serve.compare(many, one)}
+        sweep = []
+        for lam in args.serve_rates:
+            n = max(1, int(lam * args.sweep_seconds))
+            tr = serve.make_mix(n, 1000 + int(lam), rate_hz=lam)
+            m = serve.run(tr, slots=args.slots, batched=True, realtime=True, device=device)
+            o = serve.run(tr, slots=1, batched=False, realtime=True, device=device)
+            sweep.append({"rate_hz": lam, "jobs": n, "batched": pick(m), "one_at_a_time": pick(o),
+                          "mismatches": serve.compare(m, o)})
+        out["served"]["rate_sweep"] = sweep
     return out
 
 
+def reference_job(w, threads, timeout, **over):
+    """The reference engine on the workload's config (with overrides); its times.json and stats.json."""
+    from oracle import oracle as O
+    over.setdefault("output.format", "none")  # no result files: a c3 job would write 4.5 GB
+    with tempfile.TemporaryDirectory() as d:
+        cfg = w.write(d, **over)
+        out = os.path.join(d, "out")
+        subprocess.run([O.REF_ENGINE, "--config", cfg, "--out", out, "--threads", str(threads)], check=True,
+                       capture_output=True, timeout=timeout)
+        with open(os.path.join(out, "times.json")) as f:
+            t = json.load(f)
+        with open(os.path.join(out, "stats.json")) as f:
+            st = json.load(f)
+    return t, st
+
+
 def cpu_baseline(w):
-    """The reference engine on one job of the workload, all host threads."""
+    """The reference engine on one full job of the workload, all host threads."""
     from oracle import oracle as O
     if not os.path.exists(O.REF_ENGINE):
         return None
     cores = os.cpu_count() or 1
-    with tempfile.TemporaryDirectory() as d:
-        cfg = w.write(d)
-        out = os.path.join(d, "out")
-        r = subprocess.run([O.REF_ENGINE, "--config", cfg, "--out", out, "--threads", str(cores)],
-                           capture_output=True, text=True, timeout=900)
-        if r.returncode != 0:
-            return None
-        t = json.load(open(os.path.join(out, "times.json")))
-        st = json.load(open(os.path.join(out, "stats.json")))
+    try:
+        t, st = reference_job(w, cores, 1800)
+    except Exception:
+        return None
     cu = w.cells * int(t["steps"])
     return {"value": cu / (t["caSim"] * 1e-3), "unit": "cell-updates/s", "cores": cores, "kind": "reference",
             "sample": f"one full {w.name} job ({t['steps']} CA steps, ca.sweep=front, caSim {t['caSim']:.0f} ms; "
-                      f"MC {w.mcs} MCS mcSim {t['mcSim']:.0f} ms)",
+                      f"MC {w.mcs} MCS, mcSim {t['mcSim']:.0f} ms; no result files written)",
             "mc_attempts_per_s": st["mc"]["attempts"] / (t["mcSim"] * 1e-3)}
 
 
@@ -322,13 +462,14 @@ def engine_cli(w):
     if not os.path.exists(capi.ENGINE_PATH):
         return None
     with tempfile.TemporaryDirectory() as d:
-        cfg = w.write(d)
+        cfg = w.write(d, **{"output.format": "none"})
         out = os.path.join(d, "out")
         r = subprocess.run([capi.ENGINE_PATH, "--config", cfg, "--out", out, "--timing-detail"], capture_output=True,
                            text=True, timeout=900)
         if r.returncode != 0:
             return {"error": r.stderr.strip()[-300:]}
-        t = json.load(open(os.path.join(out, "times.json")))
+        with open(os.path.join(out, "times.json")) as f:
+            t = json.load(f)
     keys = ("readConfig", "allocate", "terrain", "vents", "caSim", "save", "caStats", "mcInit", "mcSim", "mcStats",
             "mcSave", "total")
     return {"times_ms": {k: t[k] for k in keys if k in t}, "detail_ms": t.get("detail"), "steps": t.get("steps"),
@@ -346,23 +487,27 @@ def ours(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     w = workloads.get(args.workload)
     flush = L2Flush(local)
+    peak, peak_kind = measured_peaks()
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
+    job = Resident(w, capi.SWEEP_ACTIVE, local)
     for _ in range(args.warmup):
-        run_job(w, capi.SWEEP_ACTIVE, local, flush)
+        job.run(flush)
 
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
     wall0 = time.perf_counter()
-    jobs = [run_job(w, capi.SWEEP_ACTIVE, local, flush) for _ in range(args.steps)]
+    jobs = [job.run(flush) for _ in range(args.steps)]
     barrier()
     wall = time.perf_counter() - wall0
     clocks = sampler.stop()
+    parity = job.parity()  # the last timed job's bytes, after the timed region
+    job.close()
 
     ca_ms = sum(j["ca_ms"] for j in jobs)
     mc_ms = sum(j["mc"]["ms"] for j in jobs)
@@ -371,45 +516,19 @@ def ours(args):
     attempts = sum(j["mc"]["attempts"] for j in jobs)
     launches = sum(j["launches"] + j["mc"]["launches"] for j in jobs)
 
-    # dense schedule, same jobs (like-for-like with a full sweep)
-    dense = [run_job(w, capi.SWEEP_DENSE, local, flush) for _ in range(max(1, min(2, args.steps)))]
-    dense_ms = sum(j["ca_ms"] for j in dense)
-    dense_cu = sum(w.cells * j["steps"] for j in dense)
-
-    # rules-kernel roofline: per-launch CUDA events on the handle's stream
-    prof = run_job(w, capi.SWEEP_ACTIVE, local, flush, profile=True)
-    prof_dense = run_job(w, capi.SWEEP_DENSE, local, flush, profile=True)
-    peak, peak_kind = measured_peaks()
-
-    def roof(p, wl_name, schedule):
-        cells = p["tiles"] * p["cells_per_tile"] / max(1, p["rules_n"])
-        bytes_per_launch = BYTES_PER_CELL_UPDATE * cells
-        ach = bytes_per_launch / (p["rules_ms"] * 1e-3) / 1e9 if p["rules_ms"] > 0 else 0.0
-        return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
-                "traffic": ncu_traffic("ca_rules_kernel", wl_name, schedule), "kernel": "ca_rules_kernel",
-                "schedule": schedule, "launch_ms": round(p["rules_ms"], 5), "bytes_per_launch": int(bytes_per_launch),
-                "launches": p["rules_n"], "peak_kind": peak_kind,
-                "note": "26 B per cell of the processed tiles (13 B state read + 13 B written); frac of measured HBM copy "
-                        "bandwidth; traffic = ncu dram bytes read+write per launch (profiles/)"}
-
-    roof_active, roof_dense = roof(prof, w.name, "active"), roof(prof_dense, w.name, "dense")
-
-    # the full-size 3D workload: one ACTIVE job (CA + MC), one DENSE job, one DENSE job with per-kernel events
-    large = None
-    if not args.no_large:
-        wl3 = workloads.get("c3")
-        j3 = run_job(wl3, capi.SWEEP_ACTIVE, local, flush)
-        d3 = run_job(wl3, capi.SWEEP_DENSE, local, flush, mc=False)
-        p3 = run_job(wl3, capi.SWEEP_DENSE, local, flush, profile=True)
-        m3 = j3["mc"]
-        large = {"workload": f"{wl3.name}: {wl3.description}", "grid": [wl3.nx, wl3.ny, wl3.nz], "ca_steps": j3["steps"],
-                 "value": wl3.cells * j3["steps"] / (j3["ca_ms"] * 1e-3), "unit": "cell-updates/s",
-                 "ms_per_job": j3["ca_ms"],
-                 "dense": {"value": wl3.cells * d3["steps"] / (d3["ca_ms"] * 1e-3), "ms_per_job": d3["ca_ms"]},
-                 "roofline": roof(p3, wl3.name, "dense"), "kernels_dense_ms": p3["kernels"],
-                 "mc": {"attempts_per_s": m3["attempts"] / (m3["ms"] * 1e-3), "trials_per_s": m3["trials"] / (m3["ms"] * 1e-3),
-                        "ms_per_job": m3["ms"], "domain_cells": m3["domain_cells"],
-                        "hbm_frac_12B_per_trial": round(BYTES_PER_TRIAL * m3["trials"] / (m3["ms"] * 1e-3) / 1e9 / peak, 4)}}
+    # the same job with the DENSE schedule, and profiled jobs (per-kernel CUDA events) of both schedules
+    dense = Resident(w, capi.SWEEP_DENSE, local)
+    dj = dense.run(flush, mc=False)
+    dense.close()
+    profs = {}
+    for name, sweep in (("active", capi.SWEEP_ACTIVE), ("dense", capi.SWEEP_DENSE)):
+        pr = Resident(w, sweep, local, profile=True)
+        pj = pr.run(flush, mc=False)
+        pj["kernels"] = pr.ca.kernel_times()
+        pr.close()
+        profs[name] = pj
+    roof_dense = roofline(profs["dense"], w, "dense", peak, peak_kind)
+    roof_active = roofline(profs["active"], w, "active", peak, peak_kind)
 
     # e2e through the C ABI with host buffers, on a resident handle
     e2e = E2E(w, local)
@@ -420,14 +539,17 @@ def ours(args):
     e2e_h2d, e2e_d2h = e2e.bytes()
     e2e.close()
 
-    ca_ms, mc_ms, dense_ms, e2e_ms, wall_ms = max_over_ranks([ca_ms, mc_ms, dense_ms, e2e_ms, wall * 1e3],
+    ca_ms, mc_ms, dense_ms, e2e_ms, wall_ms = max_over_ranks([ca_ms, mc_ms, dj["ca_ms"], e2e_ms, wall * 1e3],
                                                              f"cuda:{local}", world)
+    extra = {}
     cpu = None
-    eng = None
-    mixes = {}
     if rank == 0 and world == 1:
-        mixes = job_mixes(args, local)
+        if not args.no_c2 and w.name != "c2":
+            extra["c2"] = workload_block(workloads.get("c2"), local, flush, peak, peak_kind)
+        extra.update(job_mixes(args, local))
         eng = engine_cli(w)
+        if eng is not None:
+            extra["engine_cli"] = eng
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(w)
     if world > 1:
@@ -441,22 +563,23 @@ def ours(args):
         "warmup": args.warmup, "ms_per_step": ca_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8+i32+f32 (integer rules, f32 temperatures)",
         "data": "synthetic (seeded Gaussian-cone terrain written as the reference's CSV heightmap)",
-        "config": {"workload": f"{w.name}: {w.description}", "grid": [w.nx, w.ny, w.nz],
-                   "neighborhood": w.neighborhood, "boundary": w.boundary, "ca_steps": jobs[0]["steps"],
-                   "mc": f"Q={w.Q} kT={w.kT} {w.mcs} MCS checkerboard, cooling mobility",
-                   "schedule": "ACTIVE (tile skipping, bit-identical to DENSE)",
-                   "l2": "flushed (256 MiB write) before every CA run and MC run, outside their device events",
-                   "step": "one job: CA run to the stop rule + MC crystallisation of its basalt",
-                   "parallelism": f"{world} independent replicas (weak scaling)"},
+        "config": config_of(w),
+        "method": {"schedule": "ACTIVE (tile skipping, bit-identical to DENSE)",
+                   "l2": "flushed (256 MiB write) before every CA run and MC run, outside their device events; "
+                         "the state (13 B x 2 buffers per cell) is far larger than L2",
+                   "timing": "CUDA events on the handle's stream around the step launches of each job",
+                   "parallelism": f"{world} independent replicas (weak scaling)", "ca_steps": jobs[0]["steps"]},
+        "parity": parity,
         "mc": {"metric": "MC attempts/s", "attempts_per_s": world * attempts / (mc_ms * 1e-3),
                "trials_per_s": world * trials / (mc_ms * 1e-3), "ms_per_job": mc_ms / args.steps,
                "domain_cells": jobs[0]["mc"]["domain_cells"],
                "hbm_frac_12B_per_trial": round(BYTES_PER_TRIAL * trials / (mc_ms * 1e-3) / 1e9 / peak, 4)},
-        "dense": {"value": world * dense_cu / (dense_ms * 1e-3), "ms_per_step": dense_ms / len(dense)},
+        "dense": {"value": world * w.cells * dj["steps"] / (dense_ms * 1e-3), "ms_per_step": dense_ms},
         "roofline": roof_dense,
         "roofline_active": roof_active,
-        "kernels_ms": {"active": prof["kernels"], "dense": prof_dense["kernels"]},
-        "active_tiles_frac": round(prof["tiles"] / max(1, prof["tiles_total"] * prof["steps"]), 4),
+        "kernels_ms": {"active": profs["active"]["kernels"], "dense": profs["dense"]["kernels"]},
+        "active_tiles_frac": round(profs["active"]["tiles"] / max(1, profs["active"]["tiles_total"] *
+                                                                   profs["active"]["steps"]), 4),
         "e2e": {"value": world * e2e_cu / (e2e_ms * 1e-3), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h, "ms_per_step": e2e_ms / len(e2e_runs),
                 "path": "vca_ca_reset + apply_terrain (host priority flood + upload) + place_seeds + run + download of "
@@ -465,11 +588,7 @@ def ours(args):
         "clocks": clocks,
         "wall_s_timed_loop": round(wall_ms / 1e3, 3),
     }
-    if large is not None:
-        line["large"] = large
-    line.update(mixes)
-    if eng is not None:
-        line["engine_cli"] = eng
+    line.update(extra)
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -490,33 +609,31 @@ def reference(args):
         return
     w = workloads.get(args.workload)
     cores = os.cpu_count() or 1
-    ca_ms, mc_ms, cu, att, runs = 0.0, 0.0, 0, 0, 0
-    with tempfile.TemporaryDirectory() as d:
-        cfg = w.write(d)
-        for i in range(args.warmup + args.steps):
-            out = os.path.join(d, f"out{i}")
-            subprocess.run([O.REF_ENGINE, "--config", cfg, "--out", out, "--threads", str(cores)], check=True,
-                           capture_output=True, timeout=900)
-            if i < args.warmup:
-                continue
-            t = json.load(open(os.path.join(out, "times.json")))
-            st = json.load(open(os.path.join(out, "stats.json")))
-            ca_ms += t["caSim"]
-            mc_ms += t["mcSim"]
-            cu += w.cells * int(t["steps"])
-            att += st["mc"]["attempts"]
-            runs += 1
+    sample_steps = min(w.max_steps, REF_SAMPLE_STEPS.get(w.name, w.max_steps))
+    ca_ms, cu, runs = 0.0, 0, 0
+    for i in range(args.warmup + args.steps):
+        t, _ = reference_job(w, cores, 1800, **{"ca.maxSteps": sample_steps, "mc.enabled": False})
+        if i < args.warmup:
+            continue
+        ca_ms += t["caSim"]
+        cu += w.cells * int(t["steps"])
+        runs += 1
     value = cu / (ca_ms * 1e-3)
+    if sample_steps < w.max_steps:
+        sample = (f"the first {sample_steps} of the job's {w.max_steps} CA steps (ca.maxSteps={sample_steps}, MC off), "
+                  "caSim from the engine's times.json; the reference engine cannot resume a run, and its front sweep "
+                  "costs less per step while the lava front is small, so this sample's rate is above the full job's")
+    else:
+        sample = f"the job's full CA run ({w.max_steps} steps at most, MC off), caSim from the engine's times.json"
     line = {"impl": "reference", "metric": "CA cell-updates/s", "value": value, "unit": "cell-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ca_ms / runs,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u8+i32+f32 (integer rules, f32 temperatures)", "data": "synthetic",
-            "config": {"workload": f"{w.name}: {w.description}", "grid": [w.nx, w.ny, w.nz],
-                       "engine": "oracle/_ref/engine (reference sources, g++ -O3 -fopenmp)",
+            "config": config_of(w),
+            "method": {"engine": "oracle/_ref/engine (reference sources, g++ -O3 -fopenmp)",
                        "ca.sweep": "front (the reference default, its fastest path)", "threads": cores},
-            "mc": {"metric": "MC attempts/s", "attempts_per_s": att / (mc_ms * 1e-3)},
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
-                             "sample": f"{runs} full {w.name} jobs, caSim from times.json"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -525,6 +642,8 @@ def profile_job(args):
     """One CA job of the workload, nothing else: a bounded case for ncu."""
     from volcano_ca_mc_b200 import capi, workloads
     w = workloads.get(args.workload)
+    if args.max_steps is not None:
+        w.max_steps = args.max_steps
     sweep = capi.SWEEP_DENSE if args.profile_job == "dense" else capi.SWEEP_ACTIVE
     ca = capi.LavaCA(ca_params(w, sweep, 0))
     ca.apply_terrain(w.heights)
@@ -533,7 +652,7 @@ def profile_job(args):
     info = ca.info()
     ms, _, _ = ca.timing()
     out = {"profile_job": args.profile_job, "workload": w.name, "steps": info.steps,
-           "tiles_processed": info.tiles_processed, "ms": ms}
+           "tiles_processed": info.tiles_processed, "cells_per_tile": info.cells_per_tile, "ms": ms}
     if args.profile_job == "mc":
         mc = capi.PottsMC(mc_params(w, 0))
         mc.set_domain_from_ca(ca)

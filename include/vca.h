@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define VCA_ABI_VERSION 1
+#define VCA_ABI_VERSION 2
 
 typedef enum {
     VCA_OK = 0,
@@ -55,6 +55,7 @@ enum { VCA_AIR = 0, VCA_ROCK = 1, VCA_LAVA = 2, VCA_BASALT = 3, VCA_VOID = 255 }
 
 typedef struct vca_ca vca_ca;
 typedef struct vca_mc vca_mc;
+typedef struct vca_ca_batch vca_ca_batch;
 
 /* ------------------------------------------------------------------------------------------
  * Lava cellular automaton -- replaces LavaCA<Storage> (engine/src/ca/LavaCA.hpp:80-271)
@@ -79,6 +80,13 @@ typedef struct {
     int ponding;               /* ca.ponding */
     int sweep;                 /* VCA_SWEEP_* */
     int device;                /* CUDA device ordinal */
+    /* Launch shape of the step kernels (no counterpart in the reference; results do not depend on
+     * it).  Tiles are 64 x tile_y x tile_z cells with tile_y * tile_z = 16: 4 x 4, 2 x 8, 8 x 2,
+     * 1 x 16 or 16 x 1 in 3D, 1 x 16 for a 2D x-z section, 16 x 1 for an x-y plane; 0 x 0 picks the
+     * default (4 x 4 in 3D).  rules_blocks_per_sm caps the resident blocks of the rules pass per SM
+     * (0: as many as fit).  volcano_ca_mc_b200/tuner.py picks them per grid shape. */
+    int tile_y, tile_z;
+    int rules_blocks_per_sm;
 } vca_ca_desc;
 
 /* Vent (engine/src/terrain/VentPlacer.hpp:26-31). */
@@ -148,6 +156,34 @@ vca_status vca_ca_get_spill(vca_ca* ca, int32_t* spill);
  * flows + 1 entries; entry 0 is set to 0.  The reference's maxReach is the largest hypot over the
  * cells rounded to 0.01, which equals sqrt(reach2[f]) rounded to 0.01. */
 vca_status vca_ca_flow_stats(vca_ca* ca, int flows, uint64_t* lava, uint64_t* basalt, uint64_t* reach2);
+/* ------------------------------------------------------------------------------------------
+ * z slabs of one grid over several GPUs, as the reference's strips (engine/src/parallel/Strip.hpp:1-25,
+ * engine/src/mpi/MpiSimulation.cpp): each GPU holds the layers it owns plus 17 halo layers below and
+ * 1 above (drop depths look 17 cells down), steps them, and after every step the caller copies the
+ * owned boundary layers into its neighbours' halo layers and sums the step's counts over all slabs
+ * for the stop rule (finishStep, LavaCA.hpp:1206-1229; LavaCA.hpp:1207-1211 sums the same three
+ * counters over the strips).  volcano_ca_mc_b200/slabs.py drives it over torch.distributed.
+ * ---------------------------------------------------------------------------------------- */
+/* Makes a new lava handle the slab whose layer 0 is global layer z_offset; it owns its layers
+ * [own_z0, own_z1).  Call before vca_ca_apply_terrain (which then takes the whole grid's nx*ny
+ * heights) and vca_ca_place_seeds (vents in this slab's local coordinates).  A slab steps with the
+ * DENSE schedule, hashes global indices, counts only its owned layers and never stops by itself
+ * except at max_steps. */
+vca_status vca_ca_set_slab(vca_ca* ca, int z_offset, int own_z0, int own_z1);
+/* One step of a slab; active / changed get this step's counts over the owned layers. */
+vca_status vca_ca_slab_step(vca_ca* ca, uint64_t* active, uint64_t* changed);
+/* Sets the stop state the caller decided from the counts of all slabs (VCA_STOP_*). */
+vca_status vca_ca_slab_stop(vca_ca* ca, int stop_reason);
+/* Device pointers of layer 0 of the current planes (the next step reads them) and the cells of one
+ * layer (rows are pitched: layer z starts at z * layer_cells); any pointer may be NULL. */
+vca_status vca_ca_layers(vca_ca* ca, void** type, void** flow_id, void** temp, void** solid_step,
+                         void** arrival_step, uint64_t* layer_cells);
+/* Halo messages between slabs: copies `types` type layers from local layer z0 and, when full >= 0,
+ * the flowId, temperature, solidStep and arrivalStep of local layer `full` between the current
+ * planes and a buffer of (types + 12 * (full >= 0)) * layer_cells bytes (device, pinned or pageable
+ * memory: the copy kind is inferred), in that order.  Unpacking writes the layers back. */
+vca_status vca_ca_pack_layers(vca_ca* ca, int z0, int types, int full, void* buf);
+vca_status vca_ca_unpack_layers(vca_ca* ca, int z0, int types, int full, const void* buf);
 /* Device time of the CA steps so far [ms] (CUDA events around the step launches) and the average
  * duration of one launch of the rules kernel [ms] over the last vca_ca_run / vca_ca_step calls. */
 vca_status vca_ca_timing(vca_ca* ca, double* total_ms, double* rules_kernel_ms, uint64_t* rules_launches);
@@ -157,6 +193,37 @@ vca_status vca_ca_timing(vca_ca* ca, double* total_ms, double* rules_kernel_ms, 
 vca_status vca_ca_kernel_times(vca_ca* ca, double* drop_ms, double* rules_ms, double* cand_ms, uint64_t* steps);
 /* ~LavaCA: frees the handle's device memory, stream and graph. */
 void vca_ca_destroy(vca_ca* ca);
+
+/* ------------------------------------------------------------------------------------------
+ * Batched stepping of many lava CA grids.  No counterpart in the reference: its batch runner
+ * (engine/src/app/Batch.cpp:186-246) starts one engine process per config, one after another, and
+ * each LavaCA::run (LavaCA.hpp:253-256) steps one grid.  A batch steps every member grid -- of any
+ * size, 2D or 3D, neighbourhood, boundary, seed or schedule -- with three launches per step for all
+ * of them together (each block of a launch works on one member), captured as a CUDA graph of 16
+ * steps.  Each member ends exactly as it would alone (same planes, histories and stop step).
+ * ---------------------------------------------------------------------------------------- */
+
+/* A batch of at most max_members grids on a device (max_members is also capped by the blocks of
+ * one launch, a few hundred). */
+vca_status vca_ca_batch_create(int device, int max_members, vca_ca_batch** out);
+/* Adds a handle whose state is set up (place_seeds or set_state done).  While it is a member, every
+ * call on the handle except vca_ca_destroy returns VCA_ERR_STATE; it leaves the batch when its stop
+ * rule holds (vca_ca_batch_advance reports it) or by vca_ca_batch_remove.  VCA_ERR_ARG when the
+ * batch is full or the handle lives on another device or in another batch. */
+vca_status vca_ca_batch_add(vca_ca_batch* b, vca_ca* member);
+/* Steps the members: launches up to max_graphs graphs of 16 steps, reading each graph's stop flags
+ * while the next one runs, and returns once some member has stopped (or all graphs are done, or no
+ * member is left).  The members that stopped leave the batch and are written to finished[0..*count)
+ * (at most capacity; the others stay queued for the next call); running gets the members still
+ * stepping.  A member that had stopped before it was added is reported by the next call. */
+vca_status vca_ca_batch_advance(vca_ca_batch* b, int max_graphs, vca_ca** finished, int capacity, int* count,
+                                int* running);
+/* Takes a member out of the batch now, whatever its state (its last step completes first). */
+vca_status vca_ca_batch_remove(vca_ca_batch* b, vca_ca* member);
+/* Launch counts: graphs launched, kernel launches issued, members now. */
+vca_status vca_ca_batch_info(vca_ca_batch* b, uint64_t* graphs, uint64_t* launches, int* members);
+/* Detaches every member (as by vca_ca_batch_remove) and frees the batch. */
+void vca_ca_batch_destroy(vca_ca_batch* b);
 
 /* ------------------------------------------------------------------------------------------
  * Potts Monte Carlo, checkerboard update -- replaces PottsMC (engine/src/mc/PottsMC.hpp:52-152)

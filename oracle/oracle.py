@@ -47,6 +47,8 @@ def lib() -> ctypes.CDLL:
         L.vo_hash_rand.argtypes = [u64, u64, u64, u64]
         L.vo_fill_depressions.argtypes = [p, i32, i32, i32, i32, p]
         L.vo_ca_step.argtypes = [p, i32, p, p, i32, p, p, p, p, p, p, p, p, p, p, p]
+        L.vo_ca_step_strip.argtypes = [p, i32, u64, i32, i32, p, p, i32, p, p, p, p, p, p, p, p, p, p, p]
+        L.vo_ca_step_strip.restype = None
         L.vo_ca_stop_after.restype = i32
         L.vo_ca_stop_after.argtypes = [p, i32, p]
         L.vo_mc_init.argtypes = [p, p, p]
@@ -167,6 +169,23 @@ def ca_step(p: CaParams, t: int, s: CaState, spill: np.ndarray | None, vents: np
                      _ptr(s.type), _ptr(s.flow), _ptr(s.temp), _ptr(s.solid), _ptr(s.arrival),
                      _ptr(out.type), _ptr(out.flow), _ptr(out.temp), _ptr(out.solid), _ptr(out.arrival),
                      _ptr(counts))
+    return out, counts
+
+
+def ca_step_strip(p: CaParams, t: int, gidx_base: int, own_z0: int, own_z1: int, s: CaState,
+                  spill_local: np.ndarray | None, vents: np.ndarray) -> tuple[CaState, np.ndarray]:
+    """One step of a strip of z layers (p.nz = the strip's layers): hashRand on global indices
+    (local + gidx_base), counts over layers [own_z0, own_z1); spill levels in local z."""
+    n = s.nx * s.ny * s.nz
+    out = CaState(s.nx, s.ny, s.nz, np.empty(n, np.uint8), np.empty(n, np.int32), np.empty(n, np.float32),
+                  np.empty(n, np.uint16), np.empty(n, np.uint16))
+    counts = np.zeros(3, np.uint64)
+    vt = np.ascontiguousarray(vents, np.int32)
+    lib().vo_ca_step_strip(ctypes.byref(p), t, gidx_base, own_z0, own_z1,
+                           None if spill_local is None else _ptr(spill_local), _ptr(vt), len(vt),
+                           _ptr(s.type), _ptr(s.flow), _ptr(s.temp), _ptr(s.solid), _ptr(s.arrival),
+                           _ptr(out.type), _ptr(out.flow), _ptr(out.temp), _ptr(out.solid), _ptr(out.arrival),
+                           _ptr(counts))
     return out, counts
 
 

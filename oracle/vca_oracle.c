@@ -410,10 +410,13 @@ static void ctx_init(ca_ctx* c, const vo_ca_params* p) {
         }
 }
 
-void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_t* vent_xyz, int vent_slots,
-                const uint8_t* type, const int32_t* flow, const float* temp, const uint16_t* solid,
-                const uint16_t* arrival, uint8_t* ntype, int32_t* nflow, float* ntemp, uint16_t* nsolid,
-                uint16_t* narrival, uint64_t counts[3]) {
+/* One step of a grid that may be a strip (z layers) of a taller grid: gidx_base is the global index
+ * of local cell 0 (hashRand takes global indices) and only layers [own_z0, own_z1) are counted
+ * (the reference's strips sum their counters, engine/src/ca/LavaCA.hpp:1207-1211). */
+static void ca_step_impl(const vo_ca_params* p, int t, uint64_t gidx_base, int own_z0, int own_z1, const int32_t* spill,
+                         const int32_t* vent_xyz, int vent_slots, const uint8_t* type, const int32_t* flow,
+                         const float* temp, const uint16_t* solid, const uint16_t* arrival, uint8_t* ntype,
+                         int32_t* nflow, float* ntemp, uint16_t* nsolid, uint16_t* narrival, uint64_t counts[3]) {
     ca_ctx c;
     ctx_init(&c, p);
     c.type = type;
@@ -446,6 +449,8 @@ void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_
         for (int y = 0; y < p->ny; ++y)
             for (int x = 0; x < p->nx; ++x) {
                 const int64_t i = gidx(p, x, y, z);
+                const uint64_t gi = (uint64_t)i + gidx_base;
+                const uint64_t own = (z >= own_z0 && z < own_z1) ? 1 : 0;
                 uint8_t ty = type[i];
                 int32_t f = flow[i];
                 float te = temp[i];
@@ -453,27 +458,27 @@ void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_
                 if (!p->classic) {
                     /* updateLava (LavaCA.hpp:1109-1161) */
                     if (ty == CELL_AIR) {
-                        gather(&c, x, y, z, prefix, (uint64_t)i, &vote);
+                        gather(&c, x, y, z, prefix, gi, &vote);
                         int became = 0;
                         if (vote.n > 0) {
-                            const int w = vote_winner(&vote, p->seed, tt, (uint64_t)i);
+                            const int w = vote_winner(&vote, p->seed, tt, gi);
                             const float wt = vote.max_temp[w];
                             if (wt >= p->solidus_temp) {
                                 ty = CELL_LAVA; f = vote.ids[w]; te = wt; so = 0; ar = stamp;
-                                ++active; ++changed;
+                                active += own; changed += own;
                                 became = 1;
                             }
                         }
-                        if (!became) ++air;
+                        if (!became) air += own;
                     } else if (ty == CELL_LAVA) {
                         const float before = te;
                         if (erupting && is_vent(vent_xyz, vent_slots, f, x, y, z)) te = p->erupt_temp;
                         else te -= p->cooling_ambient;
                         if (te < p->solidus_temp) {
-                            ty = CELL_BASALT; so = stamp; ++changed;
+                            ty = CELL_BASALT; so = stamp; changed += own;
                         } else {
-                            ++active;
-                            changed += (te != before) ? 1 : 0;
+                            active += own;
+                            changed += (te != before) ? own : 0;
                         }
                     }
                 } else {
@@ -482,7 +487,7 @@ void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_
                         vote.n = 0;
                         int variant = 0;
                         if (c.variants > 1)
-                            variant = (int)(vo_hash_salt(vo_hash_index(prefix, (uint64_t)i), SALT_NEIGHBORHOOD) % (uint64_t)c.variants);
+                            variant = (int)(vo_hash_salt(vo_hash_index(prefix, gi), SALT_NEIGHBORHOOD) % (uint64_t)c.variants);
                         for (int k = 0; k < c.nb_cnt[variant]; ++k) {
                             int sx = x + c.nb_off[variant][k][0], sy = y + c.nb_off[variant][k][1], sz = z + c.nb_off[variant][k][2];
                             if (!resolve(&c, &sx, &sy, &sz)) continue;
@@ -490,14 +495,14 @@ void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_
                             if (type[s] == CELL_LAVA) vote_add(&vote, flow[s], 0.0f);
                         }
                         if (vote.n > 0) {
-                            const int w = vote_winner(&vote, p->seed, tt, (uint64_t)i);
+                            const int w = vote_winner(&vote, p->seed, tt, gi);
                             ty = CELL_LAVA; f = vote.ids[w]; te = 0.0f; so = 0; ar = stamp;
-                            ++active; ++changed;
+                            active += own; changed += own;
                         } else {
-                            ++air;
+                            air += own;
                         }
                     } else if (ty == CELL_LAVA) {
-                        ++active;
+                        active += own;
                     }
                 }
                 ntype[i] = ty; nflow[i] = f; ntemp[i] = te; nsolid[i] = so; narrival[i] = ar;
@@ -506,6 +511,22 @@ void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_
     counts[0] = active;
     counts[1] = air;
     counts[2] = changed;
+}
+
+void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_t* vent_xyz, int vent_slots,
+                const uint8_t* type, const int32_t* flow, const float* temp, const uint16_t* solid,
+                const uint16_t* arrival, uint8_t* ntype, int32_t* nflow, float* ntemp, uint16_t* nsolid,
+                uint16_t* narrival, uint64_t counts[3]) {
+    ca_step_impl(p, t, 0, 0, p->nz, spill, vent_xyz, vent_slots, type, flow, temp, solid, arrival, ntype, nflow, ntemp,
+                 nsolid, narrival, counts);
+}
+
+void vo_ca_step_strip(const vo_ca_params* p, int t, uint64_t gidx_base, int own_z0, int own_z1, const int32_t* spill,
+                      const int32_t* vent_xyz, int vent_slots, const uint8_t* type, const int32_t* flow,
+                      const float* temp, const uint16_t* solid, const uint16_t* arrival, uint8_t* ntype,
+                      int32_t* nflow, float* ntemp, uint16_t* nsolid, uint16_t* narrival, uint64_t counts[3]) {
+    ca_step_impl(p, t, gidx_base, own_z0, own_z1, spill, vent_xyz, vent_slots, type, flow, temp, solid, arrival, ntype,
+                 nflow, ntemp, nsolid, narrival, counts);
 }
 
 int vo_ca_stop_after(const vo_ca_params* p, int steps_done, const uint64_t counts[3]) {

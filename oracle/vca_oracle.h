@@ -60,6 +60,13 @@ void vo_ca_step(const vo_ca_params* p, int t, const int32_t* spill, const int32_
 /* Stop rule after a step (LavaCA::finishStep, LavaCA.hpp:1206-1229): 0 running, 1 no lava,
  * 2 no air, 3 no change, 4 max steps. */
 int vo_ca_stop_after(const vo_ca_params* p, int steps_done, const uint64_t counts[3]);
+/* vo_ca_step on a strip of z layers of a taller grid (the reference's MPI strips,
+ * engine/src/parallel/Strip.hpp:1-25): global index of local cell 0 = gidx_base (for hashRand),
+ * counts over layers [own_z0, own_z1) only; spill levels shifted to local z by the caller. */
+void vo_ca_step_strip(const vo_ca_params* p, int t, uint64_t gidx_base, int own_z0, int own_z1, const int32_t* spill,
+                      const int32_t* vent_xyz, int vent_slots, const uint8_t* type, const int32_t* flow,
+                      const float* temp, const uint16_t* solid, const uint16_t* arrival, uint8_t* ntype,
+                      int32_t* nflow, float* ntemp, uint16_t* nsolid, uint16_t* narrival, uint64_t counts[3]);
 
 typedef struct {
     int nx, ny, nz;

@@ -213,3 +213,44 @@ def test_reconfigure_runs_other_spaces_exactly():
     with pytest.raises(capi.VcaError, match="does not fit"):
         ca.reconfigure(_params(128, 40, 32, "moore", "absorbing", 300, capi.SWEEP_ACTIVE, 1))
     ca.close()
+
+
+TILE_CASES = [
+    # nx, ny, nz, neighborhood, boundary, steps
+    (70, 22, 27, "moore", "periodic", 60),
+    (48, 20, 16, "pentagonal", "periodic", 50),     # periodic x with nx a multiple of 16 (wrapped columns by TMA)
+    (65, 17, 21, "von_neumann", "absorbing", 50),
+]
+
+
+@pytest.mark.parametrize("blocks", [0, 1])
+@pytest.mark.parametrize("tile", [(4, 4), (2, 8), (8, 2), (1, 16), (16, 1)], ids=lambda t: f"{t[0]}x{t[1]}")
+@pytest.mark.parametrize("case", TILE_CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}-{c[3]}-{c[4]}")
+def test_tile_shapes_match_oracle(case, tile, blocks):
+    """The launch shape (tile 64 x tile_y x tile_z, resident rules blocks per SM) changes nothing in
+    the results: every step equals the oracle's, in both schedules."""
+    nx, ny, nz, nb, bc, steps = case
+    seed = 300 + nx + ny
+    heights = C.terrain(nx, ny, nz, seed)
+    vents = C.pick_vents(heights, nx, ny, nz, 2, seed)
+    per = bc == "periodic"
+    spill = O.fill_depressions(heights, nx, ny, per, per)
+    for sweep in (capi.SWEEP_ACTIVE, capi.SWEEP_DENSE):
+        p = _params(nx, ny, nz, nb, bc, steps, sweep, seed)
+        p.tile_y, p.tile_z, p.rules_blocks_per_sm = tile[0], tile[1], blocks
+        op = C.oracle_params(p)
+        vt = O.vent_table(vents)
+        s = C.initial_state(nx, ny, nz, heights, vents, p.erupt_temp)
+        ca = capi.LavaCA(p)
+        ca.apply_terrain(heights)
+        ca.place_seeds(vents)
+        for t in range(steps):
+            s, counts = O.ca_step(op, t, s, spill, vt)
+            stop = O.ca_stop_after(op, t + 1, counts)
+            ca.step()
+            d = C.state_diff(s, ca.download())
+            assert d == "", f"step {t + 1}: {d}"
+            if stop:
+                break
+        ca.close()
+

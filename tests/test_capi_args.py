@@ -90,3 +90,14 @@ def test_noalloc_size_limit(dims, match):
     """The 2^28-cell limit of vca_mc_energy_noalloc is checked before the pointers, so null pointers
     show which side of the limit a size falls on without any grid or device."""
     _refused(lambda: capi.mc_energy_noalloc(0, *dims, 0), match)
+
+
+@pytest.mark.parametrize("dims,tile,match", [
+    ((40, 20, 20), (4, 2), "16 cells"),
+    ((40, 20, 20), (3, 5), "16 cells"),
+    ((64, 1, 40), (4, 4), "tile_y = 1"),
+    ((64, 40, 1), (4, 4), "tile_z = 1"),
+])
+def test_ca_tile_shape_refusals(dims, tile, match):
+    mode = "classic" if dims[2] == 1 else "lava"  # a 2D lava space is the x-z section
+    _refused(lambda: capi.LavaCA(capi.CaParams(*dims, mode=mode, tile_y=tile[0], tile_z=tile[1])), match)

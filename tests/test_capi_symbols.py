@@ -21,7 +21,7 @@ def test_library_loads_and_exports_all():
     L = capi.lib()
     for name in header_symbols():
         assert hasattr(L, name), name
-    assert L.vca_version().decode().startswith("vca 1 sm_100a")
+    assert L.vca_version().decode().startswith("vca 2 sm_100a")
 
 
 def test_errors_without_device_are_reported_not_raised_in_c():

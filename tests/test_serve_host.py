@@ -39,8 +39,41 @@ def test_poisson_arrivals():
     assert 18.0 < rate < 22.0
 
 
-def test_capacity_covers_every_job():
-    jobs = serve.make_mix(50, 2, share_3d=0.0, side_2d=(64, 512))
-    cap = serve.capacity(jobs)
-    for j in jobs:
-        assert j.nx <= cap.nx and j.ny <= cap.ny and j.nz <= cap.nz and j.max_steps <= cap.max_steps
+def test_job_configs_pass_the_engine_validation(tmp_path):
+    """Every job of a mix is an engine config in the reference's schema that the engine's own
+    validation accepts (engine --validate: the same parser as a run)."""
+    import json
+    import os
+    import subprocess
+
+    from volcano_ca_mc_b200 import capi
+    if not os.path.exists(capi.ENGINE_PATH):
+        import pytest
+        pytest.skip("engine not built")
+    for j in serve.make_mix(12, 13, side_2d=(64, 256), side_3d=(32, 64)):
+        path = tmp_path / f"job{j.job_id}.json"
+        path.write_text(json.dumps(j.config(str(tmp_path))))
+        r = subprocess.run([capi.ENGINE_PATH, "--validate", "--config", str(path)], capture_output=True, text=True)
+        out = json.loads(r.stdout)
+        assert r.returncode == 0 and out["ok"], out
+
+
+def test_server_answers_refused_requests_without_a_gpu():
+    """engine --serve answers each request line; refused configs come back as errors with the
+    reference's message texts, the rest of the stream goes on, the summary counts them (exit code 5)."""
+    import os
+
+    import pytest
+
+    from volcano_ca_mc_b200 import capi
+    if not os.path.exists(capi.ENGINE_PATH):
+        pytest.skip("engine not built")
+    srv = serve.EngineServer(slots=2, batched=False)
+    srv.submit({"id": "a", "json": {"space": {"nx": 0}}})
+    srv.submit({"id": "b", "json": {"neighborhood": "hexagonal", "space": {"nx": 40, "ny": 30, "nz": 20}}})
+    srv.submit({"id": "c", "config": "does/not/exist.json"})
+    assert srv.close() == 5
+    assert srv.answers["a"]["error"].startswith("Błąd konfiguracji: Parametr „space.nx” musi być z zakresu")
+    assert "hexagonal" in srv.answers["b"]["error"]
+    assert "Nie można otworzyć pliku konfiguracyjnego" in srv.answers["c"]["error"]
+    assert srv.summary["failed"] == 3 and srv.summary["jobs"] == 0

@@ -27,6 +27,10 @@ EXPORTS = [
     "vca_ca_create", "vca_ca_footprint", "vca_ca_reconfigure", "vca_ca_reset", "vca_ca_apply_terrain", "vca_ca_place_seeds", "vca_ca_step", "vca_ca_run",
     "vca_ca_get_info", "vca_ca_history", "vca_ca_download", "vca_ca_set_state", "vca_ca_get_spill", "vca_ca_flow_stats",
     "vca_ca_timing", "vca_ca_kernel_times", "vca_ca_destroy",
+    "vca_ca_batch_create", "vca_ca_batch_add", "vca_ca_batch_advance", "vca_ca_batch_remove", "vca_ca_batch_info",
+    "vca_ca_batch_destroy",
+    "vca_ca_set_slab", "vca_ca_slab_step", "vca_ca_slab_stop", "vca_ca_layers", "vca_ca_pack_layers",
+    "vca_ca_unpack_layers",
     "vca_mc_create", "vca_mc_footprint", "vca_mc_reconfigure", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
     "vca_mc_energy", "vca_mc_grains", "vca_mc_set_mobility_values", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
@@ -46,7 +50,8 @@ class CaDesc(ctypes.Structure):
                 ("erupt_temp", ctypes.c_float), ("solidus_temp", ctypes.c_float),
                 ("cooling_ambient", ctypes.c_float), ("cooling_lateral", ctypes.c_float),
                 ("cooling_fall", ctypes.c_float), ("ponding", ctypes.c_int), ("sweep", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("tile_y", ctypes.c_int), ("tile_z", ctypes.c_int),
+                ("rules_blocks_per_sm", ctypes.c_int)]
 
 
 class Vent(ctypes.Structure):
@@ -99,6 +104,11 @@ def lib() -> ctypes.CDLL:
         "vca_ca_history": [p, p, p, i32, p], "vca_ca_download": [p, p, p, p, p, p],
         "vca_ca_set_state": [p, p, p, p, p, p, p, p, i32, i32], "vca_ca_get_spill": [p, p], "vca_ca_flow_stats": [p, i32, p, p, p],
         "vca_ca_timing": [p, p, p, p], "vca_ca_kernel_times": [p, p, p, p, p],
+        "vca_ca_batch_create": [i32, i32, p], "vca_ca_batch_add": [p, p], "vca_ca_batch_advance": [p, i32, p, i32, p, p],
+        "vca_ca_batch_remove": [p, p], "vca_ca_batch_info": [p, p, p, p],
+        "vca_ca_set_slab": [p, i32, i32, i32], "vca_ca_slab_step": [p, p, p], "vca_ca_slab_stop": [p, i32],
+        "vca_ca_layers": [p, p, p, p, p, p, p], "vca_ca_pack_layers": [p, i32, i32, i32, p],
+        "vca_ca_unpack_layers": [p, i32, i32, i32, p],
         "vca_mc_create": [p, p], "vca_mc_footprint": [p, p], "vca_mc_reconfigure": [p, p], "vca_mc_set_domain": [p, p], "vca_mc_set_mobility": [p, p],
         "vca_mc_set_domain_from_ca": [p, p], "vca_mc_set_mobility_from_ca": [p, p, f64, i32],
         "vca_mc_mobility": [p, p], "vca_mc_initialize": [p], "vca_mc_sweep": [p, i32, p],
@@ -115,6 +125,8 @@ def lib() -> ctypes.CDLL:
     L.vca_ca_destroy.restype = None
     L.vca_mc_destroy.argtypes = [p]
     L.vca_mc_destroy.restype = None
+    L.vca_ca_batch_destroy.argtypes = [p]
+    L.vca_ca_batch_destroy.restype = None
     L.vca_last_error.restype = ctypes.c_char_p
     L.vca_version.restype = ctypes.c_char_p
     _lib = L
@@ -154,12 +166,15 @@ class CaParams:
     ponding: bool = True
     sweep: int = SWEEP_ACTIVE
     device: int = 0
+    tile_y: int = 0              # launch shape (0, 0: the default tile); results do not depend on it
+    tile_z: int = 0
+    rules_blocks_per_sm: int = 0
 
     def desc(self) -> CaDesc:
         return CaDesc(self.nx, self.ny, self.nz, NB[self.neighborhood], BC[self.boundary], MODE[self.mode],
                       self.seed, self.max_steps, self.eruption_steps, self.erupt_temp, self.solidus_temp,
                       self.cooling_ambient, self.cooling_lateral, self.cooling_fall, int(self.ponding),
-                      self.sweep, self.device)
+                      self.sweep, self.device, self.tile_y, self.tile_z, self.rules_blocks_per_sm)
 
 
 def ca_footprint(params: "CaParams") -> int:
@@ -266,6 +281,35 @@ class LavaCA:
         _check(lib().vca_ca_flow_stats(self.h, flows, _ptr(lava), _ptr(basalt), _ptr(reach2)), "vca_ca_flow_stats")
         return lava, basalt, reach2
 
+    def set_slab(self, z_offset: int, own_z0: int, own_z1: int) -> None:
+        """This handle is the slab of a taller grid whose layer 0 is global layer z_offset and which owns
+        its layers [own_z0, own_z1) (vca_ca_set_slab)."""
+        _check(lib().vca_ca_set_slab(self.h, z_offset, own_z0, own_z1), "vca_ca_set_slab")
+
+    def slab_step(self) -> tuple[int, int]:
+        """One step; the (active, changed) counts of the owned layers."""
+        a, c = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().vca_ca_slab_step(self.h, ctypes.byref(a), ctypes.byref(c)), "vca_ca_slab_step")
+        return a.value, c.value
+
+    def slab_stop(self, stop_reason: int) -> None:
+        _check(lib().vca_ca_slab_stop(self.h, stop_reason), "vca_ca_slab_stop")
+
+    def layers(self) -> tuple[list[int], int]:
+        """Device addresses of layer 0 of the current type, flowId, temp, solidStep and arrivalStep planes,
+        and the cells of one (pitched) layer."""
+        ptrs = [ctypes.c_void_p() for _ in range(5)]
+        n = ctypes.c_uint64()
+        _check(lib().vca_ca_layers(self.h, *[ctypes.byref(p) for p in ptrs], ctypes.byref(n)), "vca_ca_layers")
+        return [p.value for p in ptrs], n.value
+
+    def pack_layers(self, z0: int, types: int, full: int, buf_ptr: int) -> None:
+        """Halo message into the buffer at address buf_ptr (vca_ca_pack_layers)."""
+        _check(lib().vca_ca_pack_layers(self.h, z0, types, full, ctypes.c_void_p(buf_ptr)), "vca_ca_pack_layers")
+
+    def unpack_layers(self, z0: int, types: int, full: int, buf_ptr: int) -> None:
+        _check(lib().vca_ca_unpack_layers(self.h, z0, types, full, ctypes.c_void_p(buf_ptr)), "vca_ca_unpack_layers")
+
     def timing(self) -> tuple[float, float, int]:
         tot, ker, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
         _check(lib().vca_ca_timing(self.h, ctypes.byref(tot), ctypes.byref(ker), ctypes.byref(n)), "vca_ca_timing")
@@ -277,6 +321,62 @@ class LavaCA:
         _check(lib().vca_ca_kernel_times(self.h, ctypes.byref(d), ctypes.byref(r), ctypes.byref(c), ctypes.byref(n)),
                "vca_ca_kernel_times")
         return {"drop_ms": d.value, "rules_ms": r.value, "cand_ms": c.value, "steps": n.value}
+
+
+class CaBatch:
+    """Python face of vca_ca_batch_*: many LavaCA handles stepped by shared launches.  Members are
+    added once their state is set up; advance() steps them and returns the ones whose stop rule held
+    (they have left the batch and take every LavaCA call again)."""
+
+    def __init__(self, device: int = 0, max_members: int = 256):
+        h = ctypes.c_void_p()
+        _check(lib().vca_ca_batch_create(device, max_members, ctypes.byref(h)), "vca_ca_batch_create")
+        self.h = h
+        self.members: dict[int, "LavaCA"] = {}
+
+    def add(self, ca: "LavaCA") -> None:
+        _check(lib().vca_ca_batch_add(self.h, ca.h), "vca_ca_batch_add")
+        self.members[ca.h.value] = ca
+
+    def advance(self, max_graphs: int = 1 << 30) -> tuple[list["LavaCA"], int]:
+        """Steps until some member stops (or max_graphs graphs of 16 steps); returns the members that
+        stopped and the number still running."""
+        cap = max(1, len(self.members))
+        out = (ctypes.c_void_p * cap)()
+        n, running = ctypes.c_int(), ctypes.c_int()
+        _check(lib().vca_ca_batch_advance(self.h, max_graphs, out, cap, ctypes.byref(n), ctypes.byref(running)),
+               "vca_ca_batch_advance")
+        done = [self.members.pop(out[i]) for i in range(n.value)]
+        return done, running.value
+
+    def run(self) -> list["LavaCA"]:
+        """Steps until every member has stopped; returns them in the order they stopped."""
+        order = []
+        while self.members:
+            done, _ = self.advance()
+            order += done
+        return order
+
+    def remove(self, ca: "LavaCA") -> None:
+        _check(lib().vca_ca_batch_remove(self.h, ca.h), "vca_ca_batch_remove")
+        self.members.pop(ca.h.value, None)
+
+    def info(self) -> dict:
+        g, l, m = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()
+        _check(lib().vca_ca_batch_info(self.h, ctypes.byref(g), ctypes.byref(l), ctypes.byref(m)), "vca_ca_batch_info")
+        return {"graphs": g.value, "launches": l.value, "members": m.value}
+
+    def close(self) -> None:
+        if self.h:
+            lib().vca_ca_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+            self.members.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

@@ -45,8 +45,6 @@ constexpr int kTileX = 64;
 constexpr int kMaxDrop = 16;        // LavaCA::kMaxDrop (LavaCA.hpp:1293)
 constexpr int kSmemRowBytes = 96;   // 16 pad (left frame byte at 15) + 64 cells + right frame byte + pad
 constexpr int kRowOff = 16;         // first cell of a staged row (16-byte aligned for cp.async)
-constexpr int kMaxHaloRows = 36;    // (TY + 2) * (TZ + 2) for TY = TZ = 4; 18 for the 2D tiles
-constexpr int kMaxDropRows = 24;    // (TY + 2) * TZ: the drop-depth rows at the tile's own levels
 
 // ------------------------------------------------------------------------------------------
 // Addressing with the reference's frame semantics: a coordinate one step outside the interior is
@@ -289,13 +287,14 @@ __device__ void drop_rescan18(const CaKernelArgs& k, const uint8_t* T, int x, in
 }
 
 // Rescans the columns above last step's type changes (or every column when forced or when the
-// change list overflowed), and clears the change list this step's rules will fill.
-__global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force_full) {
+// change list overflowed), and clears the change list this step's rules will fill.  Block `bid` of
+// `nblk` blocks working on this grid.
+__device__ __forceinline__ void drop_body(const CaKernelArgs& k, int force_full, uint32_t bid, uint32_t nblk) {
     CaCtrl* ctrl = k.ctrl;
     if (!force_full && (ctrl->stop || ctrl->error)) return;
     const uint32_t t = ctrl->steps;
     const int cur = t & 1, nxt = cur ^ 1;
-    if (!force_full && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!force_full && bid == 0 && threadIdx.x == 0) {
         ctrl->chg_count[nxt] = 0;   // filled by this step's rules
         ctrl->list_count[nxt] = 0;  // tiles of the next step, scheduled by this step's rules
     }
@@ -303,9 +302,10 @@ __global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force
     const CaGeom& g = k.g;
     const uint8_t* T = k.type[cur];
     const unsigned n = force_full ? 0u : ctrl->chg_count[cur];
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (force_full || n > k.chg_cap) {
+    const uint64_t stride = (uint64_t)nblk * blockDim.x;
+    const uint64_t gtid = bid * (uint64_t)blockDim.x + threadIdx.x;
+    // a slab's halo layers change by copies from its neighbours, outside the change list: rescan all
+    if (force_full || n > k.chg_cap || k.slab) {
         const uint64_t cols = (uint64_t)g.nx * g.ny;
         for (uint64_t c = gtid; c < cols; c += stride) drop_scan(k, T, (int)(c % g.nx), (int)(c / g.nx), 0, g.nz);
         return;
@@ -318,6 +318,9 @@ __global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force
         const int z = (int)(r / (uint32_t)g.ny);
         drop_rescan18(k, T, x, y, z);
     }
+}
+__global__ void ca_drop_kernel(const __grid_constant__ CaKernelArgs k, int force_full) {
+    drop_body(k, force_full, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -626,34 +629,49 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 // schedule) cannot change: thread 0 alone moves its state boxes from the current to the next buffer.
 // Tiles at the grid edge get their frame cells (VOID, or the periodic copy) patched after the load.
 // ------------------------------------------------------------------------------------------
-constexpr int kSpillCols = kTileX * 4;  // columns of a tile with nz > 1 (TY <= 4)
+// Shared-memory room of the rules pass for a family of tile shapes 64 x TY x TZ (TY * TZ = 16):
+// staged halo rows (HY * HZ, HY = TY + 2 and HZ = TZ + 2 on axes of size > 1), drop-depth rows
+// (HY * TZ) and spill columns (64 * TY).  Halo rows are a multiple of 4, so that the drop rows after
+// them start 128-byte aligned.
+template <int HALO, int DROP, int TYMAX>
+struct RulesShape {
+    static constexpr int halo = HALO, drop = DROP, ty = TYMAX;
+    static_assert(HALO % 4 == 0 && HALO * 4 <= kThreads && DROP * 4 <= kThreads, "frame patch threads");
+};
+using ShapeA = RulesShape<36, 24, 4>;   // 4 x 4 in 3D; 1 x 16 (x-z) and 16 x 1 (x-y) in 2D
+using ShapeB = RulesShape<40, 32, 8>;   // 2 x 8 and 8 x 2 in 3D
+using ShapeC = RulesShape<56, 48, 16>;  // 1 x 16 and 16 x 1 in 3D
 // a wrapped-x column buffer: 16 bytes per halo row (or drop row), each buffer 128-byte aligned
-constexpr int kXSideBytes = (kMaxHaloRows * 16 + 127) / 128 * 128;
-constexpr int kXSideDropBytes = (kMaxDropRows * 16 + 127) / 128 * 128;
+constexpr int xside_bytes(int rows) { return (rows * 16 + 127) / 128 * 128; }
 
+template <class S>
 struct __align__(128) RulesSlot {
     int32_t flow[kTileCells];
     float temp[kTileCells];
     uint16_t solid[kTileCells];
     uint16_t arrival[kTileCells];
     uint8_t own_type[kTileCells];
-    uint8_t type[kMaxHaloRows * kSmemRowBytes];
-    int8_t drop[kMaxDropRows * kSmemRowBytes];
-    int32_t spill[kSpillCols];
+    uint8_t type[S::halo * kSmemRowBytes];
+    int8_t drop[S::drop * kSmemRowBytes];
+    int32_t spill[kTileX * S::ty];
     // wrapped x columns (periodic x): [0] the 16 cells ending at x = nx - 1 (left frame, byte 15 of
     // each row), [1] the 16 cells from x = 0 (right frame or padded-row copy, byte 0)
-    __align__(128) uint8_t xside[2][kXSideBytes];
-    __align__(128) int8_t xside_drop[2][kXSideDropBytes];
+    __align__(128) uint8_t xside[2][xside_bytes(S::halo)];
+    __align__(128) int8_t xside_drop[2][xside_bytes(S::drop)];
 };
-static_assert(offsetof(RulesSlot, temp) == offsetof(RulesSlot, flow) + 4 * kTileCells &&
-                  offsetof(RulesSlot, arrival) == offsetof(RulesSlot, solid) + 2 * kTileCells,
-              "the planes of a pair follow each other in a slot, as a 4D box lands them");
-static_assert(offsetof(RulesSlot, type) % 128 == 0 && offsetof(RulesSlot, drop) % 128 == 0 &&
-                  offsetof(RulesSlot, own_type) % 128 == 0 && offsetof(RulesSlot, solid) % 128 == 0 &&
-                  offsetof(RulesSlot, xside) % 128 == 0 && offsetof(RulesSlot, xside_drop) % 128 == 0 &&
-                  kXSideBytes % 128 == 0 && kXSideDropBytes % 128 == 0,
-              "TMA destinations are 128-byte aligned");
-constexpr size_t kRulesDynSmem = 2 * sizeof(RulesSlot) + 128;
+template <class S>
+constexpr bool slot_layout_ok() {
+    using T = RulesSlot<S>;
+    return offsetof(T, temp) == offsetof(T, flow) + 4 * kTileCells && offsetof(T, arrival) == offsetof(T, solid) + 2 * kTileCells &&
+           offsetof(T, type) % 128 == 0 && offsetof(T, drop) % 128 == 0 && offsetof(T, own_type) % 128 == 0 &&
+           offsetof(T, solid) % 128 == 0 && offsetof(T, xside) % 128 == 0 && offsetof(T, xside_drop) % 128 == 0;
+}
+static_assert(slot_layout_ok<ShapeA>() && slot_layout_ok<ShapeB>() && slot_layout_ok<ShapeC>(),
+              "the planes of a pair follow each other in a slot, as a 4D box lands them; TMA destinations are "
+              "128-byte aligned");
+template <class S>
+constexpr size_t rules_dyn_smem() { return 2 * sizeof(RulesSlot<S>) + 128; }
+constexpr size_t kRulesDynSmem = rules_dyn_smem<ShapeA>();
 
 // Bytes x-1 .. x+2 / x .. x+3 / x+1 .. x+4 of a staged row around the 4 cells at p (p = row start +
 // kRowOff + 4 * xq; the frame bytes sit at kRowOff - 1 and kRowOff + 64).
@@ -665,7 +683,9 @@ __device__ __forceinline__ uint32_t win_right(const uint8_t* p) {
     return __funnelshift_r(*reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 4), 8);
 }
 
-__global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaKernelArgs k) {
+template <class S>
+__device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKernelArgs& k, uint32_t bid, uint32_t nblk) {
+    using RulesSlot = vca::RulesSlot<S>;
     extern __shared__ __align__(128) uint8_t s_dyn[];
     // the slots start on a 128-byte boundary (TMA destinations); the launch adds 128 bytes of slack
     RulesSlot* slots = reinterpret_cast<RulesSlot*>(s_dyn + ((128u - (smem_u32(s_dyn) & 127u)) & 127u));
@@ -749,42 +769,44 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             // periodic x: an x-edge tile also loads the column that holds its wrapped frame cells
             const bool wl = rules && xwrap && x0 == 0, wr = rules && xwrap && x0 + kTileX >= g.nx;
             mbar_arrive_expect_tx(&s_bar[s], (rules ? tx_rules : tx_copy) + (wl ? tx_xside : 0u) + (wr ? tx_xside : 0u));
-            tma_load_4d(sl.flow, &k.tm.ft[cur], x0, y0, z0, &s_bar[s]);   // flowId and temperature
-            tma_load_4d(sl.solid, &k.tm.sa[cur], x0, y0, z0, &s_bar[s]);  // solidStep and arrivalStep
+            tma_load_4d(sl.flow, &tm.ft[cur], x0, y0, z0, &s_bar[s]);   // flowId and temperature
+            tma_load_4d(sl.solid, &tm.sa[cur], x0, y0, z0, &s_bar[s]);  // solidStep and arrivalStep
             if (rules) {
-                tma_load_3d(sl.type, &k.tm.halo_type[cur], x0 - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
-                if (lava_mode) tma_load_3d(sl.drop, &k.tm.drop, x0 - 16, y0 - hy_on, z0, &s_bar[s]);
+                tma_load_3d(sl.type, &tm.halo_type[cur], x0 - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
+                if (lava_mode) tma_load_3d(sl.drop, &tm.drop, x0 - 16, y0 - hy_on, z0, &s_bar[s]);
                 if (wl) {
-                    tma_load_3d(sl.xside[0], &k.tm.xside_type[cur], g.nx - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
-                    if (lava_mode) tma_load_3d(sl.xside_drop[0], &k.tm.xside_drop, g.nx - 16, y0 - hy_on, z0, &s_bar[s]);
+                    tma_load_3d(sl.xside[0], &tm.xside_type[cur], g.nx - 16, y0 - hy_on, z0 - hz_on, &s_bar[s]);
+                    if (lava_mode) tma_load_3d(sl.xside_drop[0], &tm.xside_drop, g.nx - 16, y0 - hy_on, z0, &s_bar[s]);
                 }
                 if (wr) {
-                    tma_load_3d(sl.xside[1], &k.tm.xside_type[cur], 0, y0 - hy_on, z0 - hz_on, &s_bar[s]);
-                    if (lava_mode) tma_load_3d(sl.xside_drop[1], &k.tm.xside_drop, 0, y0 - hy_on, z0, &s_bar[s]);
+                    tma_load_3d(sl.xside[1], &tm.xside_type[cur], 0, y0 - hy_on, z0 - hz_on, &s_bar[s]);
+                    if (lava_mode) tma_load_3d(sl.xside_drop[1], &tm.xside_drop, 0, y0 - hy_on, z0, &s_bar[s]);
                 }
             } else {
-                tma_load_3d(sl.own_type, &k.tm.own_type[cur], x0, y0, z0, &s_bar[s]);
+                tma_load_3d(sl.own_type, &tm.own_type[cur], x0, y0, z0, &s_bar[s]);
             }
         }
-        if (rules && stage_spill && tid < kTileX * g.TY) {
-            const int xx = x0 + (tid & (kTileX - 1)), yy = y0 + tid / kTileX;
-            if (xx < g.nx && yy < g.ny)
-                cp_async4(&sl.spill[tid], k.spill + xx + (int64_t)g.nx * yy);
-            else
-                sl.spill[tid] = 0;
+        if (rules && stage_spill) {
+            for (int c = tid; c < kTileX * g.TY; c += kThreads) {
+                const int xx = x0 + (c & (kTileX - 1)), yy = y0 + c / kTileX;
+                if (xx < g.nx && yy < g.ny)
+                    cp_async4(&sl.spill[c], k.spill + xx + (int64_t)g.nx * yy);
+                else
+                    sl.spill[c] = 0;
+            }
         }
     };
     auto store_tile = [&](int s, int x0, int y0, int z0) {  // thread 0
         RulesSlot& sl = slots[s];
-        tma_store_3d(&k.tm.own_type[nxt], x0, y0, z0, sl.own_type);
-        tma_store_4d(&k.tm.ft[nxt], x0, y0, z0, sl.flow);
-        tma_store_4d(&k.tm.sa[nxt], x0, y0, z0, sl.solid);
+        tma_store_3d(&tm.own_type[nxt], x0, y0, z0, sl.own_type);
+        tma_store_4d(&tm.ft[nxt], x0, y0, z0, sl.flow);
+        tma_store_4d(&tm.sa[nxt], x0, y0, z0, sl.solid);
         bulk_commit();
     };
 
     // control pipeline: tile ids of the next two iterations, the mark of the next
-    const uint64_t G = gridDim.x;
-    uint64_t i = blockIdx.x;
+    const uint64_t G = nblk;
+    uint64_t i = bid;
     uint32_t tile_a = 0, mark_a = 0, vent_a = 0;  // iteration it
     uint32_t tile_b = 0, mark_b = 0, vent_b = 0;  // it + 1
     uint32_t tile_c = 0;                          // it + 2
@@ -879,7 +901,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                 }
                 if (drop_wrap) {
                     // drop depths are read only where the staged type is AIR: only periodic copies matter
-                    const int c = tid - 144;
+                    const int c = tid - (kThreads - 4 * drop_rows);  // the last 4 * drop_rows threads
                     if (c >= 0 && c < drop_rows * 4) {
                         const int r = c >> 2, ch = c & 3;
                         int yy = y0 - hy_on + r % HY;
@@ -889,7 +911,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                             drow_v = *reinterpret_cast<const uint4*>(k.drop + pidx(g, x0 + 16 * ch, yy, zz));
                         }
                     }
-                    const int f = tid - 128;
+                    const int f = tid - (kThreads - 3 * drop_rows);  // the last 3 * drop_rows threads
                     if (f >= 0 && f < drop_rows * 3) {
                         const int r = f / 3, which = f % 3;
                         int xx = which == 0 ? x0 - 1 : (which == 1 ? x0 + kTileX : xpad);
@@ -917,6 +939,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
 
             const int y = y0 + ly, z = z0 + lz, x = x0 + 4 * xq;
             const bool valid = y < g.ny && z < g.nz;
+            const unsigned own = (z >= k.own_z0 && z < k.own_z1) ? 1u : 0u;  // counted in the step's sums
             const int64_t p = pidx(g, valid ? x : 0, valid ? y : 0, valid ? z : 0);
             const int hr = hr_of(ly, lz, hy_on, hz_on, HY);
             const uint8_t* rowp = sl.type + hr * kSmemRowBytes + kRowOff + 4 * xq;
@@ -1013,7 +1036,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
             }
             if (lava_m) {
                 if (k.classic) {
-                    my_active += __popc(lava_m) >> 3;
+                    my_active += own * (__popc(lava_m) >> 3);
                     any_lava = true;
                 } else {
                     float te[4] = {t4.x, t4.y, t4.z, t4.w};
@@ -1034,14 +1057,14 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
                             const uint32_t half = (j & 1) * 16;
                             wout = (wout & ~(0xFFu << (8 * j))) | ((uint32_t)kBasalt << (8 * j));
                             so[j >> 1] = (so[j >> 1] & ~(0xFFFFu << half)) | (stamp << half);
-                            ++my_changed;
+                            my_changed += own;
                             bas[nbas++] = g0 + j;
                             any_changed = true;
                         } else {
-                            ++my_active;
+                            my_active += own;
                             any_lava = true;
                             if (nt != before) {
-                                ++my_changed;
+                                my_changed += own;
                                 any_changed = true;
                             }
                         }
@@ -1123,6 +1146,11 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
         if (tiles_done) atomicAdd(&ctrl->acc_tiles, (unsigned long long)tiles_done);
     }
 }
+template <class S>
+__global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaTensorMaps tm,
+                                                               const __grid_constant__ CaKernelArgs k) {
+    rules_body<S>(tm, k, blockIdx.x, gridDim.x);
+}
 
 // ------------------------------------------------------------------------------------------
 // Rules, candidate pass: resolves the listed AIR cells (gatherLavaCandidates / vote / solidus,
@@ -1131,7 +1159,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_cons
 // finishes the step (finishStep, LavaCA.hpp:1206-1229).
 // ------------------------------------------------------------------------------------------
 constexpr int kCandThreads = 128;
-__global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
+__device__ __forceinline__ void cand_body(const CaKernelArgs& k, uint32_t bid, uint32_t nblk) {
     __shared__ unsigned long long s_red[kCandThreads / 32];
     __shared__ bool s_last;
     CaCtrl* ctrl = k.ctrl;
@@ -1147,13 +1175,13 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
     const unsigned n = ctrl->cand_count;
     // the blocks that hold listed cells take part (at least one, which finishes the step); the others
     // leave at once, so a short list costs a few blocks instead of the whole grid
-    const unsigned parts = max(1u, min(gridDim.x, (n + kCandThreads - 1) / kCandThreads));
-    if (blockIdx.x >= parts) return;
+    const unsigned parts = max(1u, min(nblk, (n + kCandThreads - 1) / kCandThreads));
+    if (bid >= parts) return;
     const int lane = threadIdx.x & 31;
     unsigned born = 0;
-    const uint64_t stride = (uint64_t)gridDim.x * kCandThreads;
+    const uint64_t stride = (uint64_t)nblk * kCandThreads;
     // warp-uniform loop (the appends below use full-warp collectives)
-    for (uint64_t base = blockIdx.x * (uint64_t)kCandThreads; base < n; base += stride) {
+    for (uint64_t base = bid * (uint64_t)kCandThreads; base < n; base += stride) {
         const uint64_t j = base + threadIdx.x;
         bool gained = false;
         uint32_t gi = 0, tile = 0;
@@ -1165,7 +1193,7 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
             const int z = (int)(r / (uint32_t)g.ny);
             int32_t nf;
             float nt;
-            if (air_gains_lava(k, T, F, Te, x, y, z, prefix, gi, &nf, &nt)) {
+            if (air_gains_lava(k, T, F, Te, x, y, z, prefix, gi + k.gidx_base, &nf, &nt)) {
                 const int64_t p = pidx(g, x, y, z);
                 k.type[nxt][p] = kLava;
                 k.flow[nxt][p] = nf;
@@ -1173,7 +1201,7 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
                 k.solid[nxt][p] = 0;
                 k.arrival[nxt][p] = (uint16_t)stamp;
                 gained = true;
-                ++born;
+                born += (z >= k.own_z0 && z < k.own_z1) ? 1u : 0u;
                 tile = (uint32_t)(x / kTileX) +
                        (uint32_t)g.tiles_x * ((uint32_t)(y / g.TY) + (uint32_t)g.tiles_y * (uint32_t)(z / g.TZ));
             }
@@ -1222,13 +1250,18 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_c
         k.hist_changed[t] = changed;
         const uint32_t steps = t + 1;
         int stop = VCA_STOP_RUNNING;
-        if (!ctrl->classic && active == 0) stop = VCA_STOP_NO_LAVA;
+        if (k.slab) {
+            // the stop rule needs the sums over all slabs: the caller decides (vca_ca_slab_stop)
+        } else if (!ctrl->classic && active == 0) stop = VCA_STOP_NO_LAVA;
         else if (ctrl->classic && air == 0) stop = VCA_STOP_NO_AIR;
         else if (changed == 0 && !ctrl->random_nb) stop = VCA_STOP_NO_CHANGE;
         else if ((int)steps >= ctrl->max_steps) stop = VCA_STOP_MAX_STEPS;
         ctrl->stop = stop;
         ctrl->steps = steps;  // read by the next kernels, after this launch has completed
     }
+}
+__global__ __launch_bounds__(kCandThreads, 4) void ca_cand_kernel(const __grid_constant__ CaKernelArgs k) {
+    cand_body(k, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1370,6 +1403,76 @@ __global__ void ca_terrain_kernel(uint8_t* type, const int32_t* heights, int nx,
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Batched stepping: one launch of each step kernel for many grids.  Every block serves one member
+// grid: the block maps give, per block of a launch, the member slot and the block's index among that
+// member's blocks (slot -1: idle).  A block copies its member's arguments into shared memory and
+// runs the same body as the single-grid kernel with that block index and count, so each member steps
+// exactly as it would alone.  The tensor maps stay in global memory (TMA reads them from there).
+// ------------------------------------------------------------------------------------------
+struct CaBatchView {
+    const CaTensorMaps* tm;    // per member slot
+    const CaKernelArgs* args;  // per member slot
+    const int2* rules_map;     // per block of the drop / rules launches: (slot, block within the member)
+    const int2* cand_map;      // per block of the candidate launch
+    const int* rules_n;        // per slot: its blocks in the drop / rules launches (0: free slot)
+    const int* cand_n;         // per slot: its blocks in the candidate launch
+    int4* status;              // per slot after a graph: (stop, error, steps, member) or (-1, 0, 0, 0)
+    int slots;
+};
+
+__device__ __forceinline__ void load_args(CaKernelArgs& dst, const CaKernelArgs& src) {
+    static_assert(sizeof(CaKernelArgs) % sizeof(uint2) == 0, "copied as 8-byte words");
+    const uint2* from = reinterpret_cast<const uint2*>(&src);
+    uint2* to = reinterpret_cast<uint2*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(CaKernelArgs) / sizeof(uint2)); i += blockDim.x) to[i] = from[i];
+    __syncthreads();
+}
+
+__global__ __launch_bounds__(kThreads, 4) void ca_drop_batch_kernel(const __grid_constant__ CaBatchView b) {
+    const int2 m = b.rules_map[blockIdx.x];
+    if (m.x < 0) return;
+    __shared__ __align__(16) CaKernelArgs s_k;
+    load_args(s_k, b.args[m.x]);
+    drop_body(s_k, 0, (uint32_t)m.y, (uint32_t)b.rules_n[m.x]);
+}
+
+__global__ __launch_bounds__(kThreads, 4) void ca_rules_batch_kernel(const __grid_constant__ CaBatchView b) {
+    const int2 m = b.rules_map[blockIdx.x];
+    if (m.x < 0) return;
+    __shared__ __align__(16) CaKernelArgs s_k;
+    const CaTensorMaps& tm = b.tm[m.x];
+    if (threadIdx.x == 0) {
+        // the maps were written into global memory by a copy since the last launch: order the
+        // tensor-map proxy's reads after that write
+        const char* base = reinterpret_cast<const char*>(&tm);
+        for (int off = 0; off < (int)sizeof(CaTensorMaps); off += (int)sizeof(CUtensorMap))
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(base + off) : "memory");
+    }
+    load_args(s_k, b.args[m.x]);
+    rules_body<ShapeA>(tm, s_k, (uint32_t)m.y, (uint32_t)b.rules_n[m.x]);
+}
+
+__global__ __launch_bounds__(kCandThreads, 4) void ca_cand_batch_kernel(const __grid_constant__ CaBatchView b) {
+    const int2 m = b.cand_map[blockIdx.x];
+    if (m.x < 0) return;
+    __shared__ __align__(16) CaKernelArgs s_k;
+    load_args(s_k, b.args[m.x]);
+    cand_body(s_k, (uint32_t)m.y, (uint32_t)b.cand_n[m.x]);
+}
+
+// Stop state of every member after a graph of steps, gathered for one copy to the host.
+__global__ void ca_batch_status_kernel(const __grid_constant__ CaBatchView b) {
+    for (int i = threadIdx.x; i < b.slots; i += blockDim.x) {
+        int4 st = make_int4(-1, 0, 0, 0);
+        if (b.rules_n[i] > 0) {
+            const CaCtrl* c = b.args[i].ctrl;
+            st = make_int4(c->stop, c->error, (int)c->steps, i);
+        }
+        b.status[i] = st;
+    }
+}
+
 // Vents / seeds: CellState{Lava, flowId, temp, 0, 0} (LavaCA::placeSeeds, LavaCA.hpp:215-220).
 __global__ void ca_seed_kernel(const __grid_constant__ CaKernelArgs k, const int4* seeds, int count, int cur, float temp) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -1427,7 +1530,6 @@ CaKernelArgs make_args(const vca_ca* h) {
         k.tile_list[b] = h->tile_list[b];
     }
     k.tile_flags = h->tile_flags;
-    k.tm = h->tmaps;
     k.tile_mark[0] = h->tile_mark[0];
     k.tile_mark[1] = h->tile_mark[1];
     k.desc = h->desc_plane;
@@ -1444,6 +1546,10 @@ CaKernelArgs make_args(const vca_ca* h) {
     k.hist_active = h->hist_active;
     k.hist_changed = h->hist_changed;
     k.ntiles = h->ntiles;
+    k.slab = h->slab ? 1 : 0;
+    k.gidx_base = h->slab ? (uint64_t)h->geom.nx * h->geom.ny * (uint64_t)h->slab_z0 : 0;
+    k.own_z0 = h->slab ? h->own_z0 : 0;
+    k.own_z1 = h->slab ? h->own_z1 : h->geom.nz;
     return k;
 }
 
@@ -1451,6 +1557,15 @@ vca_status check(const vca_ca* h) {
     if (h == nullptr) {
         set_error("null vca_ca handle");
         return VCA_ERR_ARG;
+    }
+    return VCA_OK;
+}
+
+// A handle that a batch is stepping takes no other call until it leaves the batch.
+vca_status not_in_batch(const vca_ca* h, const char* who) {
+    if (h->batch != nullptr) {
+        set_error(std::string(who) + ": the handle is a member of a batch (vca_ca_batch_remove, or wait for it to stop)");
+        return VCA_ERR_STATE;
     }
     return VCA_OK;
 }
@@ -1512,7 +1627,9 @@ vca_status init_state(vca_ca* h, int steps_done) {
     m->air = air;
     // LavaCA::countInitialState (LavaCA.hpp:1272-1279)
     int stop = VCA_STOP_RUNNING;
-    if (!c.classic && lava == 0) stop = VCA_STOP_NO_LAVA;
+    if (h->slab) {  // the counts of one slab do not decide: the caller sets the stop (vca_ca_slab_stop)
+        if (h->desc.max_steps <= steps_done) stop = VCA_STOP_MAX_STEPS;
+    } else if (!c.classic && lava == 0) stop = VCA_STOP_NO_LAVA;
     else if (c.classic && air == 0) stop = VCA_STOP_NO_AIR;
     else if (h->desc.max_steps <= steps_done) stop = VCA_STOP_MAX_STEPS;
     m->stop = stop;
@@ -1523,6 +1640,22 @@ vca_status init_state(vca_ca* h, int steps_done) {
     return VCA_OK;
 }
 
+// The rules pass of the handle's tile-shape family.
+void launch_rules(const vca_ca* h, const CaKernelArgs& k) {
+    switch (h->geom.shape) {
+        case 0: ca_rules_kernel<ShapeA><<<h->grid_blocks, kThreads, rules_dyn_smem<ShapeA>(), h->stream>>>(h->tmaps, k); break;
+        case 1: ca_rules_kernel<ShapeB><<<h->grid_blocks, kThreads, rules_dyn_smem<ShapeB>(), h->stream>>>(h->tmaps, k); break;
+        default: ca_rules_kernel<ShapeC><<<h->grid_blocks, kThreads, rules_dyn_smem<ShapeC>(), h->stream>>>(h->tmaps, k); break;
+    }
+}
+
+template <class S>
+cudaError_t rules_occupancy(int* per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(ca_rules_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rules_dyn_smem<S>());
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, ca_rules_kernel<S>, kThreads, rules_dyn_smem<S>());
+}
+
 constexpr int kGraphSteps = 16;  // steps captured in one CUDA graph
 
 // The launches of kGraphSteps steps, captured once per state set-up (the kernel arguments only
@@ -1531,14 +1664,15 @@ vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
     // A captured graph stays valid while the arguments and launch shapes it was captured with are
     // unchanged (a resident handle running job after job on one space keeps them; make_args zeroes
     // the padding, so a byte comparison is exact).
-    if (h->graph_exec && std::memcmp(&h->graph_args, &k, sizeof(k)) == 0 && h->graph_grid == h->grid_blocks &&
+    if (h->graph_exec && std::memcmp(&h->graph_args, &k, sizeof(k)) == 0 &&
+        std::memcmp(&h->graph_tm, &h->tmaps, sizeof(h->tmaps)) == 0 && h->graph_grid == h->grid_blocks &&
         h->graph_cand == h->cand_blocks)
         return VCA_OK;
     drop_graph(h);
     VCA_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < kGraphSteps; ++s) {
         ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
-        ca_rules_kernel<<<h->grid_blocks, kThreads, kRulesDynSmem, h->stream>>>(k);
+        launch_rules(h, k);
         ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
     }
     cudaGraph_t graph = nullptr;
@@ -1546,6 +1680,7 @@ vca_status ensure_graph(vca_ca* h, const CaKernelArgs& k) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
     const cudaError_t e2 = cudaGraphInstantiate(&h->graph_exec, graph, 0);
     h->graph_args = k;
+    h->graph_tm = h->tmaps;
     h->graph_grid = h->grid_blocks;
     h->graph_cand = h->cand_blocks;
     cudaGraphDestroy(graph);
@@ -1615,7 +1750,7 @@ vca_status run_steps(vca_ca* h, int max_new_steps, bool until_stop) {
             if (h->profile_kernels) VCA_CUDA(mark());
             ca_drop_kernel<<<h->grid_blocks, kThreads, 0, h->stream>>>(k, 0);
             if (h->profile_kernels) VCA_CUDA(mark());
-            ca_rules_kernel<<<h->grid_blocks, kThreads, kRulesDynSmem, h->stream>>>(k);
+            launch_rules(h, k);
             if (h->profile_kernels) VCA_CUDA(mark());
             ca_cand_kernel<<<h->cand_blocks, kCandThreads, 0, h->stream>>>(k);
             if (h->profile_kernels) VCA_CUDA(mark());
@@ -1855,6 +1990,14 @@ vca_status validate_desc(const vca_ca_desc* d, const char* who) {
         return bad("unknown neighborhood, boundary, mode or sweep");
     NbTable nb;
     if (!build_nb(d->neighborhood, nx, ny, nz, nb)) return bad("the hexagonal neighbourhood is defined in 2D only");
+    if (d->tile_y != 0 || d->tile_z != 0) {
+        const int ty = d->tile_y, tz = d->tile_z;
+        const bool pow2 = ty > 0 && tz > 0 && (ty & (ty - 1)) == 0 && (tz & (tz - 1)) == 0;
+        if (!pow2 || ty * tz != 16) return bad("tile_y x tile_z must be 16 cells (1 x 16, 2 x 8, 4 x 4, 8 x 2, 16 x 1)");
+        if (ny == 1 && ty != 1) return bad("a 2D x-z section takes tiles with tile_y = 1");
+        if (nz == 1 && tz != 1) return bad("a 2D x-y plane takes tiles with tile_z = 1");
+    }
+    if (d->rules_blocks_per_sm < 0) return bad("rules_blocks_per_sm must be >= 0");
     return VCA_OK;
 }
 
@@ -1869,7 +2012,10 @@ CaGeom geometry_of(const vca_ca_desc* d) {
     g.per[0] = periodic && d->nx > 1;
     g.per[1] = periodic && d->ny > 1;
     g.per[2] = periodic && d->mode == VCA_MODE_CLASSIC && d->nz > 1;
-    if (d->ny > 1 && d->nz > 1) {
+    if (d->tile_y != 0 && d->tile_z != 0) {
+        g.TY = d->tile_y;
+        g.TZ = d->tile_z;
+    } else if (d->ny > 1 && d->nz > 1) {
         g.TY = 4;
         g.TZ = 4;
     } else if (d->ny == 1) {
@@ -1878,6 +2024,15 @@ CaGeom geometry_of(const vca_ca_desc* d) {
     } else {
         g.TY = 16;
         g.TZ = 1;
+    }
+    {
+        // the shared-memory family that holds this tile's staged rows (RulesShape)
+        const int hy = d->ny > 1 ? g.TY + 2 : 1, hz = d->nz > 1 ? g.TZ + 2 : 1;
+        const int halo = hy * hz, drop = hy * g.TZ;
+        const int spill_ty = d->nz > 1 ? g.TY : 1;  // spill levels are staged only with a z axis
+        g.shape = (halo <= ShapeA::halo && drop <= ShapeA::drop && spill_ty <= ShapeA::ty)   ? 0
+                  : (halo <= ShapeB::halo && drop <= ShapeB::drop && spill_ty <= ShapeB::ty) ? 1
+                                                                                              : 2;
     }
     g.tiles_x = g.P / kTileX;
     g.tiles_y = (d->ny + g.TY - 1) / g.TY;
@@ -1922,7 +2077,9 @@ vca_status configure(vca_ca* h, const vca_ca_desc* d) {
                 ++h->tables_host.nside;
             }
         }
-    h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)h->sms * std::max(1, h->rules_per_sm));
+    int per_sm = std::max(1, h->rules_per_sm[g.shape]);
+    if (d->rules_blocks_per_sm > 0) per_sm = std::min(per_sm, d->rules_blocks_per_sm);
+    h->grid_blocks = (int)std::min<uint64_t>(h->ntiles, (uint64_t)h->sms * per_sm);
     // one wave, and no more blocks than the grid could ever list candidates for (small grids share the GPU)
     h->cand_blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)h->sms * std::max(1, h->cand_per_sm),
                                                                   (h->ntiles * kTileCells + kCandThreads - 1) / kCandThreads));
@@ -2003,10 +2160,10 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     h->cap = need;
     e = cudaMallocHost(&h->ctrl_host, sizeof(CaCtrl));
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
-    e = cudaFuncSetAttribute(ca_rules_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRulesDynSmem);
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->rules_per_sm, ca_rules_kernel, kThreads, kRulesDynSmem);
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
+    if ((e = rules_occupancy<ShapeA>(&h->rules_per_sm[0])) != cudaSuccess ||
+        (e = rules_occupancy<ShapeB>(&h->rules_per_sm[1])) != cudaSuccess ||
+        (e = rules_occupancy<ShapeC>(&h->rules_per_sm[2])) != cudaSuccess)
+        return fail(cuda_fail(e, "rules-pass occupancy"));
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->cand_per_sm, ca_cand_kernel, kCandThreads, 0);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
     if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess ||
@@ -2023,6 +2180,7 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
 
 vca_status vca_ca_reconfigure(vca_ca* h, const vca_ca_desc* d) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_reconfigure")) return s;
     if (d == nullptr) {
         set_error("vca_ca_reconfigure: null desc");
         return VCA_ERR_ARG;
@@ -2039,6 +2197,7 @@ vca_status vca_ca_reconfigure(vca_ca* h, const vca_ca_desc* d) {
         return VCA_ERR_ARG;
     }
     VCA_CUDA(cudaSetDevice(h->device));
+    h->slab = false;
     return configure(h, d);
 }
 
@@ -2058,6 +2217,7 @@ vca_status vca_ca_footprint(const vca_ca_desc* d, uint64_t* bytes) {
 
 vca_status vca_ca_reset(vca_ca* h) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_reset")) return s;
     VCA_CUDA(cudaSetDevice(h->device));
     if (vca_status s = clear_planes(h)) return s;
     vca_vent none{0, 0, 0, 0};
@@ -2071,6 +2231,7 @@ vca_status vca_ca_reset(vca_ca* h) {
 
 vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_apply_terrain")) return s;
     if (heights == nullptr) {
         set_error("vca_ca_apply_terrain: null heights");
         return VCA_ERR_ARG;
@@ -2089,7 +2250,13 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
             return VCA_ERR_ARG;
         }
     }
-    const std::vector<int32_t> spill = fill_depressions(hv, g.nx, g.ny, g.per[0] != 0, g.per[1] != 0);
+    std::vector<int32_t> spill = fill_depressions(hv, g.nx, g.ny, g.per[0] != 0, g.per[1] != 0);
+    if (h->slab) {
+        // heights and spill levels of the whole grid, seen from this slab's layer 0: every test
+        // against them (z < h, z - 1 < spill, z <= spill) keeps its truth with both sides shifted
+        for (auto& v : hv) v -= h->slab_z0;
+        for (auto& v : spill) v -= h->slab_z0;
+    }
     VCA_CUDA(cudaMemcpyAsync(h->heights_dev, hv.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
     VCA_CUDA(cudaMemcpyAsync(h->spill, spill.data(), sizeof(int32_t) * cols, cudaMemcpyHostToDevice, h->stream));
     const int cur = h->steps & 1;
@@ -2103,6 +2270,7 @@ vca_status vca_ca_apply_terrain(vca_ca* h, const int32_t* heights) {
 
 vca_status vca_ca_place_seeds(vca_ca* h, const vca_vent* vents, int count) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_place_seeds")) return s;
     if (count < 0 || (count > 0 && vents == nullptr)) {
         set_error("vca_ca_place_seeds: bad vent list");
         return VCA_ERR_ARG;
@@ -2161,6 +2329,7 @@ vca_status vca_ca_set_state(vca_ca* h, const uint8_t* type, const int32_t* flow_
                             const uint16_t* solid_step, const uint16_t* arrival_step, const int32_t* spill,
                             const vca_vent* vents, int vent_count, int steps_done) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_set_state")) return s;
     if (!type || !flow_id || !temp || !solid_step || !arrival_step || steps_done < 0 || vent_count < 0 ||
         (vent_count > 0 && !vents)) {
         set_error("vca_ca_set_state: bad argument");
@@ -2190,6 +2359,7 @@ vca_status vca_ca_set_state(vca_ca* h, const uint8_t* type, const int32_t* flow_
 
 vca_status vca_ca_step(vca_ca* h, int* running) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_step")) return s;
     VCA_CUDA(cudaSetDevice(h->device));
     if (vca_status s = run_steps(h, 1, false)) return s;
     if (running) *running = h->stop == VCA_STOP_RUNNING;
@@ -2198,12 +2368,14 @@ vca_status vca_ca_step(vca_ca* h, int* running) {
 
 vca_status vca_ca_run(vca_ca* h) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_run")) return s;
     VCA_CUDA(cudaSetDevice(h->device));
     return run_steps(h, 0, true);
 }
 
 vca_status vca_ca_get_info(vca_ca* h, vca_ca_info* out) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_get_info")) return s;
     if (!out) {
         set_error("vca_ca_get_info: null output");
         return VCA_ERR_ARG;
@@ -2223,6 +2395,7 @@ vca_status vca_ca_get_info(vca_ca* h, vca_ca_info* out) {
 
 vca_status vca_ca_history(vca_ca* h, uint64_t* active, uint64_t* changed, int capacity, int* count) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_history")) return s;
     VCA_CUDA(cudaSetDevice(h->device));
     if (vca_status s = sync_ctrl(h)) return s;
     const int n = std::min(std::max(capacity, 0), h->steps);
@@ -2236,6 +2409,7 @@ vca_status vca_ca_history(vca_ca* h, uint64_t* active, uint64_t* changed, int ca
 vca_status vca_ca_download(vca_ca* h, uint8_t* type, int32_t* flow_id, float* temp, uint16_t* solid_step,
                            uint16_t* arrival_step) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_download")) return s;
     VCA_CUDA(cudaSetDevice(h->device));
     if (vca_status s = sync_ctrl(h)) return s;
     const int cur = h->steps & 1;
@@ -2250,6 +2424,7 @@ vca_status vca_ca_download(vca_ca* h, uint8_t* type, int32_t* flow_id, float* te
 
 vca_status vca_ca_get_spill(vca_ca* h, int32_t* spill) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_get_spill")) return s;
     if (!h->has_terrain) {
         set_error("vca_ca_get_spill: no terrain");
         return VCA_ERR_STATE;
@@ -2261,6 +2436,7 @@ vca_status vca_ca_get_spill(vca_ca* h, int32_t* spill) {
 
 vca_status vca_ca_flow_stats(vca_ca* h, int flows, uint64_t* lava, uint64_t* basalt, uint64_t* reach2) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_flow_stats")) return s;
     if (flows < 0 || (flows > 0 && (lava == nullptr || basalt == nullptr || reach2 == nullptr))) {
         set_error("vca_ca_flow_stats: bad flow count or null array");
         return VCA_ERR_ARG;
@@ -2298,6 +2474,125 @@ vca_status vca_ca_flow_stats(vca_ca* h, int flows, uint64_t* lava, uint64_t* bas
     return VCA_OK;
 }
 
+vca_status vca_ca_set_slab(vca_ca* h, int z_offset, int own_z0, int own_z1) {
+    if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_set_slab")) return s;
+    const auto& g = h->geom;
+    if (h->desc.mode != VCA_MODE_LAVA || g.nz < 2 || z_offset < 0 || own_z0 < 0 || own_z1 > g.nz || own_z0 >= own_z1) {
+        set_error("vca_ca_set_slab: a slab is a lava grid with nz > 1, z_offset >= 0 and 0 <= own_z0 < own_z1 <= nz");
+        return VCA_ERR_ARG;
+    }
+    if (h->seeded || h->has_terrain) {
+        set_error("vca_ca_set_slab: set the slab before the terrain and the seeds");
+        return VCA_ERR_STATE;
+    }
+    h->slab = true;
+    h->slab_z0 = z_offset;
+    h->own_z0 = own_z0;
+    h->own_z1 = own_z1;
+    h->desc.sweep = VCA_SWEEP_DENSE;  // halo copies change cells outside the tile scheduler's view
+    return VCA_OK;
+}
+
+vca_status vca_ca_slab_step(vca_ca* h, uint64_t* active, uint64_t* changed) {
+    if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_slab_step")) return s;
+    if (!h->slab) {
+        set_error("vca_ca_slab_step: the handle is not a slab (vca_ca_set_slab)");
+        return VCA_ERR_STATE;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    const int before = h->steps;
+    if (vca_status s = run_steps(h, 1, false)) return s;
+    unsigned long long a = 0, c = 0;
+    if (h->steps > before) {
+        VCA_CUDA(cudaMemcpyAsync(&a, h->hist_active + before, 8, cudaMemcpyDeviceToHost, h->stream));
+        VCA_CUDA(cudaMemcpyAsync(&c, h->hist_changed + before, 8, cudaMemcpyDeviceToHost, h->stream));
+        VCA_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (active) *active = a;
+    if (changed) *changed = c;
+    return VCA_OK;
+}
+
+vca_status vca_ca_slab_stop(vca_ca* h, int stop_reason) {
+    if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_slab_stop")) return s;
+    if (!h->slab || stop_reason < VCA_STOP_RUNNING || stop_reason > VCA_STOP_MAX_STEPS) {
+        set_error("vca_ca_slab_stop: a slab handle and a VCA_STOP_* value");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    const int32_t v = stop_reason;
+    VCA_CUDA(cudaMemcpyAsync(&h->ctrl->stop, &v, sizeof(v), cudaMemcpyHostToDevice, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    h->stop = stop_reason;
+    return VCA_OK;
+}
+
+vca_status vca_ca_layers(vca_ca* h, void** type, void** flow_id, void** temp, void** solid_step, void** arrival_step,
+                         uint64_t* layer_cells) {
+    if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_ca_layers")) return s;
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (vca_status s = sync_ctrl(h)) return s;
+    const int cur = h->steps & 1;
+    if (type) *type = h->type[cur];
+    if (flow_id) *flow_id = h->flow[cur];
+    if (temp) *temp = h->temp[cur];
+    if (solid_step) *solid_step = h->solid[cur];
+    if (arrival_step) *arrival_step = h->arrival[cur];
+    if (layer_cells) *layer_cells = (uint64_t)h->geom.P * h->geom.ny;
+    return VCA_OK;
+}
+
+// Halo message of a slab: `types` type layers from local layer z0, then the flowId, temperature,
+// solidStep and arrivalStep of local layer `full` (full < 0: none).  Layers are whole pitched
+// layers (their padding cells are VOID on every slab alike).
+static vca_status layers_check(vca_ca* h, int z0, int types, int full, const void* buf, const char* who) {
+    if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, who)) return s;
+    if (buf == nullptr || types < 0 || z0 < 0 || z0 + types > h->geom.nz || full >= h->geom.nz) {
+        set_error(std::string(who) + ": layers outside the grid or null buffer");
+        return VCA_ERR_ARG;
+    }
+    return VCA_OK;
+}
+
+static vca_status copy_layers(vca_ca* h, int z0, int types, int full, void* buf, bool to_buf) {
+    VCA_CUDA(cudaSetDevice(h->device));
+    if (vca_status s = sync_ctrl(h)) return s;
+    const int cur = h->steps & 1;
+    const size_t L = (size_t)h->geom.P * h->geom.ny;
+    char* b = static_cast<char*>(buf);
+    auto move = [&](void* plane, size_t elem, int z, int n, size_t at) -> cudaError_t {
+        char* dev = static_cast<char*>(plane) + (size_t)z * L * elem;
+        return to_buf ? cudaMemcpyAsync(b + at, dev, (size_t)n * L * elem, cudaMemcpyDefault, h->stream)
+                      : cudaMemcpyAsync(dev, b + at, (size_t)n * L * elem, cudaMemcpyDefault, h->stream);
+    };
+    size_t at = 0;
+    if (types > 0) VCA_CUDA(move(h->type[cur], 1, z0, types, at));
+    at += (size_t)types * L;
+    if (full >= 0) {
+        VCA_CUDA(move(h->flow[cur], 4, full, 1, at));
+        VCA_CUDA(move(h->temp[cur], 4, full, 1, at + 4 * L));
+        VCA_CUDA(move(h->solid[cur], 2, full, 1, at + 8 * L));
+        VCA_CUDA(move(h->arrival[cur], 2, full, 1, at + 10 * L));
+    }
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    return VCA_OK;
+}
+
+vca_status vca_ca_pack_layers(vca_ca* h, int z0, int types, int full, void* buf) {
+    if (vca_status s = layers_check(h, z0, types, full, buf, "vca_ca_pack_layers")) return s;
+    return copy_layers(h, z0, types, full, buf, true);
+}
+
+vca_status vca_ca_unpack_layers(vca_ca* h, int z0, int types, int full, const void* buf) {
+    if (vca_status s = layers_check(h, z0, types, full, buf, "vca_ca_unpack_layers")) return s;
+    return copy_layers(h, z0, types, full, const_cast<void*>(buf), false);
+}
+
 vca_status vca_ca_kernel_times(vca_ca* h, double* drop_ms, double* rules_ms, double* cand_ms, uint64_t* steps) {
     if (vca_status s = check(h)) return s;
     const double n = h->rules_launches ? (double)h->rules_launches : 1.0;
@@ -2318,6 +2613,7 @@ vca_status vca_ca_timing(vca_ca* h, double* total_ms, double* rules_kernel_ms, u
 
 void vca_ca_destroy(vca_ca* h) {
     if (!h) return;
+    if (h->batch) vca_ca_batch_remove(h->batch, h);
     free_all(h);
     delete h;
 }
@@ -2328,6 +2624,7 @@ void vca_ca_destroy(vca_ca* h) {
 namespace vca {
 vca_status ca_view(vca_ca* h, CaView* v) {
     if (vca_status s = check(h)) return s;
+    if (vca_status s = not_in_batch(h, "vca_mc_set_domain_from_ca / vca_mc_set_mobility_from_ca")) return s;
     if (vca_status s = sync_ctrl(h)) return s;
     const int cur = h->steps & 1;
     v->type = h->type[cur];
@@ -2342,3 +2639,399 @@ vca_status ca_view(vca_ca* h, CaView* v) {
     return VCA_OK;
 }
 }  // namespace vca
+
+// ============================================================================================
+// Batched stepping (vca_ca_batch_*): many member grids stepped by shared launches.
+// ============================================================================================
+struct vca_ca_batch {
+    int device = 0;
+    int cap = 0;                  // member slots
+    int rules_grid = 0, cand_grid = 0;
+    cudaStream_t stream = nullptr;
+    // device tables
+    CaTensorMaps* d_tm = nullptr;
+    CaKernelArgs* d_args = nullptr;
+    int2* d_rules_map = nullptr;
+    int2* d_cand_map = nullptr;
+    int* d_rules_n = nullptr;
+    int* d_cand_n = nullptr;
+    int4* d_status = nullptr;
+    int4* h_status = nullptr;     // pinned, two ring slots of cap entries
+    cudaEvent_t status_ev[2] = {nullptr, nullptr};
+    cudaEvent_t sync_ev = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<vca_ca*> slots;   // member of each slot (nullptr: free)
+    std::vector<vca_ca*> snap[2]; // the slots when the graph of a ring slot was launched
+    std::vector<vca_ca*> early;   // members that had stopped before they were added
+    std::vector<vca_ca*> done;    // stopped members not yet handed out
+    bool dirty = true;            // tables on the device are out of date
+    int pending = -1;             // ring slot whose status is not read yet
+    int ring = 0;
+    uint64_t graphs = 0, launches = 0;
+};
+
+namespace {
+
+vca_status batch_check(vca_ca_batch* b) {
+    if (b == nullptr) {
+        set_error("null vca_ca_batch");
+        return VCA_ERR_ARG;
+    }
+    return VCA_OK;
+}
+
+// Blocks of a launch of `grid` blocks shared among the members by weight (at least one each).
+void split_blocks(const std::vector<uint64_t>& w, int grid, std::vector<int>& n) {
+    const size_t m = w.size();
+    n.assign(m, 1);
+    if (m == 0) return;
+    uint64_t total = 0;
+    for (uint64_t v : w) total += v;
+    int used = 0;
+    for (size_t i = 0; i < m; ++i) {
+        n[i] = std::max<int>(1, (int)((double)grid * (double)w[i] / (double)std::max<uint64_t>(1, total)));
+        used += n[i];
+    }
+    while (used > grid) {  // take back from the largest shares
+        size_t big = 0;
+        for (size_t i = 1; i < m; ++i)
+            if (n[i] > n[big]) big = i;
+        if (n[big] <= 1) break;
+        --n[big];
+        --used;
+    }
+    while (used < grid) {  // the rest to the heaviest members, round robin by weight order
+        size_t best = 0;
+        double best_r = -1.0;
+        for (size_t i = 0; i < m; ++i) {
+            const double r = (double)w[i] / (double)n[i];
+            if (r > best_r) {
+                best_r = r;
+                best = i;
+            }
+        }
+        ++n[best];
+        ++used;
+    }
+}
+
+// Member arguments and block maps to the device (on the batch stream, ordered after the graphs
+// already launched and before the next).
+vca_status batch_upload(vca_ca_batch* b) {
+    std::vector<CaTensorMaps> tm((size_t)b->cap);
+    std::vector<CaKernelArgs> args((size_t)b->cap);
+    std::vector<int> rn((size_t)b->cap, 0), cn((size_t)b->cap, 0);
+    std::vector<int2> rmap((size_t)b->rules_grid, make_int2(-1, 0)), cmap((size_t)b->cand_grid, make_int2(-1, 0));
+    std::vector<int> members;
+    std::vector<uint64_t> w;
+    for (int i = 0; i < b->cap; ++i) {
+        vca_ca* h = b->slots[(size_t)i];
+        std::memset(&args[(size_t)i], 0, sizeof(CaKernelArgs));
+        if (!h) continue;
+        tm[(size_t)i] = h->tmaps;
+        args[(size_t)i] = make_args(h);
+        members.push_back(i);
+        w.push_back(std::max<uint64_t>(1, h->ntiles));
+    }
+    std::vector<int> nr, nc;
+    split_blocks(w, b->rules_grid, nr);
+    split_blocks(w, b->cand_grid, nc);
+    int at_r = 0, at_c = 0;
+    for (size_t j = 0; j < members.size(); ++j) {
+        const int slot = members[j];
+        rn[(size_t)slot] = nr[j];
+        cn[(size_t)slot] = nc[j];
+        for (int q = 0; q < nr[j]; ++q) rmap[(size_t)(at_r + q)] = make_int2(slot, q);
+        for (int q = 0; q < nc[j]; ++q) cmap[(size_t)(at_c + q)] = make_int2(slot, q);
+        at_r += nr[j];
+        at_c += nc[j];
+    }
+    // pageable sources: each copy is staged before the call returns, so the vectors may go
+    VCA_CUDA(cudaMemcpyAsync(b->d_tm, tm.data(), sizeof(CaTensorMaps) * tm.size(), cudaMemcpyHostToDevice, b->stream));
+    VCA_CUDA(cudaMemcpyAsync(b->d_args, args.data(), sizeof(CaKernelArgs) * args.size(), cudaMemcpyHostToDevice, b->stream));
+    VCA_CUDA(cudaMemcpyAsync(b->d_rules_n, rn.data(), sizeof(int) * rn.size(), cudaMemcpyHostToDevice, b->stream));
+    VCA_CUDA(cudaMemcpyAsync(b->d_cand_n, cn.data(), sizeof(int) * cn.size(), cudaMemcpyHostToDevice, b->stream));
+    VCA_CUDA(cudaMemcpyAsync(b->d_rules_map, rmap.data(), sizeof(int2) * rmap.size(), cudaMemcpyHostToDevice, b->stream));
+    VCA_CUDA(cudaMemcpyAsync(b->d_cand_map, cmap.data(), sizeof(int2) * cmap.size(), cudaMemcpyHostToDevice, b->stream));
+    b->dirty = false;
+    return VCA_OK;
+}
+
+// A member leaves: its slot is freed and its own stream waits for everything the batch launched so
+// far, so the member's next calls see its final state.
+vca_status batch_detach(vca_ca_batch* b, vca_ca* h, const int4* st) {
+    b->slots[(size_t)h->batch_slot] = nullptr;
+    b->dirty = true;
+    VCA_CUDA(cudaEventRecord(b->sync_ev, b->stream));
+    VCA_CUDA(cudaStreamWaitEvent(h->stream, b->sync_ev, 0));
+    if (st) {
+        h->steps = st->z;
+        h->stop = st->x;
+    }
+    h->batch = nullptr;
+    h->batch_slot = -1;
+    return VCA_OK;
+}
+
+// Reads the status of the graph in ring slot r (waits for it) and takes the members that stopped
+// out of the batch.
+vca_status batch_collect(vca_ca_batch* b, int r) {
+    VCA_CUDA(cudaEventSynchronize(b->status_ev[r]));
+    const int4* st = b->h_status + (size_t)r * b->cap;
+    for (int i = 0; i < b->cap; ++i) {
+        vca_ca* h = b->snap[r][(size_t)i];
+        if (!h || b->slots[(size_t)i] != h || st[i].x < 0) continue;
+        if (st[i].x != VCA_STOP_RUNNING || st[i].y != 0) {
+            if (vca_status s = batch_detach(b, h, &st[i])) return s;
+            b->done.push_back(h);
+        }
+    }
+    return VCA_OK;
+}
+
+vca_status batch_capture(vca_ca_batch* b) {
+    CaBatchView v{b->d_tm, b->d_args, b->d_rules_map, b->d_cand_map, b->d_rules_n, b->d_cand_n, b->d_status, b->cap};
+    VCA_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < kGraphSteps; ++s) {
+        ca_drop_batch_kernel<<<b->rules_grid, kThreads, 0, b->stream>>>(v);
+        ca_rules_batch_kernel<<<b->rules_grid, kThreads, kRulesDynSmem, b->stream>>>(v);
+        ca_cand_batch_kernel<<<b->cand_grid, kCandThreads, 0, b->stream>>>(v);
+    }
+    ca_batch_status_kernel<<<1, 256, 0, b->stream>>>(v);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t e2 = cudaGraphInstantiate(&b->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+        b->graph = nullptr;
+        return cuda_fail(e2, "cudaGraphInstantiate");
+    }
+    return VCA_OK;
+}
+
+void batch_free(vca_ca_batch* b) {
+    cudaSetDevice(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    cudaFree(b->d_tm);
+    cudaFree(b->d_args);
+    cudaFree(b->d_rules_map);
+    cudaFree(b->d_cand_map);
+    cudaFree(b->d_rules_n);
+    cudaFree(b->d_cand_n);
+    cudaFree(b->d_status);
+    if (b->h_status) cudaFreeHost(b->h_status);
+    for (cudaEvent_t e : b->status_ev)
+        if (e) cudaEventDestroy(e);
+    if (b->sync_ev) cudaEventDestroy(b->sync_ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+vca_status vca_ca_batch_create(int device, int max_members, vca_ca_batch** out) {
+    if (out == nullptr || max_members < 1) {
+        set_error("vca_ca_batch_create: null output or max_members < 1");
+        return VCA_ERR_ARG;
+    }
+    *out = nullptr;
+    vca_ca_batch* b = new vca_ca_batch();
+    b->device = device;
+    auto fail = [&](vca_status s) {
+        batch_free(b);
+        delete b;
+        return s;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return fail(cuda_fail(e, "cudaGetDeviceProperties"));
+    if (prop.major < 10) {
+        set_error("vca_ca_batch_create: needs an sm_100 (Blackwell) device");
+        return fail(VCA_ERR_CUDA);
+    }
+    int rules_per_sm = 0, cand_per_sm = 0;
+    if ((e = cudaFuncSetAttribute(ca_rules_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRulesDynSmem)) !=
+        cudaSuccess)
+        return fail(cuda_fail(e, "cudaFuncSetAttribute"));
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rules_per_sm, ca_rules_batch_kernel, kThreads, kRulesDynSmem)) !=
+        cudaSuccess)
+        return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cand_per_sm, ca_cand_batch_kernel, kCandThreads, 0)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
+    b->rules_grid = prop.multiProcessorCount * std::max(1, rules_per_sm);
+    b->cand_grid = prop.multiProcessorCount * std::max(1, cand_per_sm);
+    b->cap = std::min(max_members, std::min(b->rules_grid, b->cand_grid));
+    b->slots.assign((size_t)b->cap, nullptr);
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaStreamCreate"));
+#define BALLOC(ptr, bytes)                                                    \
+    do {                                                                      \
+        e = cudaMalloc(&(ptr), (bytes));                                      \
+        if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc " #ptr));  \
+    } while (0)
+    BALLOC(b->d_tm, sizeof(CaTensorMaps) * (size_t)b->cap);
+    BALLOC(b->d_args, sizeof(CaKernelArgs) * (size_t)b->cap);
+    BALLOC(b->d_rules_map, sizeof(int2) * (size_t)b->rules_grid);
+    BALLOC(b->d_cand_map, sizeof(int2) * (size_t)b->cand_grid);
+    BALLOC(b->d_rules_n, sizeof(int) * (size_t)b->cap);
+    BALLOC(b->d_cand_n, sizeof(int) * (size_t)b->cap);
+    BALLOC(b->d_status, sizeof(int4) * (size_t)b->cap);
+#undef BALLOC
+    if ((e = cudaMallocHost(&b->h_status, sizeof(int4) * 2 * (size_t)b->cap)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaEventCreateWithFlags(&b->status_ev[0], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->status_ev[1], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->sync_ev, cudaEventDisableTiming)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaEventCreate"));
+    if (vca_status s = batch_upload(b)) return fail(s);
+    if (vca_status s = batch_capture(b)) return fail(s);
+    *out = b;
+    return VCA_OK;
+}
+
+vca_status vca_ca_batch_add(vca_ca_batch* b, vca_ca* h) {
+    if (vca_status s = batch_check(b)) return s;
+    if (vca_status s = check(h)) return s;
+    if (h->batch != nullptr) {
+        set_error("vca_ca_batch_add: the handle is already in a batch");
+        return VCA_ERR_ARG;
+    }
+    if (h->device != b->device) {
+        set_error("vca_ca_batch_add: the handle lives on another device");
+        return VCA_ERR_ARG;
+    }
+    if (!h->seeded) {
+        set_error("vca_ca_batch_add: place_seeds or set_state must come before stepping");
+        return VCA_ERR_STATE;
+    }
+    if (h->geom.shape != 0) {
+        set_error("vca_ca_batch_add: batched launches take the tile shapes of 4 x 4 or smaller halos "
+                  "(4 x 4 in 3D, the 2D tiles); this handle uses " + std::to_string(h->geom.TY) + " x " +
+                  std::to_string(h->geom.TZ));
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(b->device));
+    if (h->stop != VCA_STOP_RUNNING) {  // nothing to step: reported by the next advance
+        h->batch = b;
+        b->early.push_back(h);
+        return VCA_OK;
+    }
+    int slot = -1;
+    for (int i = 0; i < b->cap && slot < 0; ++i)
+        if (!b->slots[(size_t)i]) slot = i;
+    if (slot < 0) {
+        set_error("vca_ca_batch_add: the batch is full (" + std::to_string(b->cap) + " members)");
+        return VCA_ERR_ARG;
+    }
+    // the batch's next launches come after the member's set-up work
+    VCA_CUDA(cudaEventRecord(b->sync_ev, h->stream));
+    VCA_CUDA(cudaStreamWaitEvent(b->stream, b->sync_ev, 0));
+    b->slots[(size_t)slot] = h;
+    h->batch = b;
+    h->batch_slot = slot;
+    b->dirty = true;
+    return VCA_OK;
+}
+
+vca_status vca_ca_batch_advance(vca_ca_batch* b, int max_graphs, vca_ca** finished, int capacity, int* count,
+                                int* running) {
+    if (vca_status s = batch_check(b)) return s;
+    if (capacity < 0 || (capacity > 0 && finished == nullptr)) {
+        set_error("vca_ca_batch_advance: bad output list");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(b->device));
+    for (vca_ca* h : b->early) {
+        h->batch = nullptr;
+        b->done.push_back(h);
+    }
+    b->early.clear();
+    auto members = [&]() {
+        int n = 0;
+        for (vca_ca* h : b->slots) n += h != nullptr;
+        return n;
+    };
+    for (int g = 0; g < max_graphs && b->done.empty(); ++g) {
+        if (members() == 0) break;
+        if (b->dirty)
+            if (vca_status s = batch_upload(b)) return s;
+        const int r = b->ring;
+        VCA_CUDA(cudaGraphLaunch(b->graph, b->stream));
+        VCA_CUDA(cudaMemcpyAsync(b->h_status + (size_t)r * b->cap, b->d_status, sizeof(int4) * (size_t)b->cap,
+                                 cudaMemcpyDeviceToHost, b->stream));
+        VCA_CUDA(cudaEventRecord(b->status_ev[r], b->stream));
+        b->snap[r] = b->slots;
+        b->graphs += 1;
+        b->launches += 3 * kGraphSteps + 1;
+        b->ring ^= 1;
+        if (b->pending >= 0) {
+            if (vca_status s = batch_collect(b, b->pending)) return s;
+        }
+        b->pending = r;
+    }
+    // with nothing left to launch, the last graph's status is read now
+    if (b->done.empty() && b->pending >= 0) {
+        if (vca_status s = batch_collect(b, b->pending)) return s;
+        b->pending = -1;
+    }
+    int n = 0;
+    while (n < capacity && !b->done.empty()) {
+        finished[n++] = b->done.front();
+        b->done.erase(b->done.begin());
+    }
+    if (count) *count = n;
+    if (running) *running = members();
+    return VCA_OK;
+}
+
+vca_status vca_ca_batch_remove(vca_ca_batch* b, vca_ca* h) {
+    if (vca_status s = batch_check(b)) return s;
+    if (vca_status s = check(h)) return s;
+    if (h->batch != b) {
+        set_error("vca_ca_batch_remove: the handle is not in this batch");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(b->device));
+    for (size_t i = 0; i < b->early.size(); ++i)
+        if (b->early[i] == h) {
+            b->early.erase(b->early.begin() + (long)i);
+            h->batch = nullptr;
+            return VCA_OK;
+        }
+    if (vca_status s = batch_detach(b, h, nullptr)) return s;
+    return sync_ctrl(h);  // steps and stop of the member as it left
+}
+
+vca_status vca_ca_batch_info(vca_ca_batch* b, uint64_t* graphs, uint64_t* launches, int* members) {
+    if (vca_status s = batch_check(b)) return s;
+    if (graphs) *graphs = b->graphs;
+    if (launches) *launches = b->launches;
+    if (members) {
+        int n = 0;
+        for (vca_ca* h : b->slots) n += h != nullptr;
+        *members = n;
+    }
+    return VCA_OK;
+}
+
+void vca_ca_batch_destroy(vca_ca_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    std::vector<vca_ca*> left;
+    for (vca_ca* h : b->slots)
+        if (h) {
+            batch_detach(b, h, nullptr);
+            left.push_back(h);
+        }
+    for (vca_ca* h : b->early) h->batch = nullptr;
+    for (vca_ca* h : b->done) h->batch = nullptr;
+    cudaStreamSynchronize(b->stream);
+    for (vca_ca* h : left) sync_ctrl(h);  // steps and stop of each member as it left
+    batch_free(b);
+    delete b;
+}
+
+}  // extern "C"

@@ -178,5 +178,5 @@ bool build_nb(int kind, int nx, int ny, int nz, NbTable& t) {
 
 extern "C" {
 const char* vca_last_error(void) { return vca::g_last_error.c_str(); }
-const char* vca_version(void) { return "vca 1 sm_100a (lava CA + Potts checkerboard MC)"; }
+const char* vca_version(void) { return "vca 2 sm_100a (lava CA + Potts checkerboard MC)"; }
 }

@@ -220,6 +220,21 @@ Config Config::load(const std::string& path, const std::vector<std::string>& ove
     return c;
 }
 
+Config Config::load_object(const Json& file, const std::string& source_path, const std::vector<std::string>& overrides) {
+    Json j = defaults_json();
+    if (!file.is_object()) throw ConfigError("Plik konfiguracyjny " + source_path + " musi zawierać obiekt JSON { ... }");
+    merge(j, file, "");
+    bool space_given = file.contains("space");
+    for (const std::string& o : overrides) {
+        apply_override(j, o);
+        space_given = space_given || o.rfind("space", 0) == 0;
+    }
+    Config c = from_json(j);
+    c.source_path = source_path;
+    c.space_from_user = space_given;
+    return c;
+}
+
 // Validation in the order of Config::fromJson (engine/src/io/Config.cpp:268-437).
 Config Config::from_json(const Json& j) {
     Config c;

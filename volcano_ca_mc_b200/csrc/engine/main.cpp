@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "job.hpp"
 #include "model.hpp"
 #include "vca.h"
 
@@ -32,8 +33,6 @@ namespace eng {
 
 namespace fs = std::filesystem;
 
-using Clock = std::chrono::steady_clock;
-double ms_since(Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
 
 void vcheck(vca_status s, const char* what) {
     if (s != VCA_OK) {
@@ -42,10 +41,6 @@ void vcheck(vca_status s, const char* what) {
     }
 }
 
-double round_to(double v, int decimals) {
-    const double f = std::pow(10.0, decimals);
-    return std::round(v * f) / f;
-}
 std::string fixed(double v, int decimals) {
     char buf[64];
     std::snprintf(buf, sizeof(buf), "%.*f", decimals, v);
@@ -65,72 +60,17 @@ const char* stop_text(int s) {
     return "?";
 }
 
-// ---------------------------------------------------------------------------------------------
-// times.json (engine/src/io/TimingReport.cpp:140-157): sections in ms (summed), then info.
-// ---------------------------------------------------------------------------------------------
-struct Timing {
-    std::vector<std::pair<std::string, double>> sections;
-    Json info = Json::object();
-    std::vector<std::pair<std::string, double>> files;
-    std::vector<std::pair<std::string, double>> details;
-    bool detail = false;
-    void add(const std::string& name, double ms) {
-        for (auto& s : sections)
-            if (s.first == name) {
-                s.second += ms;
-                return;
-            }
-        sections.emplace_back(name, ms);
-    }
-    void add_detail(const std::string& name, double ms) { details.emplace_back(name, ms); }
-    void add_file(const std::string& path, double ms) { files.emplace_back(path, ms); }
-    void set(const std::string& k, Json v) { info[k] = std::move(v); }
-    Json to_json() const {
-        Json j = Json::object();
-        j["unit"] = "ms";
-        for (const auto& s : sections) j[s.first] = round_to(s.second, 3);
-        for (const auto& kv : info.members()) j[kv.first] = kv.second;
-        if (detail) {
-            Json d = Json::object();
-            d["unit"] = "ms";
-            for (const auto& x : details) d[x.first] = round_to(x.second, 3);
-            j["detail"] = d;
-        }
-        return j;
-    }
-    void record_files() {
-        Json f = Json::object();
-        for (const auto& r : files) {
-            std::error_code ec;
-            const uint64_t bytes = fs::is_regular_file(r.first, ec) ? (uint64_t)fs::file_size(r.first, ec) : 0;
-            Json e = Json::object();
-            e["bytes"] = (unsigned long long)bytes;
-            e["writeMs"] = round_to(r.second, 3);
-            f[fs::path(r.first).filename().string()] = e;
-        }
-        set("files", f);
-    }
-};
 
-// PROGRESS lines for a parent process (engine/src/app/Progress.hpp:20-54).
-struct Progress {
-    bool on = false;
-    Clock::time_point last = Clock::now() - std::chrono::hours(1);
-    void report(const char* stage, long long done, long long total, bool force = false, const char* key = nullptr,
-                uint64_t value = 0) {
-        if (!on || (!force && ms_since(last) < 500.0)) return;
-        std::cout << "PROGRESS " << stage << ' ' << done << '/' << total;
-        if (key) std::cout << ' ' << key << '=' << value;
-        std::cout << '\n' << std::flush;
-        last = Clock::now();
-    }
-};
 
 struct CliOptions {
     std::string config, out, mc_from, batch;
     std::vector<std::string> overrides;
     bool help = false, print_defaults = false, validate = false, progress = false, timing_detail = false,
          thread_stats = false, benchmark = false;
+    // the job server (no counterpart in the reference's command line)
+    bool serve = false, serve_batch = true;
+    int slots = 16;
+    double budget_gb = 120.0;
 };
 
 // Cli::parse (engine/src/app/Cli.cpp:36-131).
@@ -165,8 +105,26 @@ CliOptions parse_cli(int argc, char** argv) {
         else if (a == "--print-defaults") o.print_defaults = true;
         else if (a == "--validate") o.validate = true;
         else if (a == "--progress") o.progress = true;
-        else throw CliError("unknown argument: " + a + " (see --help)");
+        else if (a == "--serve") o.serve = true;
+        else if (a == "--no-batch") o.serve_batch = false;
+        else if (a == "--slots") {
+            const std::string n = need(i, a);
+            if (n.empty() || n.find_first_not_of("0123456789") != std::string::npos || std::atoi(n.c_str()) < 1)
+                throw CliError("option --slots needs an integer >= 1, given: " + n);
+            o.slots = std::atoi(n.c_str());
+        } else if (a == "--budget-gb") {
+            const std::string n = need(i, a);
+            char* end = nullptr;
+            o.budget_gb = std::strtod(n.c_str(), &end);
+            if (n.empty() || *end != '\0' || !(o.budget_gb > 0.0))
+                throw CliError("option --budget-gb needs a number > 0, given: " + n);
+        } else throw CliError("unknown argument: " + a + " (see --help)");
     }
+    if (o.serve && (o.print_defaults || o.validate || o.benchmark || !o.config.empty() || !o.out.empty() ||
+                    !o.mc_from.empty() || !o.batch.empty() || !o.overrides.empty()))
+        throw CliError("--serve reads its jobs from standard input and takes only --slots, --budget-gb and --no-batch");
+    if (!o.serve && (o.slots != 16 || o.budget_gb != 120.0 || !o.serve_batch))
+        throw CliError("--slots, --budget-gb and --no-batch belong to --serve");
     if (o.print_defaults && (o.validate || o.benchmark || o.progress || o.timing_detail || o.thread_stats ||
                              !o.config.empty() || !o.out.empty() || !o.mc_from.empty() || !o.batch.empty() ||
                              !o.overrides.empty()))
@@ -194,6 +152,7 @@ std::string usage() {
            "  engine --mc-from <ca_result_folder> --config <mc.json> --out <folder> [--set key=value]... [--progress]\n"
            "  engine --batch <config_folder> --out <results_folder> [--set key=value]... [--progress]\n"
            "  engine --validate [--config <file.json>] [--set key=value]... [--mc-from <folder>]\n"
+           "  engine --serve [--slots N] [--budget-gb G] [--no-batch]   (jobs as JSON lines on stdin)\n"
            "  engine --print-defaults\n"
            "  engine --help\n"
            "\n"
@@ -212,14 +171,6 @@ int device_ordinal() {
 // ---------------------------------------------------------------------------------------------
 // CA stage (Simulation::runWith, engine/src/app/Simulation.cpp:158-292)
 // ---------------------------------------------------------------------------------------------
-struct RunSummary {
-    bool ca_ran = true;
-    int steps = 0;
-    int stop = 0;
-    std::vector<uint64_t> active, changed;
-    Microstructure result;
-    std::vector<Vent> vents;
-};
 
 std::string resolve_terrain_file(const Config& c) {
     const fs::path p(c.terrain.file);
@@ -273,14 +224,24 @@ Microstructure download(vca_ca* ca, const Dims& d) {
 
 struct CaHandle {
     vca_ca* h = nullptr;
-    ~CaHandle() { vca_ca_destroy(h); }
+    bool owned = true;  // a resident handle of the job server belongs to the server
+    ~CaHandle() {
+        if (owned) vca_ca_destroy(h);
+    }
 };
 
-RunSummary run_ca(const Config& cfg, const std::string& out_dir, Timing& timing, Progress& progress, CaHandle& ca) {
+RunSummary run_ca(const Config& cfg, const std::string& out_dir, Timing& timing, Progress& progress, CaHandle& ca,
+                  const RunHandles& res) {
     RunSummary s;
     auto t = Clock::now();
     const vca_ca_desc d = ca_desc(cfg);
-    vcheck(vca_ca_create(&d, &ca.h), "vca_ca_create");
+    if (res.ca) {  // a resident handle takes this job's space and parameters without allocating
+        ca.h = res.ca;
+        ca.owned = false;
+        vcheck(vca_ca_reconfigure(ca.h, &d), "vca_ca_reconfigure");
+    } else {
+        vcheck(vca_ca_create(&d, &ca.h), "vca_ca_create");
+    }
     timing.add("allocate", ms_since(t));
 
     t = Clock::now();
@@ -299,7 +260,10 @@ RunSummary run_ca(const Config& cfg, const std::string& out_dir, Timing& timing,
     vca_ca_info info{};
     if (every <= 0 && !progress.on) {
         t = Clock::now();
-        vcheck(vca_ca_run(ca.h), "vca_ca_run");
+        if (res.ca_run)
+            res.ca_run(ca.h);
+        else
+            vcheck(vca_ca_run(ca.h), "vca_ca_run");
         timing.add("caSim", ms_since(t));
     } else {
         // step by step: snapshots step_<k>.bin (Simulation.cpp:212-243) and/or progress lines
@@ -351,6 +315,10 @@ RunSummary run_ca(const Config& cfg, const std::string& out_dir, Timing& timing,
     s.changed.resize((size_t)s.steps);
     s.result = download(ca.h, cfg.space);
     const fs::path out(out_dir);
+    if (out_dir.empty()) {  // job server without an output folder: the results leave as digests
+        timing.add("save", ms_since(t));
+        return s;
+    }
     if (cfg.output.format == OutputFormat::Txt || cfg.output.format == OutputFormat::Both) {
         const auto tf = Clock::now();
         write_ca_txt((out / "ca_result.txt").string(), s.result);
@@ -439,22 +407,7 @@ Json parallel_json(const Config& c) {
 // ---------------------------------------------------------------------------------------------
 enum class Cooling { None, SolidOnly, Full };
 
-struct McStats {
-    int mcs = 0;
-    uint64_t grains = 0;
-    double mean = 0.0, energy = 0.0, accept_rate = 0.0;
-};
 
-struct McSummary {
-    bool full = false;
-    int mcs = 0, Q = 0;
-    uint64_t domain_cells = 0;
-    bool mobility_used = false;
-    std::vector<std::string> warnings;
-    std::vector<McStats> history;
-    Json stats;
-    CrystalMap crystals;
-};
 
 struct ClassGrains {
     uint64_t grains = 0, cells = 0, largest = 0;
@@ -514,13 +467,16 @@ std::vector<float> mobility_host(const Microstructure& m, const std::vector<uint
 
 struct McHandle {
     vca_mc* h = nullptr;
-    ~McHandle() { vca_mc_destroy(h); }
+    bool owned = true;
+    ~McHandle() {
+        if (owned) vca_mc_destroy(h);
+    }
 };
 
 // ca: the CA handle of an in-memory run (domain and mobility built on the device) or null;
-// file: the CA result read for --mc-from, or null.
+// file: the CA result read for --mc-from, or null; resident: the job server's MC handle, or null.
 McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cooling cooling, Timing& timing,
-                 Progress& progress, const std::string& out_dir) {
+                 Progress& progress, const std::string& out_dir, vca_mc* resident) {
     McSummary s;
     const bool full = ca == nullptr && file == nullptr;
     s.full = full;
@@ -541,7 +497,13 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     d.kT = cfg.mc.kT;
     d.device = device_ordinal();
     McHandle mc;
-    vcheck(vca_mc_create(&d, &mc.h), "vca_mc_create");
+    if (resident) {
+        mc.h = resident;
+        mc.owned = false;
+        vcheck(vca_mc_reconfigure(mc.h, &d), "vca_mc_reconfigure");
+    } else {
+        vcheck(vca_mc_create(&d, &mc.h), "vca_mc_create");
+    }
     timing.add_detail("mcCreate", ms_since(t));
     auto td = Clock::now();
     bool have_mobility = false;  // mobility values held by the handle: the byMobility classes exist
@@ -764,11 +726,6 @@ void env_info(Timing& timing) {
     timing.set("gpuLibrary", vca_version());
 }
 
-// Resident set of this process from /proc/self/status (VmRSS, VmHWM), bytes.
-struct Rss {
-    uint64_t current = 0, peak = 0;
-    bool ok = false;
-};
 Rss read_rss() {
     Rss r;
     std::ifstream in("/proc/self/status");
@@ -795,6 +752,78 @@ void memory_info(Timing& timing, const Rss& start) {
         m["peakRssBytes"] = (unsigned long long)now.peak;
     }
     timing.set("memory", m);
+}
+
+// The CA stage, its statistics, the MC stage and every result file of one job (the run of
+// Simulation::runFromCli, Simulation.cpp:526-683, after the config is read).  With an empty out_dir
+// nothing is written: the job server hands the results on as digests.
+JobOutcome run_job(const Config& cfg, const std::string& out_dir, Timing& timing, Progress& progress,
+                   const RunHandles& res, Clock::time_point start, const Rss& rss_start) {
+    JobOutcome job;
+    const bool files = !out_dir.empty();
+    const fs::path out(out_dir);
+    auto t = Clock::now();
+    if (files) {
+        write_json((out / "config_used.json").string(), cfg.effective);
+        timing.add_file((out / "config_used.json").string(), ms_since(t));
+    }
+    RunSummary& s = job.ca;
+    s.ca_ran = !cfg.mc.full_only();
+    CaHandle ca;
+    Json stats = Json::object();
+    if (s.ca_ran) {
+        s = run_ca(cfg, out_dir, timing, progress, ca, res);
+        s.ca_ran = true;
+        t = Clock::now();
+        stats = ca_stats(cfg, s, ca.h);
+        timing.add("caStats", ms_since(t));
+        if (res.ca_done) res.ca_done();
+    }
+    stats["parallel"] = parallel_json(cfg);
+    McSummary& mc = job.mc;
+    job.mc_ran = cfg.mc.enabled;
+    if (job.mc_ran) {
+        mc = run_mc(cfg, s.ca_ran ? ca.h : nullptr, nullptr, Cooling::Full, timing, progress, out_dir, res.mc);
+        progress.report("save", 0, 1, true);
+        if (files) save_mc(cfg, mc, out_dir, timing);
+        stats["mc"] = mc.stats;
+    }
+    job.stats = stats;
+    t = Clock::now();
+    if (files) {
+        write_json((out / "stats.json").string(), stats);
+        timing.add_file((out / "stats.json").string(), ms_since(t));
+    }
+    timing.add(job.mc_ran ? "mcSave" : "save", ms_since(t));
+    timing.add("total", ms_since(start));
+    timing.set("cells", (unsigned long long)cfg.space.cells());
+    Json sp = Json::array();
+    sp.push_back(cfg.space.nx);
+    sp.push_back(cfg.space.ny);
+    sp.push_back(cfg.space.nz);
+    timing.set("space", sp);
+    timing.set("neighborhood", nb_name(cfg.neighborhood));
+    timing.set("boundary", bc_name(cfg.boundary));
+    if (s.ca_ran) {
+        timing.set("steps", s.steps);
+        timing.set("grid", cfg.grid);
+        timing.set("mode", mode_name(cfg.ca.mode));
+        timing.set("stopReason", stop_text(s.stop));
+    } else {
+        timing.set("mode", "mc_full");
+    }
+    if (job.mc_ran) {
+        timing.set("mcDomain", mc.full ? "full" : "basalt");
+        timing.set("mcs", mc.mcs);
+        timing.set("domainCells", (unsigned long long)mc.domain_cells);
+        timing.set("Q", mc.Q);
+        timing.set("mcMobility", mc.mobility_used);
+    }
+    env_info(timing);
+    memory_info(timing, rss_start);
+    timing.record_files();
+    if (files) write_json((out / "times.json").string(), timing.to_json());
+    return job;
 }
 
 int run_from_cli(const CliOptions& opt, Clock::time_point start) {
@@ -866,7 +895,7 @@ int run_from_cli(const CliOptions& opt, Clock::time_point start) {
         write_json((out / "config_used.json").string(), cfg.effective);
         timing.add_file((out / "config_used.json").string(), ms_since(t));
         const Cooling cooling = src.has_arrival ? Cooling::Full : src.has_solid ? Cooling::SolidOnly : Cooling::None;
-        McSummary mc = run_mc(cfg, nullptr, &ca, cooling, timing, progress, out_dir);
+        McSummary mc = run_mc(cfg, nullptr, &ca, cooling, timing, progress, out_dir, nullptr);
         mc.warnings.insert(mc.warnings.begin(), warnings.begin(), warnings.end());
         progress.report("save", 0, 1, true);
         save_mc(cfg, mc, out_dir, timing);
@@ -901,49 +930,11 @@ int run_from_cli(const CliOptions& opt, Clock::time_point start) {
         return kExitOk;
     }
 
-    t = Clock::now();
-    write_json((out / "config_used.json").string(), cfg.effective);
-    timing.add_file((out / "config_used.json").string(), ms_since(t));
-    RunSummary s;
-    s.ca_ran = !cfg.mc.full_only();
-    CaHandle ca;
-    Json stats = Json::object();
-    if (s.ca_ran) {
-        s = run_ca(cfg, out_dir, timing, progress, ca);
-        s.ca_ran = true;
-        t = Clock::now();
-        stats = ca_stats(cfg, s, ca.h);
-        timing.add("caStats", ms_since(t));
-    }
-    stats["parallel"] = parallel_json(cfg);
-    McSummary mc;
-    const bool mc_ran = cfg.mc.enabled;
-    if (mc_ran) {
-        mc = run_mc(cfg, s.ca_ran ? ca.h : nullptr, nullptr, Cooling::Full, timing, progress, out_dir);
-        progress.report("save", 0, 1, true);
-        save_mc(cfg, mc, out_dir, timing);
-        stats["mc"] = mc.stats;
-    }
-    t = Clock::now();
-    write_json((out / "stats.json").string(), stats);
-    timing.add_file((out / "stats.json").string(), ms_since(t));
-    timing.add(mc_ran ? "mcSave" : "save", ms_since(t));
-    timing.add("total", ms_since(start));
-    common(cfg, cfg.space);
-    if (s.ca_ran) {
-        timing.set("steps", s.steps);
-        timing.set("grid", cfg.grid);
-        timing.set("mode", mode_name(cfg.ca.mode));
-        timing.set("stopReason", stop_text(s.stop));
-    } else {
-        timing.set("mode", "mc_full");
-    }
-    if (mc_ran) mc_info(mc);
-    env_info(timing);
-    memory_info(timing, rss_start);
-    timing.record_files();
-    write_json((out / "times.json").string(), timing.to_json());
-    for (const std::string& w : mc.warnings) std::cerr << "Ostrzeżenie: " << w << '\n';
+    JobOutcome job = run_job(cfg, out_dir, timing, progress, RunHandles{}, start, rss_start);
+    for (const std::string& w : job.mc.warnings) std::cerr << "Ostrzeżenie: " << w << '\n';
+    const RunSummary& s = job.ca;
+    const McSummary& mc = job.mc;
+    const bool mc_ran = job.mc_ran;
 
     std::ostringstream os;
     os << "=== Simulation done ===\n";
@@ -1196,6 +1187,7 @@ int main(int argc, char** argv) {
         }
         if (opt.validate) return validate(opt);
         if (!opt.batch.empty()) return run_batch(opt);
+        if (opt.serve) return run_server(opt.slots, opt.budget_gb, opt.serve_batch);
         return run_from_cli(opt, start);
     } catch (const CliError& e) {
         std::cerr << "Błąd argumentów: " << e.what() << "\n\n" << usage();

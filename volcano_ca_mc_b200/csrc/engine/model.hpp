@@ -131,6 +131,9 @@ struct Config {
 
     static Json defaults_json();
     static Config load(const std::string& path, const std::vector<std::string>& overrides);
+    // the same merge and validation for a config object already in memory (the job server's requests);
+    // source_path resolves a relative terrain.file
+    static Config load_object(const Json& file, const std::string& source_path, const std::vector<std::string>& overrides);
     static Config from_json(const Json& j);
     std::vector<std::pair<int, int>> vent_columns() const;
 };

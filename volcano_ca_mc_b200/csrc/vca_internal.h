@@ -54,6 +54,7 @@ struct CaGeom {
     int P;                    // row pitch in cells
     int per[3];               // periodic axes (Boundary, engine/src/core/Boundary.cpp:5-11)
     int TY, TZ;               // tile rows: TY * TZ = 16, tile = 64 x TY x TZ cells
+    int shape;                // shared-memory family of the rules pass for this tile (0, 1, 2)
     int tiles_x, tiles_y, tiles_z;
     FastDiv32 div_tx, div_ty;  // / tiles_x and / tiles_y (tile id -> tile coordinates)
 };
@@ -77,8 +78,9 @@ struct CaTensorMaps {
     CUtensorMap xside_type[2], xside_drop;
 };
 
+// Everything a step kernel needs besides the tensor maps (those are a separate kernel parameter, so
+// that a batched launch can copy the rest of a grid's arguments into shared memory).
 struct CaKernelArgs {
-    CaTensorMaps tm;
     CaGeom g;
     int classic;
     int ponding;
@@ -111,6 +113,11 @@ struct CaKernelArgs {
     unsigned long long* hist_active;
     unsigned long long* hist_changed;
     uint64_t ntiles;
+    // z slab of a taller grid (vca_ca_set_slab): globalIndex = local index + gidx_base; the counts of
+    // a step cover the owned layers [own_z0, own_z1) only; the caller decides the stop
+    uint64_t gidx_base;
+    int own_z0, own_z1;
+    int slab;
 };
 
 // Read-only view of a CA handle's current planes (the MC domain and mobility are built from it).
@@ -140,7 +147,8 @@ struct CaSizes {
 struct vca_ca {
     vca::CaTensorMaps tmaps;  // first member: CUtensorMap needs 64-byte alignment
     vca::CaSizes cap;         // what the device buffers can hold
-    int sms = 0, rules_per_sm = 0, cand_per_sm = 0;
+    int sms = 0, cand_per_sm = 0;
+    int rules_per_sm[3] = {0, 0, 0};  // resident rules blocks per SM of each shape family
     size_t vent_cap = 0, seed_cap = 0;
     vca_ca_desc desc;
     vca::CaGeom geom;
@@ -191,8 +199,14 @@ struct vca_ca {
     int profile_kernels = 0;  // bracket each rules launch with events (set by VCA_PROFILE_KERNELS=1)
     std::vector<cudaEvent_t> prof_events;
     cudaGraphExec_t graph_exec = nullptr;   // kGraphSteps steps of launches
-    vca::CaKernelArgs graph_args;            // the arguments and grids graph_exec was captured with
+    vca::CaKernelArgs graph_args;            // the arguments, maps and grids graph_exec was captured with
+    vca::CaTensorMaps graph_tm;
     int graph_grid = 0, graph_cand = 0;
     vca::CaCtrl* ctrl_ring = nullptr;       // pinned: two in-flight copies of the control block
     cudaEvent_t ring_ev[2] = {nullptr, nullptr};
+    vca_ca_batch* batch = nullptr;          // the batch stepping this handle, if any (vca_ca_batch_add)
+    int batch_slot = -1;
+    // z slab of a taller grid (vca_ca_set_slab); slab_z0 = global z of local layer 0
+    bool slab = false;
+    int slab_z0 = 0, own_z0 = 0, own_z1 = 0;
 };

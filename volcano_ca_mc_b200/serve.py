@@ -1,21 +1,21 @@
-"""Batched and served execution of many independent lava CA + Potts MC jobs on one GPU.
+"""Batched and served execution of many independent lava CA + Potts MC jobs on one GPU, through the
+job server of the engine command (``engine --serve``, volcano_ca_mc_b200/csrc/engine/serve.cpp).
 
 The reference runs one job per engine process (its batch runner starts the engine once per config,
-engine/src/app/Batch.cpp:147-246; its GUI queues jobs one after the other).  Here a job server keeps
-a fixed number of worker slots, each with a resident CA handle and a resident MC handle on its own
-CUDA streams, sized once for the largest job of the mix:
+engine/src/app/Batch.cpp:147-246; its GUI queue, gui/jobs.py, starts one job after another).  Here
+the jobs are engine configs in the reference's schema, sent to one server process as they arrive:
 
-* a job is admitted when a slot is free and the device bytes of the running jobs plus its own
-  (``vca_ca_footprint`` + ``vca_mc_footprint``) stay within the HBM budget;
-* an admitted job reconfigures its slot's handles to its space and parameters
-  (``vca_ca_reconfigure`` / ``vca_mc_reconfigure``: no allocation), runs the CA to its stop rule,
-  crystallises the basalt, computes the grain statistics on the device and returns its planes;
-* jobs that arrive while others run are admitted as slots free up, so the short, latency-bound
-  launches of many small grids overlap on the GPU (continuous batching).
+* each job is a config object (space, boundary, neighbourhood, seed, a CSV heightmap of Gaussian
+  cones with value noise, vents at given columns, ca.* and mc.* parameters) with ``output.format``
+  none: the server answers with digests of its ca_result.bin / mc_result.bin bytes;
+* the server admits a job when a worker is free and its resident device handles fit the HBM budget,
+  steps the CA grids of all running jobs together in one batch, and runs each job's MC stage and
+  statistics on the worker's own streams;
+* ``run(..., slots=1, batched=False)`` is the one-at-a-time plain GPU path on the same trace
+  (vca_ca_run per job, no overlap), the baseline of the jobs/s and latency figures.
 
-``run(jobs, slots=1)`` is the one-at-a-time baseline on the same trace.  Every job's result is a
-pure function of its spec, so a job's result hash is the same alone and in the mix (checked by
-``compare``).
+Every job's result is a pure function of its config, so its digests are the same alone and in the
+mix (``compare``).
 
 The mixes follow the batched/served benchmark definitions: 2D x-z sections with sides drawn
 log-uniformly from 128 to 2048, 3D grids with sides from 64 to 256 and z = side / 2, all four
@@ -24,8 +24,10 @@ neighbourhoods (hexagonal in 2D only), both boundaries, 1-8 vents on Gaussian-co
 """
 from __future__ import annotations
 
-import hashlib
-import queue
+import json
+import os
+import subprocess
+import tempfile
 import threading
 import time
 from dataclasses import dataclass, field
@@ -96,11 +98,36 @@ class JobSpec:
                 used.add((vx, vy))
                 vents.append((vx, vy, int(hm[vy, vx]), i + 1))
             vents = [v for v in vents if v[2] < nz]
+            if not vents:  # every pick landed on a full column: the lowest column instead
+                y0, x0 = np.unravel_index(int(np.argmin(hm)), hm.shape)
+                vents = [(int(x0), int(y0), int(hm[y0, x0]), 1)]
             self._terrain = (heights, vents)
         return self._terrain
 
     def footprint(self) -> int:
         return capi.ca_footprint(self.ca_params()) + capi.mc_footprint(self.mc_params())
+
+    def config(self, folder: str) -> dict:
+        """The job as an engine config in the reference's schema (engine/src/io/Config.cpp:153-176):
+        its heightmap written as a CSV file into folder (terrain.type = "file"), vents at its columns."""
+        heights, vents = self.terrain()
+        csv = os.path.join(folder, f"job{self.job_id}_heightmap.csv")
+        if not os.path.exists(csv):
+            with open(csv, "w") as f:
+                for row in heights.reshape(self.ny, self.nx):
+                    f.write(",".join(str(int(v)) for v in row) + "\n")
+        return {
+            "space": {"nx": self.nx, "ny": self.ny, "nz": self.nz}, "boundary": self.boundary,
+            "neighborhood": self.neighborhood, "rngSeed": self.seed,
+            "terrain": {"type": "file", "file": csv},
+            "vents": {"count": len(vents), "placement": "positions", "positions": [[v[0], v[1]] for v in vents],
+                      "eruptionSteps": self.max_steps // 2, "eruptTemp": 1200},
+            "ca": {"mode": "lava", "maxSteps": self.max_steps, "coolingAmbient": 2.0, "coolingLateral": 4.0,
+                   "coolingFall": 2.0, "solidusTemp": 800, "ponding": True, "sweep": "front"},
+            "mc": {"enabled": True, "domain": "basalt", "Q": self.Q, "mcs": self.mcs, "J": 1.0, "kT": self.kT,
+                   "mobilityFromCooling": True, "statsEvery": max(1, self.mcs), "update": "checkerboard"},
+            "output": {"format": "none"},
+        }
 
 
 def make_mix(n: int, master_seed: int, share_3d: float = 0.3, rate_hz: float | None = None, side_2d=(128, 2048),
@@ -131,176 +158,92 @@ def make_mix(n: int, master_seed: int, share_3d: float = 0.3, rate_hz: float | N
     return jobs
 
 
-class ResultBuffers:
-    """Pinned host buffers that jobs' results are downloaded into and handed to the consumer in.
-    A slot takes a free buffer set for each job and is released as soon as the result is in it; the
-    consumer (here the result hash) returns the set when it is done, so a slow consumer holds back
-    new jobs only when every set is taken."""
 
-    def __init__(self, cap_cells: int, count: int):
-        import torch
-        pin = lambda dt: torch.empty(cap_cells, dtype=dt, pin_memory=True).numpy()
-        self.free: queue.Queue = queue.Queue()
-        for _ in range(count):
-            self.free.put((pin(torch.uint8), pin(torch.int32), pin(torch.float32), pin(torch.int16).view("uint16"),
-                           pin(torch.int16).view("uint16"), pin(torch.int32)))
+class EngineServer:
+    """One ``engine --serve`` process: requests go to its standard input as JSON lines, its answers
+    are collected by a reader thread."""
 
-    def get(self):
-        return self.free.get()
+    def __init__(self, slots: int = 16, batched: bool = True, budget_gb: float = 120.0, device: int = 0):
+        args = [capi.ENGINE_PATH, "--serve", "--slots", str(slots), "--budget-gb", f"{budget_gb:g}"]
+        if not batched:
+            args.append("--no-batch")
+        if not os.path.exists(capi.ENGINE_PATH):
+            raise capi.VcaError(f"{capi.ENGINE_PATH} is missing: the engine has not been built")
+        self.proc = subprocess.Popen(args, stdin=subprocess.PIPE, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                     text=True, bufsize=1, env=dict(os.environ, VCA_DEVICE=str(device)))
+        self.answers: dict[str, dict] = {}
+        self.summary: dict | None = None
+        self._err: list[str] = []
+        self._reader = threading.Thread(target=self._read, daemon=True)
+        self._reader.start()
+        self._err_reader = threading.Thread(target=lambda: self._err.extend(self.proc.stderr), daemon=True)
+        self._err_reader.start()
 
-    def put(self, bufs):
-        self.free.put(bufs)
+    def _read(self):
+        for line in self.proc.stdout:
+            d = json.loads(line)
+            if "summary" in d:
+                self.summary = d["summary"]
+            else:
+                self.answers[str(d["id"])] = d
 
+    def submit(self, request: dict) -> None:
+        self.proc.stdin.write(json.dumps(request) + "\n")
+        self.proc.stdin.flush()
 
-class Slot:
-    """A worker's resident CA and MC handles, sized for the largest job it may get."""
+    def close(self, timeout: float = 3600.0) -> int:
+        self.proc.stdin.close()
+        rc = self.proc.wait(timeout=timeout)
+        self._reader.join(timeout=10)
+        self._err_reader.join(timeout=10)
+        return rc
 
-    def __init__(self, cap: JobSpec, device: int):
-        self.device = device
-        self.ca = capi.LavaCA(cap.ca_params(device))
-        self.mc = capi.PottsMC(cap.mc_params(device))
-        # one small job first: the handles' set-up buffers are allocated on first use, sized for the
-        # capacity, so no job of the trace waits on a device-wide allocation
-        three_d = cap.ny > 1
-        self.run(JobSpec(job_id=-2, nx=32 if three_d else 64, ny=32 if three_d else 1, nz=16 if three_d else 64,
-                         neighborhood="moore", boundary="absorbing", seed=1, max_steps=8, n_vents=1, Q=32, kT=0.0,
-                         mcs=1))
-
-    def run(self, job: JobSpec, bufs=None) -> tuple[dict, tuple]:
-        """Runs the job; returns its record and its result arrays (the five CA planes and the crystal
-        orientations, views of ``bufs`` when given)."""
-        t = [time.perf_counter()]
-        heights, vents = job.terrain()
-        self.ca.reconfigure(job.ca_params(self.device))
-        self.ca.apply_terrain(heights)
-        self.ca.place_seeds(vents)
-        t.append(time.perf_counter())
-        self.ca.run()
-        info = self.ca.info()
-        lava, basalt, reach2 = self.ca.flow_stats(len(vents))
-        t.append(time.perf_counter())
-        n = job.cells
-        planes = self.ca.download(None if bufs is None else tuple(a[:n] for a in bufs[:5]))
-        t.append(time.perf_counter())
-        self.mc.reconfigure(job.mc_params(self.device))
-        self.mc.set_domain_from_ca(self.ca)
-        self.mc.set_mobility_from_ca(self.ca, 0.05, True)
-        self.mc.initialize()
-        self.mc.sweep(job.mcs)
-        g = self.mc.grains(moore=job.neighborhood != "von_neumann")
-        crystals = self.mc.crystals(None if bufs is None else bufs[5][:n])
-        mi = self.mc.info()
-        energy = self.mc.energy()
-        t.append(time.perf_counter())
-        rec = {"job": job.job_id, "steps": info.steps, "stop": info.stop_reason, "energy": energy, "grains": g.grains,
-               "lava_volume": int(lava.sum() + basalt.sum()), "max_reach": round(float(np.sqrt(reach2.max())), 2),
-               "attempts": mi.attempts, "cell_updates": job.cells * info.steps, "done": t[-1],
-               "phases_ms": {k: round((t[i + 1] - t[i]) * 1e3, 3)
-                             for i, k in enumerate(("setup", "ca", "download", "mc"))}}
-        return rec, (*planes, crystals)
-
-    def close(self):
-        self.mc.close()
-        self.ca.close()
+    def stderr(self) -> str:
+        return "".join(self._err)
 
 
-def result_hash(arrays) -> str:
-    h = hashlib.sha256()
-    for a in arrays:
-        h.update(memoryview(np.ascontiguousarray(a)).cast("B"))
-    return h.hexdigest()[:24]
-
-
-def capacity(jobs: list[JobSpec]) -> JobSpec:
-    """A spec whose handles hold every job of the list (all 2D or all 3D): the largest size on each
-    axis and the longest step history; the buffer sizes grow with each axis, so every job fits."""
-    return JobSpec(job_id=-1, nx=max(j.nx for j in jobs), ny=max(j.ny for j in jobs), nz=max(j.nz for j in jobs),
-                   neighborhood="moore", boundary="absorbing", seed=1, max_steps=65535, n_vents=1, Q=2, kT=0.0, mcs=0)
-
-
-def run(jobs: list[JobSpec], slots: int = 8, budget_bytes: int = 120 << 30, realtime: bool = False,
-        device: int = 0) -> dict:
-    """Run the jobs on `slots` workers with footprint admission; realtime replays the arrival times.
-    Returns per-job records (arrival, start, end in seconds from the trace start, result) and totals."""
-    by_dim = {"2d": [j for j in jobs if j.ny == 1], "3d": [j for j in jobs if j.ny > 1]}
-    caps = {k: capacity(v) for k, v in by_dim.items() if v}
-    per_slot = sum(capi.ca_footprint(c.ca_params()) + capi.mc_footprint(c.mc_params()) for c in caps.values())
-    slots = max(1, min(slots, budget_bytes // max(1, per_slot)))
-    pool: queue.Queue = queue.Queue()
-    for _ in range(slots):
-        pool.put({k: Slot(c, device) for k, c in caps.items()})
-    results = {k: ResultBuffers(c.cells, slots + 4) for k, c in caps.items()}
-    lock = threading.Condition()
-    in_use = [0]
-    records: dict[int, dict] = {}
-    errors: list[BaseException] = []
-    order = sorted(jobs, key=lambda j: j.arrival_s)
-    for j in order:  # host-side set-up outside the trace (terrain synthesis)
-        j.terrain()
-    t0 = time.perf_counter()
-
-    def worker(job: JobSpec, slot_set: dict, start: float, fp: int):
-        dim = "3d" if job.ny > 1 else "2d"
-        bufs = results[dim].get()
-        rec = None
-        try:
-            rec, arrays = slot_set[dim].run(job, bufs)
-        except BaseException as e:  # reported after the run
-            errors.append(e)
-        finally:  # the slot is free once the result is in host memory
-            pool.put(slot_set)
-            with lock:
-                in_use[0] -= fp
-                lock.notify_all()
-        try:  # the consumer: checks the result, then gives the buffers back
-            if rec is not None:
-                rec["sha"] = result_hash(arrays)
-                records[job.job_id] = {"arrival": job.arrival_s, "start": start, "end": rec.pop("done") - t0, **rec}
-        except BaseException as e:
-            errors.append(e)
-        finally:
-            results[dim].put(bufs)
-
-    threads = []
-    for job in order:
-        if realtime:
-            delay = job.arrival_s - (time.perf_counter() - t0)
-            if delay > 0:
-                time.sleep(delay)
-        fp = job.footprint()
-        slot_set = pool.get()  # a free slot
-        with lock:
-            while in_use[0] + fp > budget_bytes and in_use[0] > 0:
-                lock.wait(timeout=1.0)
-            in_use[0] += fp
-        th = threading.Thread(target=worker, args=(job, slot_set, time.perf_counter() - t0, fp), daemon=True)
-        th.start()
-        threads.append(th)
-    for th in threads:
-        th.join()
-    while not pool.empty():
-        for s in pool.get().values():
-            s.close()
-    if errors:
-        raise errors[0]
-    makespan = max((r["end"] for r in records.values()), default=0.0)  # the last result in host memory
-    lat = np.array([r["end"] - (r["arrival"] if realtime else 0.0) for r in records.values()])
-    busy = sum(r["end"] - r["start"] for r in records.values())
-    phases = {}
-    for r in records.values():
-        for k, v in r["phases_ms"].items():
-            phases[k] = phases.get(k, 0.0) + v
-    return {"records": records, "slots": slots, "makespan_s": makespan, "jobs": len(records),
-            "mean_concurrency": busy / makespan if makespan > 0 else 0.0,
-            "phase_ms_total": {k: round(v, 1) for k, v in phases.items()},
-            "jobs_per_s": len(records) / makespan if makespan > 0 else 0.0,
-            "cell_updates_per_s": sum(r["cell_updates"] for r in records.values()) / makespan if makespan > 0 else 0.0,
-            "p50_s": float(np.percentile(lat, 50)) if len(lat) else 0.0,
-            "p99_s": float(np.percentile(lat, 99)) if len(lat) else 0.0,
-            "per_slot_bytes": per_slot, "budget_bytes": budget_bytes}
+def run(jobs: list[JobSpec], slots: int = 16, batched: bool = True, budget_gb: float = 120.0, realtime: bool = False,
+        device: int = 0, folder: str | None = None) -> dict:
+    """Sends the jobs to a job server (at their arrival times when realtime, else all at once) and
+    returns per-job records and totals: jobs/s over the makespan (first arrival to last completion),
+    cell-updates/s, p50 / p99 of completion - arrival, mean concurrency."""
+    tmp = None
+    if folder is None:
+        tmp = tempfile.TemporaryDirectory(prefix="vca_serve_")
+        folder = tmp.name
+    try:
+        order = sorted(jobs, key=lambda j: j.arrival_s)
+        configs = {j.job_id: j.config(folder) for j in order}  # terrains and heightmaps before the trace
+        srv = EngineServer(slots=slots, batched=batched, budget_gb=budget_gb, device=device)
+        t0 = time.perf_counter()
+        for j in order:
+            if realtime:
+                delay = j.arrival_s - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            srv.submit({"id": str(j.job_id), "json": configs[j.job_id]})
+        rc = srv.close()
+        if rc != 0 or srv.summary is None:
+            raise RuntimeError(f"engine --serve ended with {rc}: {srv.stderr()[-2000:]} "
+                               f"{[a for a in srv.answers.values() if a.get('status') != 'ok'][:3]}")
+    finally:
+        if tmp is not None:
+            tmp.cleanup()
+    recs = {int(k): v for k, v in srv.answers.items()}
+    first = min(r["arrival_ms"] for r in recs.values())
+    last = max(r["done_ms"] for r in recs.values())
+    makespan = (last - first) / 1e3
+    lat = np.array([r["latency_ms"] / 1e3 for r in recs.values()])
+    busy = sum(r["done_ms"] - r["admitted_ms"] for r in recs.values()) / 1e3
+    return {"records": recs, "slots": slots, "batched": batched, "jobs": len(recs), "makespan_s": makespan,
+            "jobs_per_s": len(recs) / makespan if makespan > 0 else 0.0,
+            "cell_updates_per_s": sum(r["cell_updates"] for r in recs.values()) / makespan if makespan > 0 else 0.0,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_concurrency": busy / makespan if makespan > 0 else 0.0, "server": srv.summary}
 
 
 def compare(a: dict, b: dict) -> int:
-    """Number of jobs whose results differ between two runs of the same jobs."""
+    """Number of jobs whose results (digests of ca_result.bin and mc_result.bin) differ between two
+    runs of the same jobs."""
     ra, rb = a["records"], b["records"]
-    return sum(1 for k in ra if ra[k]["sha"] != rb.get(k, {}).get("sha"))
+    return sum(1 for k in ra if ra[k]["digest"] != rb.get(k, {}).get("digest"))

@@ -1,0 +1,190 @@
+"""Autotuner of the lava CA's launch shape: tile shape (64 x tile_y x tile_z cells, the z extent being
+the depth of a tile's z slab) and resident rules blocks per SM, per grid shape class and
+neighbourhood.
+
+The results of a run do not depend on the launch shape (every shape is bit-identical, see
+tests/test_ca_parity.py::test_tile_shapes_match_oracle); only its speed does.  The reference has no
+counterpart: its nearest knob is the OpenMP schedule and chunk of the CPU sweep
+(engine/src/parallel/Omp.hpp:438-501), fixed per run.
+
+A shape class is (dimensionality, neighbourhood, log2 of the cell count).  For each class the tuner
+times every candidate launch shape on a calibration job -- a seeded Gaussian-cone terrain of the
+class's size with a few vents, run for a fixed number of ACTIVE steps from the same start -- and
+keeps the fastest.  Cells per thread are fixed at 4 (one 32-bit byte window per thread in the rules
+pass), so they are not a tuned knob.
+
+    python -m volcano_ca_mc_b200.tuner --out volcano_ca_mc_b200/tuning.json   # on a GPU
+    tuner.lookup(params) -> (tile_y, tile_z, rules_blocks_per_sm) from the table (defaults if absent)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import capi
+
+TABLE_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
+TILES_3D = [(4, 4), (2, 8), (8, 2), (1, 16), (16, 1)]
+BLOCKS = [0, 2]  # 0: as many rules blocks per SM as fit
+
+
+def shape_class(nx: int, ny: int, nz: int, neighborhood: str) -> str:
+    dim = "3d" if (ny > 1 and nz > 1) else ("xz" if ny == 1 else "xy")
+    return f"{dim}-{neighborhood}-{int(round(math.log2(max(1, nx * ny * nz))))}"
+
+
+def candidates(nx: int, ny: int, nz: int) -> list[tuple[int, int, int]]:
+    tiles = TILES_3D if (ny > 1 and nz > 1) else [(0, 0)]
+    return [(ty, tz, b) for (ty, tz) in tiles for b in BLOCKS]
+
+
+def calibration_grid(cls: str) -> tuple[int, int, int]:
+    """A grid of the class's size: 3D sides with z = side / 2, 2D square sections."""
+    dim, _, lg = cls.rsplit("-", 2)[0], None, int(cls.rsplit("-", 1)[1])
+    cells = 2 ** lg
+    if dim == "3d":
+        side = max(16, int(round((2 * cells) ** (1 / 3))))
+        return side, side, max(8, side // 2)
+    side = max(16, int(round(math.sqrt(cells))))
+    return (side, 1, side) if dim == "xz" else (side, side, 1)
+
+
+def calibration_terrain(nx: int, ny: int, nz: int, seed: int = 11):
+    """A Gaussian cone (or two) with value noise, and 4 vents near the summit."""
+    from .workloads import _finish, value_noise
+    rng = np.random.default_rng(seed)
+    x = np.arange(nx)[None, :]
+    y = np.arange(ny)[:, None]
+    cx, cy = 0.5 * nx, (0.5 * ny if ny > 1 else 0.0)
+    sig = 0.25 * max(nx, ny)
+    h = 0.6 * nz * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * sig * sig)) + 0.02 * nz * value_noise(nx, ny, seed)
+    heights = _finish(h, nz)
+    hm = heights.reshape(ny, nx)
+    vents = []
+    for i in range(4):
+        vx = int(np.clip(cx + rng.normal(0, 2), 0, nx - 1))
+        vy = int(np.clip(cy + rng.normal(0, 2), 0, ny - 1)) if ny > 1 else 0
+        if hm[vy, vx] < nz and all((vx, vy) != v[:2] for v in vents):
+            vents.append((vx, vy, int(hm[vy, vx]), i + 1))
+    return heights, vents
+
+
+def time_candidate(nx, ny, nz, neighborhood, cand, steps, heights, vents, device=0, reps=2) -> float:
+    """Device time [ms] of `steps` ACTIVE steps of the calibration job with this launch shape (the best
+    of `reps` runs on one handle)."""
+    ty, tz, b = cand
+    p = capi.CaParams(nx, ny, nz, neighborhood=neighborhood, boundary="absorbing", seed=5, max_steps=steps,
+                      eruption_steps=steps, cooling_ambient=2.0, cooling_lateral=4.0, cooling_fall=2.0, device=device,
+                      tile_y=ty, tile_z=tz, rules_blocks_per_sm=b)
+    ca = capi.LavaCA(p)
+    best = float("inf")
+    for r in range(reps + 1):
+        if r:
+            ca.reset()
+        ca.apply_terrain(heights)
+        ca.place_seeds(vents)
+        t0 = ca.timing()[0]
+        ca.run()
+        ms = ca.timing()[0] - t0
+        if r:  # the first run warms the graph up
+            best = min(best, ms)
+    ca.close()
+    return best
+
+
+def tune_class(cls: str, steps: int = 96, device: int = 0) -> dict:
+    dim_nb = cls.rsplit("-", 1)[0]
+    neighborhood = dim_nb.split("-", 1)[1]
+    nx, ny, nz = calibration_grid(cls)
+    heights, vents = calibration_terrain(nx, ny, nz)
+    times = {}
+    for cand in candidates(nx, ny, nz):
+        times[f"{cand[0]}x{cand[1]}/b{cand[2]}"] = round(
+            time_candidate(nx, ny, nz, neighborhood, cand, steps, heights, vents, device), 4)
+    best = min(times, key=times.get)
+    tile, blocks = best.split("/b")
+    ty, tz = (int(v) for v in tile.split("x"))
+    return {"grid": [nx, ny, nz], "steps": steps, "tile": [ty, tz], "rules_blocks_per_sm": int(blocks), "ms": times}
+
+
+def load_table(path: str = TABLE_PATH) -> dict:
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+_TABLE: dict | None = None
+
+
+def lookup(nx: int, ny: int, nz: int, neighborhood: str, table: dict | None = None) -> tuple[int, int, int]:
+    """(tile_y, tile_z, rules_blocks_per_sm) for a grid: the tuned entry of its class, else of the
+    nearest tuned size of the same dimensionality and neighbourhood, else the defaults (0, 0, 0)."""
+    global _TABLE
+    if table is None:
+        if _TABLE is None:
+            _TABLE = load_table()
+        table = _TABLE
+    classes = table.get("classes", {})
+    key = shape_class(nx, ny, nz, neighborhood)
+    entry = classes.get(key)
+    if entry is None:
+        prefix, lg = key.rsplit("-", 1)
+        near = [(abs(int(k.rsplit("-", 1)[1]) - int(lg)), k) for k in classes if k.rsplit("-", 1)[0] == prefix]
+        if near:
+            entry = classes[min(near)[1]]
+    if entry is None:
+        return 0, 0, 0
+    ty, tz = entry["tile"]
+    if ny == 1 or nz == 1:
+        ty, tz = 0, 0
+    return ty, tz, entry["rules_blocks_per_sm"]
+
+
+def apply(params: "capi.CaParams", table: dict | None = None) -> "capi.CaParams":
+    """params with the tuned launch shape filled in (results are unchanged)."""
+    params.tile_y, params.tile_z, params.rules_blocks_per_sm = lookup(params.nx, params.ny, params.nz,
+                                                                       params.neighborhood, table)
+    return params
+
+
+def default_classes() -> list[str]:
+    """The classes of the benchmark workloads and of the batched / served job mix: 2D sections with
+    sides 128-2048 and 3D grids with sides 64-256 (z = side / 2), all neighbourhoods."""
+    out = []
+    for nb in ("von_neumann", "moore", "pentagonal"):
+        for lg in range(18, 25, 2):  # 3D: 2^18 .. 2^24 cells (64^3/2 .. 256^3/2)
+            out.append(f"3d-{nb}-{lg}")
+    out += ["3d-pentagonal-28", "3d-moore-23"]  # the 1024 x 1024 x 256 and 256 x 256 x 128 workloads
+    return sorted(set(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=TABLE_PATH)
+    ap.add_argument("--classes", nargs="*", default=None)
+    ap.add_argument("--steps", type=int, default=96)
+    args = ap.parse_args()
+    table = load_table(args.out)
+    table.setdefault("classes", {})
+    t0 = time.time()
+    for cls in args.classes or default_classes():
+        table["classes"][cls] = tune_class(cls, args.steps)
+        print(cls, table["classes"][cls]["tile"], table["classes"][cls]["rules_blocks_per_sm"],
+              table["classes"][cls]["ms"], flush=True)
+    table["note"] = ("fastest launch shape per class: device time of the calibration job's ACTIVE steps "
+                     "(tuner.tune_class); results are identical for every shape")
+    with open(args.out, "w") as f:
+        json.dump(table, f, indent=1)
+        f.write("\n")
+    print(f"tuned {len(args.classes or default_classes())} classes in {time.time() - t0:.1f} s")
+
+
+if __name__ == "__main__":
+    main()

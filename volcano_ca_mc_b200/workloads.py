@@ -11,6 +11,7 @@ Workloads (sizes from the benchmark definitions):
   c1  2D cross-section 512 x 1 x 256, one cone, 2 vents, Moore, absorbing, 300 steps, MC Q=64 kT=0.6 50 MCS
   c2  3D 256 x 256 x 128, two cones + crater, 3 vents, Moore, periodic, 400 steps, MC Q=128 kT=0.6 100 MCS
   c3  3D 1024 x 1024 x 256, six cones, 8 vents, pentagonal, absorbing, 800 steps, MC Q=256 kT=0.5 200 MCS
+  c3q the c3 family on 512 x 512 x 256 (a bounded profiling case)
 """
 from __future__ import annotations
 
@@ -139,8 +140,7 @@ def c2() -> Workload:
                     100, description="3D 256x256x128, cones (90, s50) + (60, s35), crater r10 d6, noise 2, 3 vents")
 
 
-def c3() -> Workload:
-    nx, ny, nz = 1024, 1024, 256
+def c3(nx: int = 1024, ny: int = 1024, nz: int = 256, name: str = "c3") -> Workload:
     rng = np.random.default_rng(3)
     x = np.arange(nx)[None, :]
     y = np.arange(ny)[:, None]
@@ -157,11 +157,17 @@ def c3() -> Workload:
     for k in range(8):
         cx, cy = centers[k % 6]
         vents.append((int(cx) + 3 * (k // 6), int(cy)))
-    return Workload("c3", nx, ny, nz, "pentagonal", "absorbing", 3, 800, hh, vents, 256, 0.5, 200,
-                    description="3D 1024x1024x256, six cones peak U[40,200] sigma U[60,250], noise 3, 8 vents")
+    return Workload(name, nx, ny, nz, "pentagonal", "absorbing", 3, 800, hh, vents, 256, 0.5, 200,
+                    description=f"3D {nx}x{ny}x{nz}, six cones peak U[40,200] sigma U[60,250], noise 3, 8 vents")
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c3": c3}
+def c3q() -> Workload:
+    """The c3 family at a quarter of its cells (512 x 512 x 256, 67 M cells, 3.5 GB of state): the
+    bounded case on which a profiler captures the c3 kernels (their DRAM traffic grows with the cells)."""
+    return c3(512, 512, 256, "c3q")
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c3": c3, "c3q": c3q}
 
 
 def get(name: str) -> Workload:
