@@ -71,6 +71,9 @@ def parse():
                     help="run exactly one CA job with this schedule (no warm-up, no MC), or with mc one ACTIVE "
                          "CA job and its MC stage, and exit: the case ncu captures")
     ap.add_argument("--max-steps", type=int, default=None, help="with --profile-job: stop the CA after this many steps")
+    ap.add_argument("--slabs", action="store_true",
+                    help="with --gpus N > 1: one grid of the workload split into N z slabs (strong scaling, halo "
+                         "exchange over NCCL) instead of N independent replicas")
     return ap.parse_args()
 
 
@@ -379,6 +382,32 @@ def workload_block(w, device, flush, peak, peak_kind, jobs=2):
             "parity": par}
 
 
+def mc_full_block(device, flush, peak, peak_kind, sweeps=20):
+    """Potts sweeps on a whole 3D space (mc.domain = full, as the reference's configs/mc_full_3d.json,
+    scaled up): 512 x 512 x 256 = 67 M cells, Moore, periodic, Q = 64, kT = 0.5, no mobility.  Every
+    cell is a trial every MCS: 12 B per trial (spin read + write + the trial's share of a mobility
+    read, counted as in the basalt case) against the HBM copy bandwidth."""
+    from volcano_ca_mc_b200 import capi
+    nx, ny, nz = 512, 512, 256
+    mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood="moore", boundary="periodic", domain_full=True, seed=9,
+                                    Q=64, J=1.0, kT=0.5, device=device))
+    mc.set_domain(None)
+    mc.initialize()
+    mc.sweep(2)  # warm-up
+    flush()
+    t0 = mc.timing()[0]
+    mc.sweep(sweeps)
+    ms = mc.timing()[0] - t0
+    info = mc.info()
+    mc.close()
+    trials = nx * ny * nz * sweeps
+    gbs = BYTES_PER_TRIAL * trials / (ms * 1e-3) / 1e9
+    return {"space": [nx, ny, nz], "neighborhood": "moore", "boundary": "periodic", "Q": 64, "kT": 0.5,
+            "sweeps": sweeps, "colors": info.colors, "ms_per_sweep": ms / sweeps,
+            "trials_per_s": trials / (ms * 1e-3), "achieved_gbs_12B_per_trial": round(gbs, 1),
+            "hbm_frac": round(gbs / peak, 4), "peak_kind": peak_kind}
+
+
 def job_mixes(args, device):
     """Many small independent jobs on one GPU through the engine's job server (engine --serve: engine
     configs in, resident handles admitted against the HBM budget, all running CA grids stepped in one
@@ -546,6 +575,7 @@ def ours(args):
     if rank == 0 and world == 1:
         if not args.no_c2 and w.name != "c2":
             extra["c2"] = workload_block(workloads.get("c2"), local, flush, peak, peak_kind)
+        extra["mc_full"] = mc_full_block(local, flush, peak, peak_kind)
         extra.update(job_mixes(args, local))
         eng = engine_cli(w)
         if eng is not None:
@@ -666,8 +696,54 @@ def profile_job(args):
     ca.close()
 
 
+def slab_arm(args):
+    """One CA run of the workload split into z slabs, one per rank (volcano_ca_mc_b200.slabs): each
+    rank steps its slab, the step counts are summed over NCCL, halos move by NCCL send / receive.
+    CA time = CUDA events around the whole loop on each rank, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from volcano_ca_mc_b200 import capi, slabs, workloads
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    w = workloads.get(args.workload)
+    p = ca_params(w, capi.SWEEP_DENSE, local)
+    lay = slabs.partition(w.nz, world)[rank]
+    comm = slabs.TorchComm(f"cuda:{local}")
+    random_nb = w.neighborhood in ("pentagonal", "hexagonal")
+    times = []
+    for it in range(args.warmup + args.steps):
+        slab = slabs.GpuSlab(p, lay, w.heights, w.vent_cells())
+        dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        steps, stop, _, _ = slabs.run_distributed(slab, comm, w.max_steps, random_nb, len(w.vents))
+        b.record()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            times.append(a.elapsed_time(b))
+        slab.close()
+    ms = max_over_ranks([sum(times)], f"cuda:{local}", world)[0]
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        value = w.cells * steps * args.steps / (ms * 1e-3)
+        print(json.dumps({"metric": "CA cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                          "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                          "dtype": "u8+i32+f32 (integer rules, f32 temperatures)", "data": "synthetic",
+                          "config": config_of(w),
+                          "method": {"parallelism": f"{world} z slabs of one grid (DENSE schedule, halo exchange and "
+                                                    "count sums over NCCL every step)", "ca_steps": steps}}),
+              flush=True)
+
+
 def main():
     args = parse()
+    if args.slabs and args.impl == "ours" and dist_env()[1] > 1:
+        slab_arm(args)
+        return
     if args.profile_job:
         profile_job(args)
     elif args.impl == "reference":

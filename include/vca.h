@@ -318,6 +318,18 @@ vca_status vca_mc_crystals(vca_mc* mc, int32_t* out);
 vca_status vca_mc_set_spins(vca_mc* mc, const int32_t* spins);
 /* Device time of the sweeps so far [ms] and of one colour-pass launch on average [ms]. */
 vca_status vca_mc_timing(vca_mc* mc, double* total_ms, double* color_kernel_ms, uint64_t* color_launches);
+/* z slabs of the MC stage (the reference's strips exchange one halo layer after every colour,
+ * engine/src/mc/PottsMC.cpp:451-460): the handle holds the owned layers and one halo layer on each
+ * side, its domain lists only owned cells, and its layer 0 is global layer z_offset (hashRand takes
+ * global indices, colours follow the global z).  Set before vca_mc_initialize; the z axis must not be
+ * periodic.  The caller sweeps colour by colour (vca_mc_color_pass; the last colour of a sweep ends
+ * the MCS) and copies the halo layers between slabs after each colour. */
+vca_status vca_mc_set_slab(vca_mc* mc, int z_offset);
+vca_status vca_mc_color_pass(vca_mc* mc, int color);
+/* Orientations of `layers` layers from local layer z0 to / from a buffer of layers * nx * ny int32
+ * (any memory the device can address; the copy kind is inferred). */
+vca_status vca_mc_pack_spins(vca_mc* mc, int z0, int layers, void* buf);
+vca_status vca_mc_unpack_spins(vca_mc* mc, int z0, int layers, const void* buf);
 /* ~PottsMC: frees the handle's device memory and stream. */
 void vca_mc_destroy(vca_mc* mc);
 

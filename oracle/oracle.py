@@ -55,6 +55,8 @@ def lib() -> ctypes.CDLL:
         L.vo_mc_sweep.argtypes = [p, i32, p, p, p, p]
         L.vo_mc_energy.restype = f64
         L.vo_mc_energy.argtypes = [p, i32, p]
+        L.vo_mc_color_strip.argtypes = [p, i32, i32, u64, i32, p, p, p, p]
+        L.vo_mc_color_strip.restype = None
         L.vo_mc_colors.restype = i32
         L.vo_mc_colors.argtypes = [p]
         _lib = L
@@ -228,6 +230,16 @@ def mc_sweep(p: McParams, t: int, domain: np.ndarray, mobility: np.ndarray | Non
     d = np.ascontiguousarray(domain, np.uint8)
     m = None if mobility is None else np.ascontiguousarray(mobility, np.float32)
     lib().vo_mc_sweep(ctypes.byref(p), t, _ptr(d), None if m is None else _ptr(m), _ptr(spin), _ptr(out))
+    return out
+
+
+def mc_color_strip(p: McParams, t: int, col: int, gidx_base: int, zoff: int, domain: np.ndarray,
+                   mobility: np.ndarray | None, spin: np.ndarray) -> np.ndarray:
+    """One colour of MCS t on a strip of z layers (p.nz = the strip's layers), in place; returns
+    (attempts, accepted, uphill)."""
+    out = np.zeros(3, np.uint64)
+    lib().vo_mc_color_strip(ctypes.byref(p), t, col, gidx_base, zoff, _ptr(domain),
+                            None if mobility is None else _ptr(mobility), _ptr(spin), _ptr(out))
     return out
 
 

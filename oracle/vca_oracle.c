@@ -586,21 +586,22 @@ int vo_mc_color_of(const vo_mc_params* p, int x, int y, int z) {
     return cx + classes_of(p, 0) * (cy + classes_of(p, 1) * cz);
 }
 
-void vo_mc_sweep(const vo_mc_params* p, int t, const uint8_t* domain, const float* mobility, int32_t* spin,
-                 uint64_t out[3]) {
+/* colorTrials (PottsMC.cpp:394-448) of one colour; order within a colour does not matter.  For a
+ * strip of z layers of a taller grid (PottsMC.cpp:451-460): hashRand takes global indices (local +
+ * gidx_base) and colours follow the global z (local + zoff). */
+static void mc_color_impl(const vo_mc_params* p, int t, int col, uint64_t gidx_base, int zoff, const uint8_t* domain,
+                          const float* mobility, int32_t* spin, uint64_t out[3]) {
     int off[6][26][3], cnt[6];
     const int variants = vo_nb_build(p->neighborhood, p->nx, p->ny, p->nz, off, cnt);
     const uint64_t prefix = vo_hash_prefix(p->seed, (uint64_t)t);
     const uint64_t other = (uint64_t)(p->Q - 1);
-    const int colors = vo_mc_colors(p);
-    for (int col = 0; col < colors; ++col) {
-        /* colorTrials (PottsMC.cpp:394-448); order within a colour does not matter. */
+    {
         for (int z = 0; z < p->nz; ++z)
             for (int y = 0; y < p->ny; ++y)
                 for (int x = 0; x < p->nx; ++x) {
                     const int64_t g = mgidx(p, x, y, z);
-                    if (!domain[g] || vo_mc_color_of(p, x, y, z) != col) continue;
-                    const uint64_t h = vo_hash_index(prefix, (uint64_t)g);
+                    if (!domain[g] || vo_mc_color_of(p, x, y, z + zoff) != col) continue;
+                    const uint64_t h = vo_hash_index(prefix, (uint64_t)g + gidx_base);
                     if (mobility != NULL && to_uniform(vo_hash_salt(h, SALT_MC_MOBILITY)) >= (double)mobility[g]) continue;
                     ++out[0];
                     int v = 0;
@@ -629,6 +630,17 @@ void vo_mc_sweep(const vo_mc_params* p, int t, const uint8_t* domain, const floa
                     }
                 }
     }
+}
+
+void vo_mc_sweep(const vo_mc_params* p, int t, const uint8_t* domain, const float* mobility, int32_t* spin,
+                 uint64_t out[3]) {
+    const int colors = vo_mc_colors(p);
+    for (int col = 0; col < colors; ++col) mc_color_impl(p, t, col, 0, 0, domain, mobility, spin, out);
+}
+
+void vo_mc_color_strip(const vo_mc_params* p, int t, int col, uint64_t gidx_base, int zoff, const uint8_t* domain,
+                       const float* mobility, int32_t* spin, uint64_t out[3]) {
+    mc_color_impl(p, t, col, gidx_base, zoff, domain, mobility, spin, out);
 }
 
 double vo_mc_energy(const vo_mc_params* p, int t, const int32_t* spin) {

@@ -93,6 +93,10 @@ void vo_mc_sweep(const vo_mc_params* p, int t, const uint8_t* domain, const floa
 
 /* Energy after t sweeps (PottsMC::totalEnergy, PottsMC.cpp:590-664). */
 double vo_mc_energy(const vo_mc_params* p, int t, const int32_t* spin);
+/* One colour of MCS t on a strip of z layers of a taller grid (PottsMC.cpp:451-460): global index of
+ * local cell 0 = gidx_base, global z = local z + zoff. */
+void vo_mc_color_strip(const vo_mc_params* p, int t, int col, uint64_t gidx_base, int zoff, const uint8_t* domain,
+                       const float* mobility, int32_t* spin, uint64_t out[3]);
 
 #ifdef __cplusplus
 }

@@ -34,6 +34,7 @@ EXPORTS = [
     "vca_mc_create", "vca_mc_footprint", "vca_mc_reconfigure", "vca_mc_set_domain", "vca_mc_set_mobility", "vca_mc_set_domain_from_ca",
     "vca_mc_set_mobility_from_ca", "vca_mc_mobility", "vca_mc_initialize", "vca_mc_sweep", "vca_mc_get_info",
     "vca_mc_energy", "vca_mc_grains", "vca_mc_set_mobility_values", "vca_mc_crystals", "vca_mc_set_spins", "vca_mc_timing", "vca_mc_destroy",
+    "vca_mc_set_slab", "vca_mc_color_pass", "vca_mc_pack_spins", "vca_mc_unpack_spins",
     "vca_mc_energy_noalloc",
     "vca_last_error", "vca_version",
 ]
@@ -116,6 +117,8 @@ def lib() -> ctypes.CDLL:
         "vca_mc_set_mobility_values": [p, p, i32], "vca_mc_crystals": [p, p],
         "vca_mc_set_spins": [p, p], "vca_mc_timing": [p, p, p, p],
         "vca_mc_energy_noalloc": [p, i32, i32, i32, i32, i32, i32, u64, i32, f64, p, p],
+        "vca_mc_set_slab": [p, i32], "vca_mc_color_pass": [p, i32], "vca_mc_pack_spins": [p, i32, i32, p],
+        "vca_mc_unpack_spins": [p, i32, i32, p],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -487,6 +490,18 @@ class PottsMC:
     def set_spins(self, spins: np.ndarray) -> None:
         s = np.ascontiguousarray(spins, np.int32)
         _check(lib().vca_mc_set_spins(self.h, _ptr(s)), "vca_mc_set_spins")
+
+    def set_slab(self, z_offset: int) -> None:
+        _check(lib().vca_mc_set_slab(self.h, z_offset), "vca_mc_set_slab")
+
+    def color_pass(self, color: int) -> None:
+        _check(lib().vca_mc_color_pass(self.h, color), "vca_mc_color_pass")
+
+    def pack_spins(self, z0: int, layers: int, buf_ptr: int) -> None:
+        _check(lib().vca_mc_pack_spins(self.h, z0, layers, ctypes.c_void_p(buf_ptr)), "vca_mc_pack_spins")
+
+    def unpack_spins(self, z0: int, layers: int, buf_ptr: int) -> None:
+        _check(lib().vca_mc_unpack_spins(self.h, z0, layers, ctypes.c_void_p(buf_ptr)), "vca_mc_unpack_spins")
 
     def timing(self) -> tuple[float, float, int]:
         tot, ker, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()

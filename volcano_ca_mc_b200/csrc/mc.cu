@@ -71,6 +71,10 @@ struct McArgs {
     const unsigned long long* table;  // 27 x 27 acceptance thresholds
     const NbTable* nb;
     McCtrl* ctrl;
+    // z slab of a taller grid (vca_mc_set_slab): hashRand takes local index + gidx_base, colours
+    // the global z = local z + zoff
+    uint64_t gidx_base;
+    int zoff;
 };
 
 __device__ __forceinline__ bool mc_wrap(int& v, int n, int periodic) {
@@ -146,6 +150,7 @@ __host__ __device__ inline int axis_class(int c, int n, int periodic) {
     return c & 1;
 }
 __host__ __device__ inline int color_of(const McArgs& a, int x, int y, int z) {
+    z += a.zoff;  // a slab colours by global z (its z axis is never periodic)
     if (a.parity_colors) return (x + y + z) & 1;
     const int cx = axis_class(x, a.nx, a.per[0]), cy = axis_class(y, a.ny, a.per[1]), cz = axis_class(z, a.nz, a.per[2]);
     return cx + a.classes[0] * (cy + a.classes[1] * cz);
@@ -163,7 +168,8 @@ __device__ __forceinline__ void decode(const McArgs& a, uint32_t g, int& x, int&
 __global__ void mc_init_kernel(McArgs a, const uint8_t* domain, uint64_t n) {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x) {
         int32_t s = 0;
-        if (domain[g]) s = 1 + (int32_t)fast_mod(hash_salt(hash_index(hash_prefix(a.seed, 0), g), kSaltMcInit), a.q_mod);
+        if (domain[g])
+            s = 1 + (int32_t)fast_mod(hash_salt(hash_index(hash_prefix(a.seed, 0), g + a.gidx_base), kSaltMcInit), a.q_mod);
         a.spin[g] = s;
     }
 }
@@ -219,7 +225,7 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
     unsigned my_att = 0, my_acc = 0, my_up = 0;
     for (uint64_t j = blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < count; j += (uint64_t)gridDim.x * kMcThreads) {
         const uint32_t g = list[j];
-        const uint64_t h = hash_index(prefix, g);
+        const uint64_t h = hash_index(prefix, g + a.gidx_base);
         if (kMobility) {
             const uint64_t r = hash_salt(h, kSaltMcMobility);
             if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)list_mob[j]) continue;
@@ -348,7 +354,7 @@ __global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel
             const uint64_t b = col.off[c], e = col.off[c + 1];
             for (uint64_t j = b + blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < e; j += (uint64_t)gridDim.x * kMcThreads) {
                 const uint32_t g = a.list[j];
-                const uint64_t h = hash_index(prefix, g);
+                const uint64_t h = hash_index(prefix, g + a.gidx_base);
                 if (kMobility) {
                     const uint64_t r = hash_salt(h, kSaltMcMobility);
                     if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)a.list_mob[j]) continue;
@@ -429,7 +435,8 @@ __global__ __launch_bounds__(kMcThreads) void mc_energy_kernel(McArgs a, const u
         decode(a, g, x, y, z);
         const int32_t s = a.spin[g];
         int var = 0;
-        if (!forward && a.variants > 1) var = (int)fast_mod(hash_salt(hash_index(prefix, g), kSaltNeighborhood), a.var_mod);
+        if (!forward && a.variants > 1)
+            var = (int)fast_mod(hash_salt(hash_index(prefix, g + a.gidx_base), kSaltNeighborhood), a.var_mod);
         int in_dom = 0, same = 0;
         for (int k = 0; k < nb.count[var]; ++k) {
             const int dx = nb.off[var][k][0], dy = nb.off[var][k][1], dz = nb.off[var][k][2];
@@ -693,6 +700,7 @@ struct vca_mc {
     uint64_t launches = 0;
     int profile_kernels = 0;
     std::vector<cudaEvent_t> prof_events;
+    int slab_zoff = -1;                  // z slab of a taller grid (vca_mc_set_slab), -1: none
 };
 
 namespace {
@@ -729,6 +737,8 @@ McArgs mc_args(const vca_mc* h) {
     a.table = h->table;
     a.nb = h->nb;
     a.ctrl = h->ctrl;
+    a.zoff = h->slab_zoff > 0 ? h->slab_zoff : 0;
+    a.gidx_base = (uint64_t)h->desc.nx * h->desc.ny * (uint64_t)a.zoff;
     return a;
 }
 
@@ -822,6 +832,7 @@ vca_status mc_configure(vca_mc* h, const vca_mc_desc* d) {
     h->desc = *d;
     h->n = (uint64_t)d->nx * d->ny * d->nz;
     build_nb(d->neighborhood, d->nx, d->ny, d->nz, h->nb_host);
+    h->slab_zoff = -1;
     // Periodic axes: PottsMC ctor (PottsMC.cpp:18) with the Boundary of McStage::run (McStage.cpp:106).
     const bool periodic = d->boundary == VCA_BC_PERIODIC;
     h->per[0] = periodic && d->nx > 1;
@@ -1323,6 +1334,76 @@ vca_status vca_mc_set_spins(vca_mc* h, const int32_t* spins) {
     VCA_CUDA(cudaMemcpyAsync(h->spin, spins, 4 * h->n, cudaMemcpyHostToDevice, h->stream));
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     return VCA_OK;
+}
+
+vca_status vca_mc_set_slab(vca_mc* h, int z_offset) {
+    if (vca_status s = mc_check(h)) return s;
+    if (z_offset < 0 || h->per[2] || h->desc.nz < 2) {
+        set_error("vca_mc_set_slab: a slab needs z_offset >= 0, nz > 1 and no periodic z axis");
+        return VCA_ERR_ARG;
+    }
+    if (h->initialized) {
+        set_error("vca_mc_set_slab: set the slab before vca_mc_initialize");
+        return VCA_ERR_STATE;
+    }
+    h->slab_zoff = z_offset;
+    return VCA_OK;
+}
+
+vca_status vca_mc_color_pass(vca_mc* h, int color) {
+    if (vca_status s = mc_check(h)) return s;
+    if (!h->initialized) {
+        set_error("vca_mc_color_pass: initialize first");
+        return VCA_ERR_STATE;
+    }
+    if (color < 0 || color >= h->colors) {
+        set_error("vca_mc_color_pass: colour out of range");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    const McArgs a = mc_args(h);
+    const uint64_t b = h->color_off[color], cnt = h->color_off[color + 1] - b;
+    const int grid = grid_for(cnt, h->sms);
+    const uint32_t* list = h->list + b;
+    const float* mob = h->mobility_on ? h->list_mob + b : nullptr;
+    const int last = color == h->colors - 1;
+    const bool random_nb = h->nb_host.variants > 1;
+    if (h->mobility_on) {
+        if (random_nb) mc_color_kernel<true, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+        else mc_color_kernel<true, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+    } else {
+        if (random_nb) mc_color_kernel<false, true><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+        else mc_color_kernel<false, false><<<grid, kMcThreads, 0, h->stream>>>(a, list, mob, cnt, last);
+    }
+    VCA_CUDA(cudaGetLastError());
+    h->launches += 1;
+    return VCA_OK;
+}
+
+static vca_status spin_layers(vca_mc* h, int z0, int layers, void* buf, bool to_buf, const char* who) {
+    if (vca_status s = mc_check(h)) return s;
+    if (buf == nullptr || z0 < 0 || layers < 0 || z0 + layers > h->desc.nz) {
+        set_error(std::string(who) + ": layers outside the grid or null buffer");
+        return VCA_ERR_ARG;
+    }
+    VCA_CUDA(cudaSetDevice(h->device));
+    const size_t L = (size_t)h->desc.nx * h->desc.ny;
+    int32_t* dev = h->spin + (size_t)z0 * L;
+    const size_t bytes = (size_t)layers * L * sizeof(int32_t);
+    if (to_buf)
+        VCA_CUDA(cudaMemcpyAsync(buf, dev, bytes, cudaMemcpyDefault, h->stream));
+    else
+        VCA_CUDA(cudaMemcpyAsync(dev, buf, bytes, cudaMemcpyDefault, h->stream));
+    VCA_CUDA(cudaStreamSynchronize(h->stream));
+    return VCA_OK;
+}
+
+vca_status vca_mc_pack_spins(vca_mc* h, int z0, int layers, void* buf) {
+    return spin_layers(h, z0, layers, buf, true, "vca_mc_pack_spins");
+}
+
+vca_status vca_mc_unpack_spins(vca_mc* h, int z0, int layers, const void* buf) {
+    return spin_layers(h, z0, layers, const_cast<void*>(buf), false, "vca_mc_unpack_spins");
 }
 
 vca_status vca_mc_timing(vca_mc* h, double* total_ms, double* color_kernel_ms, uint64_t* color_launches) {

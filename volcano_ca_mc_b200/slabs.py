@@ -22,6 +22,13 @@ halo messages (``GpuSlab``: a vca_ca handle on this process's GPU), and a commun
 and moves messages (``TorchComm``: torch.distributed send / recv and all-reduce, NCCL between GPUs).
 ``run_local`` drives several slabs in one process (one GPU holding every slab; no kernel waits on
 another, the host orders the steps and the copies).
+
+The MC stage splits the same way (PottsMC.cpp:451-460): each slab holds its owned layers and one
+halo layer on each side, its domain is the basalt of its owned layers, and after every colour of
+every MCS the slabs exchange their boundary layers of orientations.  The cooling mobility needs the
+end step and the liquid-time range of the whole domain: those three numbers are reduced over the
+slabs (min / max), then each slab normalises its own cells (CoolingMobility::fromCooling,
+engine/src/mc/CoolingMobility.cpp:16-83).
 """
 from __future__ import annotations
 
@@ -151,9 +158,10 @@ class TorchComm:
         import torch.distributed as dist
         self.dist, self.torch, self.device = dist, torch, device
 
-    def allreduce(self, values):
+    def allreduce(self, values, op: str = "sum"):
         t = self.torch.tensor(values, dtype=self.torch.int64, device=self.device)
-        self.dist.all_reduce(t)
+        red = {"sum": self.dist.ReduceOp.SUM, "min": self.dist.ReduceOp.MIN, "max": self.dist.ReduceOp.MAX}[op]
+        self.dist.all_reduce(t, op=red)
         return [int(v) for v in t.tolist()]
 
     def buffer(self, nbytes: int):
@@ -238,3 +246,181 @@ def run_local(slabs: list, max_steps: int, random_nb: bool, initial_lava: int, b
 def assemble(parts: list) -> list:
     """The whole grid's five planes from the owned planes of every slab, bottom slab first."""
     return [np.concatenate([p[i] for p in parts]) for i in range(5)]
+
+
+# ------------------------------------------------------------------------------------------
+# MC stage over slabs
+# ------------------------------------------------------------------------------------------
+LAVA, BASALT = 2, 3
+
+
+def mc_layout(lay: SlabLayout) -> tuple[int, int]:
+    """Global layers [lo, hi) an MC slab holds: its owned layers and one halo layer on each side."""
+    return max(0, lay.z0 - 1), min(lay.nz, lay.z1 + 1)
+
+
+def basalt_domain(types) -> np.ndarray:
+    """CoolingMobility::basaltDomain (CoolingMobility.cpp:8-14): BASALT or LAVA cells."""
+    return ((types == BASALT) | (types == LAVA)).astype(np.uint8)
+
+
+def local_end(planes) -> int:
+    """This slab's share of CoolingMobility::endStep (CoolingMobility.cpp:16-25): the largest stamp
+    of its owned domain cells (max-reduced over the slabs)."""
+    t, _, _, so, ar = planes
+    dom = basalt_domain(t) > 0
+    return int(np.maximum(so[dom], ar[dom]).max()) if dom.any() else 0
+
+
+def liquid_time(planes, end: int) -> np.ndarray:
+    """CoolingMobility::liquidTime (CoolingMobility.cpp:31-45) of the owned cells, 0 outside the domain."""
+    t, _, _, so, ar = planes
+    dom = basalt_domain(t) > 0
+    sol = np.where(t == BASALT, so.astype(np.int64), end)
+    return np.where(dom, np.maximum(sol - ar.astype(np.int64), 0), 0)
+
+
+def local_time_range(planes, end: int) -> tuple[int, int]:
+    """This slab's (min, max) liquid time over its domain (min- / max-reduced over the slabs)."""
+    dom = basalt_domain(planes[0]) > 0
+    if not dom.any():
+        return np.iinfo(np.int64).max, -1
+    tm = liquid_time(planes, end)[dom]
+    return int(tm.min()), int(tm.max())
+
+
+def normalize(time, domain, tmin: int, tmax: int, mobility_min: float) -> np.ndarray:
+    """CoolingMobility::normalize (CoolingMobility.cpp:62-77): double steps rounded one by one, then
+    to float."""
+    dom = domain.astype(bool)
+    mob = np.zeros(len(domain), np.float32)
+    if tmax < 0:
+        return mob
+    if tmax == tmin:
+        mob[dom] = 1.0
+        return mob
+    norm = (time[dom] - tmin).astype(np.float64) / float(tmax - tmin)
+    mob[dom] = (mobility_min + (1.0 - mobility_min) * norm).astype(np.float32)
+    return mob
+
+
+def mobility_terms(planes_of_slabs, reduce=None):
+    """(end, tmin, tmax) of the whole domain: from the owned planes of every slab of this process,
+    reduced further over the ranks by reduce(values, op) when given."""
+    end = max(local_end(p) for p in planes_of_slabs)
+    if reduce:
+        end = reduce([end], "max")[0]
+    ranges = [local_time_range(p, end) for p in planes_of_slabs]
+    tmin, tmax = min(r[0] for r in ranges), max(r[1] for r in ranges)
+    if reduce:
+        tmin, tmax = reduce([tmin], "min")[0], reduce([tmax], "max")[0]
+    return end, tmin, tmax
+
+
+class McSlab:
+    """One slab of the MC stage on this process's GPU (a vca_mc handle of nx x ny x held layers): the
+    basalt of its owned layers, the cooling mobility from the whole domain's (end, tmin, tmax)."""
+
+    def __init__(self, mcp: "capi.McParams", lay: SlabLayout, owned_planes, terms, mobility_min: float,
+                 use_mobility: bool = True):
+        lo, hi = mc_layout(lay)
+        self.lay, self.lo, self.hi = lay, lo, hi
+        self.L = mcp.nx * mcp.ny
+        end, tmin, tmax = terms
+        own_dom = basalt_domain(owned_planes[0])
+        mob_own = normalize(liquid_time(owned_planes, end), own_dom, tmin, tmax, mobility_min)
+        held = hi - lo
+        dom = np.zeros(held * self.L, np.uint8)
+        mob = np.zeros(held * self.L, np.float32)
+        a, b = (lay.z0 - lo) * self.L, (lay.z1 - lo) * self.L
+        dom[a:b] = own_dom
+        mob[a:b] = mob_own
+        self.mc = capi.PottsMC(capi.McParams(**{**mcp.__dict__, "nz": held}))
+        self.mc.set_slab(lo)
+        self.mc.set_domain(dom)
+        self.mc.set_mobility(mob if use_mobility else None)
+        self.mc.initialize()
+        self.colors = self.mc.info().colors
+
+    def plan(self) -> dict:
+        """Halo layers in local z: up (to rank + 1) the top owned layer into its lower halo, down (to
+        rank - 1) the lowest owned layer into its upper halo."""
+        lay, lo = self.lay, self.lo
+        p = {}
+        if lay.rank + 1 < lay.world:
+            p["send_up"] = lay.z1 - 1 - lo
+            p["recv_up"] = lay.z1 - lo
+        if lay.rank > 0:
+            p["send_down"] = lay.z0 - lo
+            p["recv_down"] = lay.z0 - 1 - lo
+        return p
+
+    def color_pass(self, c: int) -> None:
+        self.mc.color_pass(c)
+
+    def pack(self, z, buf):
+        self.mc.pack_spins(z, 1, buf.data_ptr())
+
+    def unpack(self, z, buf):
+        self.mc.unpack_spins(z, 1, buf.data_ptr())
+
+    def counters(self) -> tuple[int, int, int]:
+        i = self.mc.info()
+        return i.attempts, i.accepted, i.uphill
+
+    def owned_spins(self) -> np.ndarray:
+        c = self.mc.crystals()
+        return c[(self.lay.z0 - self.lo) * self.L:(self.lay.z1 - self.lo) * self.L]
+
+    def close(self):
+        self.mc.close()
+
+
+def run_mc_local(mslabs: list, sweeps: int, buffer) -> None:
+    """`sweeps` checkerboard MCS on the MC slabs of this process: each colour on every slab, then the
+    boundary layers of orientations move to the neighbours' halos (an exchange also comes first,
+    so the halos hold the initial orientations)."""
+    def exchange():
+        for r, s in enumerate(mslabs):
+            p = s.plan()
+            for key, peer, into in (("send_up", r + 1, "recv_down"), ("send_down", r - 1, "recv_up")):
+                if key in p:
+                    buf = buffer(4 * s.L)
+                    s.pack(p[key], buf)
+                    mslabs[peer].unpack(mslabs[peer].plan()[into], buf)
+    exchange()
+    colors = mslabs[0].colors
+    for _ in range(sweeps):
+        for c in range(colors):
+            for s in mslabs:
+                s.color_pass(c)
+            exchange()
+
+
+def run_mc_distributed(mslab, comm, sweeps: int) -> None:
+    """The same loop on one rank; halo layers over comm (torch.distributed)."""
+    p = mslab.plan()
+    bufs = {k: comm.buffer(4 * mslab.L) for k in p}
+    lay = mslab.lay
+
+    def exchange():
+        for key in ("send_up", "send_down"):
+            if key in p:
+                mslab.pack(p[key], bufs[key])
+        sends = {}
+        recvs = {}
+        if "send_up" in p:
+            sends[lay.rank + 1] = bufs["send_up"]
+            recvs[lay.rank + 1] = bufs["recv_up"]
+        if "send_down" in p:
+            sends[lay.rank - 1] = bufs["send_down"]
+            recvs[lay.rank - 1] = bufs["recv_down"]
+        comm.exchange(sends, recvs)
+        for key in ("recv_up", "recv_down"):
+            if key in p:
+                mslab.unpack(p[key], bufs[key])
+    exchange()
+    for _ in range(sweeps):
+        for c in range(mslab.colors):
+            mslab.color_pass(c)
+            exchange()
