@@ -42,11 +42,13 @@ enum { VCA_NB_VON_NEUMANN = 0, VCA_NB_MOORE = 1, VCA_NB_PENTAGONAL = 2, VCA_NB_H
 enum { VCA_BC_ABSORBING = 0, VCA_BC_PERIODIC = 1 };
 /* CaMode (engine/src/core/Types.hpp:28) */
 enum { VCA_MODE_LAVA = 0, VCA_MODE_CLASSIC = 1 };
-/* Step schedule.  Both give bit-identical results (grids, histories, stop step), like the
+/* Step schedule.  All give bit-identical results (grids, histories, stop step), like the
  * reference's ca.sweep = front / full (engine/src/ca/LavaCA.hpp:13-29):
- *   ACTIVE -- tiles with no lava within one cell, and unchanged since the last step, are skipped;
- *   DENSE  -- every cell of the grid is read and written every step. */
-enum { VCA_SWEEP_ACTIVE = 0, VCA_SWEEP_DENSE = 1 };
+ *   ACTIVE      -- tiles with no lava within one cell, and unchanged since the last step, are
+ *                  skipped; a grid whose every tile has a rules block of its own runs DENSE;
+ *   DENSE       -- every cell of the grid is read and written every step;
+ *   ACTIVE_LIST -- ACTIVE with the tile list whatever the grid size. */
+enum { VCA_SWEEP_ACTIVE = 0, VCA_SWEEP_DENSE = 1, VCA_SWEEP_ACTIVE_LIST = 2 };
 /* StopReason (engine/src/ca/CaRules.hpp:108) */
 enum { VCA_STOP_RUNNING = 0, VCA_STOP_NO_LAVA = 1, VCA_STOP_NO_AIR = 2, VCA_STOP_NO_CHANGE = 3,
        VCA_STOP_MAX_STEPS = 4 };

@@ -55,7 +55,7 @@ def _distinct_lava_ids_around(s, x, y, z):
     return len(ids)
 
 
-@pytest.mark.parametrize("sweep", [capi.SWEEP_ACTIVE, capi.SWEEP_DENSE], ids=["active", "dense"])
+@pytest.mark.parametrize("sweep", [capi.SWEEP_ACTIVE_LIST, capi.SWEEP_DENSE], ids=["active", "dense"])
 @pytest.mark.parametrize("nb", ["moore", "pentagonal"])
 def test_wide_vote_junctions_match_oracle(nb, sweep):
     nx, ny, nz = 40, 22, 10
@@ -82,7 +82,7 @@ def test_wide_vote_junctions_match_oracle(nb, sweep):
     ca.close()
 
 
-@pytest.mark.parametrize("sweep", [capi.SWEEP_ACTIVE, capi.SWEEP_DENSE], ids=["active", "dense"])
+@pytest.mark.parametrize("sweep", [capi.SWEEP_ACTIVE_LIST, capi.SWEEP_DENSE], ids=["active", "dense"])
 def test_last_steps_before_max_steps_limit(sweep):
     nx, ny, nz = 48, 20, 24
     seed = 4242

@@ -38,7 +38,7 @@ def _params(nx, ny, nz, nb, bc, steps, sweep, seed):
                          cooling_lateral=4.0, cooling_fall=2.0, ponding=True, sweep=sweep)
 
 
-@pytest.mark.parametrize("sweep", [capi.SWEEP_ACTIVE, capi.SWEEP_DENSE], ids=["active", "dense"])
+@pytest.mark.parametrize("sweep", [capi.SWEEP_ACTIVE_LIST, capi.SWEEP_DENSE], ids=["active", "dense"])
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}x{c[1]}x{c[2]}-{c[3]}-{c[4]}")
 def test_lava_steps_match_oracle(case, sweep):
     nx, ny, nz, nb, bc, steps, nv = case
@@ -114,7 +114,7 @@ def test_run_to_stop_matches_stepwise():
     spill = O.fill_depressions(heights, nx, ny, False, False)
     s0 = C.initial_state(nx, ny, nz, heights, vents, p.erupt_temp)
     s, steps, stop, act, chg = O.ca_run(C.oracle_params(p), s0, spill, O.vent_table(vents))
-    for sweep in (capi.SWEEP_ACTIVE, capi.SWEEP_DENSE):
+    for sweep in (capi.SWEEP_ACTIVE, capi.SWEEP_ACTIVE_LIST, capi.SWEEP_DENSE):
         p.sweep = sweep
         ca = capi.LavaCA(p)
         ca.apply_terrain(heights)
@@ -130,7 +130,7 @@ def test_run_to_stop_matches_stepwise():
 def test_set_state_resumes():
     """A state uploaded mid-run (steps_done = k) continues exactly like the uninterrupted run."""
     nx, ny, nz = 40, 12, 24
-    p = _params(nx, ny, nz, "moore", "periodic", 60, capi.SWEEP_ACTIVE, 9)
+    p = _params(nx, ny, nz, "moore", "periodic", 60, capi.SWEEP_ACTIVE_LIST, 9)
     heights = C.terrain(nx, ny, nz, 9)
     vents = C.pick_vents(heights, nx, ny, nz, 2, 9)
     spill = O.fill_depressions(heights, nx, ny, True, True)
@@ -235,7 +235,7 @@ def test_tile_shapes_match_oracle(case, tile, blocks):
     vents = C.pick_vents(heights, nx, ny, nz, 2, seed)
     per = bc == "periodic"
     spill = O.fill_depressions(heights, nx, ny, per, per)
-    for sweep in (capi.SWEEP_ACTIVE, capi.SWEEP_DENSE):
+    for sweep in (capi.SWEEP_ACTIVE_LIST, capi.SWEEP_DENSE):
         p = _params(nx, ny, nz, nb, bc, steps, sweep, seed)
         p.tile_y, p.tile_z, p.rules_blocks_per_sm = tile[0], tile[1], blocks
         op = C.oracle_params(p)

@@ -19,7 +19,7 @@ ENGINE_PATH = os.path.join(PKG_DIR, "bin", "engine")
 NB = {"von_neumann": 0, "moore": 1, "pentagonal": 2, "hexagonal": 3}
 BC = {"absorbing": 0, "periodic": 1}
 MODE = {"lava": 0, "classic": 1}
-SWEEP_ACTIVE, SWEEP_DENSE = 0, 1
+SWEEP_ACTIVE, SWEEP_DENSE, SWEEP_ACTIVE_LIST = 0, 1, 2
 STOP_NAMES = {0: "running", 1: "no lava", 2: "no air", 3: "no change", 4: "max steps"}
 
 # Every entry point declared in include/vca.h.

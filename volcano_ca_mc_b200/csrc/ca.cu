@@ -1495,13 +1495,17 @@ using namespace vca;
 
 namespace {
 
-CaKernelArgs make_args(const vca_ca* h) {
+// batched: the arguments of a batch member, whose blocks the batch shares out.  A single grid whose
+// every tile has a rules block of its own runs every tile every step under VCA_SWEEP_ACTIVE (the
+// tile list and its atomics buy nothing there, and the results are the same either way).
+CaKernelArgs make_args(const vca_ca* h, bool batched = false) {
     CaKernelArgs k;
     std::memset(&k, 0, sizeof(k));
     k.g = h->geom;
     k.classic = h->desc.mode == VCA_MODE_CLASSIC;
     k.ponding = h->desc.ponding != 0;
-    k.dense = h->desc.sweep == VCA_SWEEP_DENSE;
+    k.dense = h->desc.sweep == VCA_SWEEP_DENSE ||
+              (h->desc.sweep == VCA_SWEEP_ACTIVE && !batched && h->ntiles <= (uint64_t)h->grid_blocks);
     k.seed = h->desc.seed;
     k.max_steps = h->desc.max_steps;
     k.eruption_steps = h->desc.eruption_steps;
@@ -1986,7 +1990,7 @@ vca_status validate_desc(const vca_ca_desc* d, const char* who) {
         return bad("a 2D lava space is the x-z cross-section (ny = 1)");
     if (d->max_steps < 0 || d->max_steps > 65535) return bad("max_steps must be in 0..65535");
     if (d->neighborhood < 0 || d->neighborhood > 3 || d->boundary < 0 || d->boundary > 1 || d->mode < 0 || d->mode > 1 ||
-        d->sweep < 0 || d->sweep > 1)
+        d->sweep < 0 || d->sweep > 2)
         return bad("unknown neighborhood, boundary, mode or sweep");
     NbTable nb;
     if (!build_nb(d->neighborhood, nx, ny, nz, nb)) return bad("the hexagonal neighbourhood is defined in 2D only");
@@ -2729,7 +2733,7 @@ vca_status batch_upload(vca_ca_batch* b) {
         std::memset(&args[(size_t)i], 0, sizeof(CaKernelArgs));
         if (!h) continue;
         tm[(size_t)i] = h->tmaps;
-        args[(size_t)i] = make_args(h);
+        args[(size_t)i] = make_args(h, true);
         members.push_back(i);
         w.push_back(std::max<uint64_t>(1, h->ntiles));
     }

@@ -145,5 +145,6 @@ JobOutcome run_job(const Config& cfg, const std::string& out_dir, Timing& timing
 vca_ca_desc ca_desc(const Config& c);
 const char* stop_text(int s);
 int run_server(int slots, double budget_gb, bool batched);
+extern bool g_use_tuning;  // launch shapes from the tuned table (single runs)
 
 }  // namespace eng

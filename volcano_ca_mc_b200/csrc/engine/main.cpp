@@ -191,6 +191,61 @@ std::vector<Vent> build_vents(const Config& c, const Heightmap& hm) {
     return place_vents(c, hm);
 }
 
+// The launch shape tuned for a grid's class (volcano_ca_mc_b200/tuner.py writes the table
+// volcano_ca_mc_b200/tuning.json, found beside bin/ or named by VCA_TUNING): tile 64 x tile_y x
+// tile_z and resident rules blocks per SM.  The results do not depend on it.  The job server keeps
+// the default tiles (its batch steps them).
+bool g_use_tuning = true;
+
+const Json& tuning_table() {
+    static const Json table = [] {
+        std::string path;
+        if (const char* e = std::getenv("VCA_TUNING")) {
+            path = e;
+        } else {
+            std::error_code ec;
+            const fs::path exe = fs::read_symlink("/proc/self/exe", ec);
+            if (!ec) path = (exe.parent_path().parent_path() / "tuning.json").string();
+        }
+        std::ifstream in(path);
+        if (!in) return Json::object();
+        std::stringstream ss;
+        ss << in.rdbuf();
+        try {
+            return Json::parse(ss.str(), false);
+        } catch (const std::exception&) {
+            return Json::object();
+        }
+    }();
+    return table;
+}
+
+void apply_tuning(vca_ca_desc& d, const Config& c) {
+    if (!g_use_tuning || c.space.ny == 1 || c.space.nz == 1) return;  // the 2D tiles have one shape
+    const Json* classes = tuning_table().find("classes");
+    if (!classes || !classes->is_object()) return;
+    const std::string prefix = std::string("3d-") + nb_name(c.neighborhood) + "-";
+    const long lg = std::lround(std::log2((double)c.space.cells()));
+    const Json* best = nullptr;
+    long best_gap = 1L << 30;
+    for (const auto& kv : classes->members()) {
+        if (kv.first.rfind(prefix, 0) != 0) continue;
+        const long gap = std::labs(std::atol(kv.first.c_str() + prefix.size()) - lg);
+        if (gap < best_gap) {
+            best_gap = gap;
+            best = &kv.second;
+        }
+    }
+    if (!best) return;
+    const Json* tile = best->find("tile");
+    const Json* blocks = best->find("rules_blocks_per_sm");
+    if (tile && tile->is_array() && tile->size() == 2 && blocks) {
+        d.tile_y = (int)(*tile)[0].as_i64();
+        d.tile_z = (int)(*tile)[1].as_i64();
+        d.rules_blocks_per_sm = (int)blocks->as_i64();
+    }
+}
+
 vca_ca_desc ca_desc(const Config& c) {
     vca_ca_desc d{};
     d.nx = c.space.nx;
@@ -211,6 +266,7 @@ vca_ca_desc ca_desc(const Config& c) {
     d.ponding = c.ca.ponding ? 1 : 0;
     d.sweep = c.ca.front ? VCA_SWEEP_ACTIVE : VCA_SWEEP_DENSE;
     d.device = device_ordinal();
+    apply_tuning(d, c);
     return d;
 }
 

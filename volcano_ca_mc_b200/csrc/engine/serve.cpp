@@ -525,6 +525,7 @@ private:
 }  // namespace
 
 int run_server(int workers, double budget_gb, bool batched) {
+    g_use_tuning = false;  // batch members keep the default tiles
     Server s(std::max(1, workers), (uint64_t)(budget_gb * 1024.0 * 1024.0 * 1024.0), batched);
     return s.run();
 }
