@@ -573,15 +573,24 @@ def ours(args):
     extra = {}
     cpu = None
     if rank == 0 and world == 1:
+        # the side measurements report their own failure; the headline line prints either way
+        def side(name, fn):
+            try:
+                return fn()
+            except Exception as e:  # noqa: BLE001
+                print(f"bench: {name} failed: {type(e).__name__}: {e}", file=sys.stderr, flush=True)
+                return {"failed": f"{type(e).__name__}: {str(e)[:300]}"}
+
         if not args.no_c2 and w.name != "c2":
-            extra["c2"] = workload_block(workloads.get("c2"), local, flush, peak, peak_kind)
-        extra["mc_full"] = mc_full_block(local, flush, peak, peak_kind)
-        extra.update(job_mixes(args, local))
-        eng = engine_cli(w)
+            extra["c2"] = side("c2", lambda: workload_block(workloads.get("c2"), local, flush, peak, peak_kind))
+        extra["mc_full"] = side("mc_full", lambda: mc_full_block(local, flush, peak, peak_kind))
+        mixes = side("job_mixes", lambda: job_mixes(args, local))
+        extra.update(mixes if "failed" not in mixes else {"job_mixes": mixes})
+        eng = side("engine_cli", lambda: engine_cli(w))
         if eng is not None:
             extra["engine_cli"] = eng
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline(w)
+            cpu = side("cpu_baseline", lambda: cpu_baseline(w))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -686,7 +686,11 @@ __device__ __forceinline__ uint32_t win_right(const uint8_t* p) {
 template <class S>
 __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKernelArgs& k, uint32_t bid, uint32_t nblk) {
     using RulesSlot = vca::RulesSlot<S>;
-    extern __shared__ __align__(128) uint8_t s_dyn[];
+    // Declared with the 16-byte alignment that dynamic shared memory is guaranteed to have, so that
+    // the rounding below is computed at run time: the dynamic part starts after the kernel's static
+    // shared variables, whose total need not be a multiple of 128 bytes (the batched kernel adds its
+    // member's arguments).
+    extern __shared__ __align__(16) uint8_t s_dyn[];
     // the slots start on a 128-byte boundary (TMA destinations); the launch adds 128 bytes of slack
     RulesSlot* slots = reinterpret_cast<RulesSlot*>(s_dyn + ((128u - (smem_u32(s_dyn) & 127u)) & 127u));
     __shared__ __align__(8) uint64_t s_bar[2];
