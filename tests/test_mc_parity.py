@@ -69,28 +69,53 @@ def test_basalt_sweeps_match_oracle(case):
     mc.close()
 
 
-@pytest.mark.parametrize("nb,bc,dims", [("moore", "periodic", (25, 1, 31)), ("von_neumann", "periodic", (24, 20, 1)),
-                                        ("pentagonal", "periodic", (15, 13, 11)), ("von_neumann", "periodic", (9, 10, 7))])
-def test_full_domain_sweeps_match_oracle(nb, bc, dims):
-    """mc.domain = full: all axes periodic, odd periodic axes give 3 classes (PottsMC.cpp:145-193)."""
+FULL_CASES = [
+    # nb, bc, dims, Q, mobility
+    ("moore", "periodic", (25, 1, 31), 20, False),
+    ("von_neumann", "periodic", (24, 20, 1), 20, False),
+    ("pentagonal", "periodic", (15, 13, 11), 20, False),
+    ("von_neumann", "periodic", (9, 10, 7), 20, False),
+    ("moore", "absorbing", (14, 12, 10), 256, False),
+    ("moore", "periodic", (16, 10, 12), 256, True),
+    ("hexagonal", "periodic", (21, 17, 1), 64, True),
+    ("von_neumann", "absorbing", (11, 9, 7), 40, True),
+    ("pentagonal", "absorbing", (12, 1, 13), 300, False),
+]
+
+
+@pytest.mark.parametrize("nb,bc,dims,Q,use_mob", FULL_CASES,
+                         ids=lambda c: str(c) if not isinstance(c, tuple) else "x".join(map(str, c)))
+def test_full_domain_sweeps_match_oracle(nb, bc, dims, Q, use_mob):
+    """mc.domain = full: odd periodic axes give 3 classes (PottsMC.cpp:145-193).  Q <= 256 runs the
+    whole-space sweeps on the byte copy of the orientations, Q = 300 the list sweeps."""
     nx, ny, nz = dims
     seed = 11 + nx
-    mp = O.mc_params(nx, ny, nz, nb, bc, True, seed, 20, 1.0, 0.4)
+    mp = O.mc_params(nx, ny, nz, nb, bc, True, seed, Q, 1.0, 0.4)
     domain = np.ones(nx * ny * nz, np.uint8)
     spin = O.mc_init(mp, domain)
-    mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood=nb, boundary=bc, domain_full=True, seed=seed, Q=20,
+    mob = None
+    if use_mob:
+        mob = np.random.default_rng(seed).uniform(0.05, 1.0, nx * ny * nz).astype(np.float32)
+    mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood=nb, boundary=bc, domain_full=True, seed=seed, Q=Q,
                                     kT=0.4))
     mc.set_domain(None)
+    if use_mob:
+        mc.set_mobility(mob)
     mc.initialize()
     assert mc.info().colors == O.mc_colors(mp)
     tot = np.zeros(3, np.uint64)
     for t in range(8):
-        tot += O.mc_sweep(mp, t, domain, None, spin)
+        tot += O.mc_sweep(mp, t, domain, mob, spin)
         mc.sweep(1)
         assert np.array_equal(mc.crystals(), spin), f"sweep {t + 1}"
+    # several sweeps in one call
+    for t in range(8, 11):
+        tot += O.mc_sweep(mp, t, domain, mob, spin)
+    mc.sweep(3)
+    assert np.array_equal(mc.crystals(), spin), "sweeps 9-11"
     info = mc.info()
     assert (info.attempts, info.accepted, info.uphill) == tuple(int(v) for v in tot)
-    assert mc.energy() == O.mc_energy(mp, 8, spin)
+    assert mc.energy() == O.mc_energy(mp, 11, spin)
     mc.close()
 
 

@@ -760,6 +760,16 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         nbuf = 0;
     };
     auto tile_at = [&](uint64_t i) -> uint32_t { return k.dense ? (uint32_t)i : k.tile_list[cur][i]; };
+    // Rules (not the plain copy) for a tile: its mark says LAVA lies within one tile.  A z slab's
+    // halo layers are rewritten by copies from the neighbouring slabs, which the marks never see, so
+    // there the tiles within one tile of a halo layer take the rules every step.
+    auto takes_rules = [&](uint32_t tile, uint32_t mark) -> bool {
+        if (mark == live_mark) return true;
+        if (!k.slab) return false;
+        int tx0, ty0, tz0;
+        tile_origin(g, tile, tx0, ty0, tz0);
+        return tz0 < k.own_z0 + g.TZ || tz0 + 2 * g.TZ > k.own_z1;
+    };
 
     // Fill a slot: TMA boxes by thread 0 (the slot's earlier stores must have been read first),
     // spill levels by the threads.
@@ -820,7 +830,7 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         vent_a = k.tile_flags[tile_a];
         if (i + G < count) tile_b = tile_at(i + G);
         if (i + 2 * G < count) tile_c = tile_at(i + 2 * G);
-        stage(0, tile_a, mark_a == live_mark);
+        stage(0, tile_a, takes_rules(tile_a, mark_a));
     }
     cp_async_commit();
     if (i + G < count) {
@@ -832,10 +842,10 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         const int si = it & 1;
         RulesSlot& sl = slots[si];
         const uint32_t tile = tile_a;
-        const bool rules = mark_a == live_mark;
+        const bool rules = takes_rules(tile_a, mark_a);
         const bool tile_vent = (vent_a & 2u) != 0;
         // next tile into the other slot, then the control loads of the tiles after it
-        if (i + G < count) stage(si ^ 1, tile_b, mark_b == live_mark);
+        if (i + G < count) stage(si ^ 1, tile_b, takes_rules(tile_b, mark_b));
         cp_async_commit();
         uint32_t mark_c = 0, vent_c = 0, tile_d = 0;
         if (i + 2 * G < count) {

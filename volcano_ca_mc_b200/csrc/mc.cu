@@ -292,9 +292,16 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
     }
 }
 
-// Colour classes of the domain list: colour c is list[off[c] .. off[c + 1]).
+// Colour classes of the domain list: colour c is list[off[c] .. off[c + 1]).  Thread i of the sweep
+// launch (T threads) takes the entries off[c] + i + k T, k < rounds[c], of colour c; with `cached`
+// set, each block keeps its threads' entries (and their mobilities) in shared memory for the whole
+// launch, round r of the launch at [round0[c] + k] x kMcThreads.
 struct McColors {
     int colors;
+    int cached;
+    int total_rounds;
+    int rounds[28];
+    int round0[28];
     uint64_t off[28];
 };
 
@@ -322,7 +329,7 @@ __device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks, unsigned long lo
                 atomicOr(&ctrl->error, 1);
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(20);
         }
         s_ok = ok;
     }
@@ -332,15 +339,31 @@ __device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks, unsigned long lo
 
 // `sweeps` checkerboard MCS in one cooperative launch: the colour classes in ascending order
 // (sweepColors, PottsMC.cpp:495-514), a grid barrier after each, the same trial as mc_color_kernel
-// (colorTrials, PottsMC.cpp:394-493).  Replaces `sweeps` x `colors` launches; for domains of a few
-// hundred thousand cells the launches, not the trials, were the cost.
-template <bool kMobility, bool kRandomNb, bool kBatched>
-__global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel(McArgs a, McColors col, int sweeps) {
+// (colorTrials, PottsMC.cpp:394-493).  Replaces `sweeps` x `colors` launches.  A colour pass costs
+// the latency of its rounds: per trial the entry and mobility come from shared memory (staged once
+// per launch), the cell's spin and all its neighbours' spins are loaded together (one round trip to
+// L2), then the decision and the store.
+template <bool kMobility, bool kRandomNb>
+__global__ __launch_bounds__(kMcThreads, 2) void mc_sweeps_kernel(McArgs a, McColors col, int sweeps) {
+    extern __shared__ __align__(16) uint32_t s_ent[];  // [total_rounds][kMcThreads] entries, then mobilities
     __shared__ unsigned long long s_table[kTableSide * kTableSide];
     __shared__ unsigned long long s_red[3][kMcThreads / 32];
     __shared__ NbTable s_nb;
     for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
     stage_nb(a, s_nb);
+    const uint64_t T = (uint64_t)gridDim.x * kMcThreads;
+    const uint64_t me = (uint64_t)blockIdx.x * kMcThreads + threadIdx.x;
+    float* s_mob = reinterpret_cast<float*>(s_ent + (size_t)col.total_rounds * kMcThreads);
+    if (col.cached) {
+        for (int c = 0; c < col.colors; ++c)
+            for (int k = 0; k < col.rounds[c]; ++k) {
+                const uint64_t j = col.off[c] + me + (uint64_t)k * T;
+                const int slot = (col.round0[c] + k) * kMcThreads + threadIdx.x;
+                const bool in = j < col.off[c + 1];
+                s_ent[slot] = in ? a.list[j] : 0xFFFFFFFFu;
+                if (kMobility) s_mob[slot] = in ? a.list_mob[j] : 0.f;
+            }
+    }
     __syncthreads();
     McCtrl* ctrl = a.ctrl;
     const uint32_t t0 = ctrl->sweeps;
@@ -351,13 +374,23 @@ __global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel
     for (int s = 0; s < sweeps && ok; ++s) {
         const uint64_t prefix = hash_prefix(a.seed, t0 + (uint32_t)s);
         for (int c = 0; c < col.colors && ok; ++c) {
-            const uint64_t b = col.off[c], e = col.off[c + 1];
-            for (uint64_t j = b + blockIdx.x * (uint64_t)kMcThreads + threadIdx.x; j < e; j += (uint64_t)gridDim.x * kMcThreads) {
-                const uint32_t g = a.list[j];
+            for (int k = 0; k < col.rounds[c]; ++k) {
+                uint32_t g;
+                float mob = 0.f;
+                if (col.cached) {
+                    const int slot = (col.round0[c] + k) * kMcThreads + threadIdx.x;
+                    g = s_ent[slot];
+                    if (kMobility) mob = s_mob[slot];
+                } else {
+                    const uint64_t j = col.off[c] + me + (uint64_t)k * T;
+                    g = j < col.off[c + 1] ? a.list[j] : 0xFFFFFFFFu;
+                    if (kMobility && g != 0xFFFFFFFFu) mob = a.list_mob[j];
+                }
+                if (g == 0xFFFFFFFFu) continue;
                 const uint64_t h = hash_index(prefix, g + a.gidx_base);
                 if (kMobility) {
                     const uint64_t r = hash_salt(h, kSaltMcMobility);
-                    if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)a.list_mob[j]) continue;
+                    if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)mob) continue;
                 }
                 ++my_att;
                 int var = 0;
@@ -368,10 +401,7 @@ __global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel
                 int32_t prop = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
                 if (prop >= cur) ++prop;
                 int in_dom, same_a, same_b;
-                if (kBatched)
-                    nb_counts(a, nb, var, x, y, z, g, cur, prop, in_dom, same_a, same_b);
-                else
-                    nb_counts_loop(a, nb, var, x, y, z, cur, prop, in_dom, same_a, same_b);
+                nb_counts(a, nb, var, x, y, z, g, cur, prop, in_dom, same_a, same_b);
                 const unsigned long long th = s_table[(in_dom - same_a) * kTableSide + (in_dom - same_b)];
                 bool accept;
                 if (th >> 63) {
@@ -415,6 +445,169 @@ __global__ __launch_bounds__(kMcThreads, kBatched ? 2 : 1) void mc_sweeps_kernel
         }
         if (su) atomicAdd(&ctrl->uphill, su);
         // every block passed the last barrier, so no block reads ctrl->sweeps any more
+        if (blockIdx.x == 0 && ok) ctrl->sweeps = t0 + (uint32_t)sweeps;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Whole-space domain (mc.domain = full, every cell a trial each MCS) with Q <= 256: the sweeps run on
+// a one-byte copy of the orientations (orientation - 1, so 67 M cells take 67 MB and stay in L2) and
+// enumerate the cells of each colour class directly instead of reading a list.  A cell's neighbours
+// are loaded at fixed linear offsets when the cell is away from every face (no wrap or frame test),
+// else through the frame as everywhere else.  Same trials, same order of colours, same results.
+// ------------------------------------------------------------------------------------------
+struct McDense {
+    uint8_t* sp;             // orientation - 1 of every cell
+    const float* mob;        // mobility of every cell (kMobility)
+    int cnt[3][3];           // per axis and class: coordinates of the class
+    FastDiv32 div[2][3];     // / cnt[0][c] and / cnt[1][c]
+    int delta[6][26];        // linear offsets of each variant's neighbours
+};
+
+// Coordinate i of class c on an axis of n cells split into `classes` classes (axisClass,
+// PottsMC.cpp:145-151): every coordinate (1 class), c + 2 i (classes 0 and 1), the last cell (class 2
+// of a periodic odd axis).
+__device__ __forceinline__ int class_coord(int i, int c, int classes, int n) {
+    return classes == 1 ? i : (c == 2 ? n - 1 : 2 * i + c);
+}
+
+__global__ void mc_pack8_kernel(const int32_t* spin, uint8_t* sp, uint64_t n) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x)
+        sp[g] = (uint8_t)(spin[g] - 1);
+}
+__global__ void mc_unpack8_kernel(const uint8_t* sp, int32_t* spin, uint64_t n) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n; g += (uint64_t)gridDim.x * blockDim.x)
+        spin[g] = (int32_t)sp[g] + 1;
+}
+
+template <bool kMobility, bool kRandomNb, bool kParity>
+__global__ __launch_bounds__(kMcThreads, 2) void mc_dense_sweeps_kernel(McArgs a, McDense d, int sweeps) {
+    __shared__ unsigned long long s_table[kTableSide * kTableSide];
+    __shared__ unsigned long long s_red[3][kMcThreads / 32];
+    __shared__ NbTable s_nb;
+    __shared__ int s_delta[6][26];
+    for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
+    for (int i = threadIdx.x; i < 6 * 26; i += kMcThreads) s_delta[i / 26][i % 26] = d.delta[i / 26][i % 26];
+    stage_nb(a, s_nb);
+    __syncthreads();
+    McCtrl* ctrl = a.ctrl;
+    const uint32_t t0 = ctrl->sweeps;
+    const NbTable& nb = s_nb;
+    const uint8_t* sp = d.sp;
+    const uint64_t T = (uint64_t)gridDim.x * kMcThreads;
+    const uint64_t me = (uint64_t)blockIdx.x * kMcThreads + threadIdx.x;
+    const int colors = kParity ? 2 : a.classes[0] * a.classes[1] * a.classes[2];
+    unsigned long long my_att = 0, my_acc = 0, my_up = 0;
+    bool ok = true;
+    unsigned long long epoch = 0;
+    for (int s = 0; s < sweeps && ok; ++s) {
+        const uint64_t prefix = hash_prefix(a.seed, t0 + (uint32_t)s);
+        for (int c = 0; c < colors && ok; ++c) {
+            int cx = 0, cy = 0, cz = 0;
+            if (!kParity) {
+                cx = c % a.classes[0];
+                const int r = c / a.classes[0];
+                cy = r % a.classes[1];
+                cz = r / a.classes[1];
+            }
+            const uint32_t nxc = (uint32_t)d.cnt[0][cx], nyc = (uint32_t)d.cnt[1][cy];
+            const uint64_t total = (uint64_t)nxc * nyc * (uint32_t)d.cnt[2][cz];
+            for (uint64_t i = me; i < total; i += T) {
+                uint32_t ix, iy;
+                const uint32_t r = fast_divmod((uint32_t)i, d.div[0][cx], ix);
+                const uint32_t iz = fast_divmod(r, d.div[1][cy], iy);
+                int x, y, z;
+                if (kParity) {
+                    y = (int)iy;
+                    z = (int)iz;
+                    x = 2 * (int)ix + ((c + y + z + a.zoff) & 1);
+                    if (x >= a.nx) continue;
+                } else {
+                    x = class_coord((int)ix, cx, a.classes[0], a.nx);
+                    y = class_coord((int)iy, cy, a.classes[1], a.ny);
+                    z = class_coord((int)iz, cz, a.classes[2], a.nz);
+                }
+                const uint32_t g = (uint32_t)x + (uint32_t)a.nx * ((uint32_t)y + (uint32_t)a.ny * (uint32_t)z);
+                const uint64_t h = hash_index(prefix, g + a.gidx_base);
+                if (kMobility) {
+                    const uint64_t rr = hash_salt(h, kSaltMcMobility);
+                    if (__dmul_rn((double)(rr >> 11), 1.0 / 9007199254740992.0) >= (double)d.mob[g]) continue;
+                }
+                ++my_att;
+                int var = 0;
+                if (kRandomNb) var = (int)fast_mod(hash_salt(h, kSaltNeighborhood), a.var_mod);
+                const int cur = (int)sp[g] + 1;
+                int prop = 1 + (int)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
+                if (prop >= cur) ++prop;
+                const uint32_t cb = (uint32_t)(cur - 1), pb = (uint32_t)(prop - 1);
+                const int cnt = nb.count[var];
+                const bool inner = (a.nx == 1 || (x >= 1 && x <= a.nx - 2)) && (a.ny == 1 || (y >= 1 && y <= a.ny - 2)) &&
+                                   (a.nz == 1 || (z >= 1 && z <= a.nz - 2));
+                int in_dom = 0, same_a = 0, same_b = 0;
+                if (inner) {
+                    in_dom = cnt;
+#pragma unroll
+                    for (int k = 0; k < 26; ++k) {
+                        if (k < cnt) {
+                            const uint32_t v = sp[(int64_t)g + s_delta[var][k]];
+                            same_a += v == cb;
+                            same_b += v == pb;
+                        }
+                    }
+                } else {
+                    for (int k = 0; k < cnt; ++k) {
+                        int sx = x + nb.off[var][k][0], sy = y + nb.off[var][k][1], sz = z + nb.off[var][k][2];
+                        if (!mc_wrap1_sel(sx, a.nx, a.per[0]) || !mc_wrap1_sel(sy, a.ny, a.per[1]) ||
+                            !mc_wrap1_sel(sz, a.nz, a.per[2]))
+                            continue;
+                        const uint32_t v = sp[(uint32_t)sx + (uint32_t)a.nx * ((uint32_t)sy + (uint32_t)a.ny * (uint32_t)sz)];
+                        ++in_dom;
+                        same_a += v == cb;
+                        same_b += v == pb;
+                    }
+                }
+                const unsigned long long th = s_table[(in_dom - same_a) * kTableSide + (in_dom - same_b)];
+                bool accept;
+                if (th >> 63) {
+                    accept = true;
+                } else {
+                    accept = th != 0 && (hash_salt(h, kSaltMcAccept) >> 11) < th;
+                    my_up += accept ? 1u : 0u;
+                }
+                if (accept) {
+                    d.sp[g] = (uint8_t)pb;
+                    ++my_acc;
+                }
+            }
+            ok = mc_grid_barrier(ctrl, gridDim.x, ++epoch);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long ra = my_att, rc = my_acc, ru = my_up;
+    for (int off = 16; off > 0; off >>= 1) {
+        ra += __shfl_down_sync(0xFFFFFFFFu, ra, off);
+        rc += __shfl_down_sync(0xFFFFFFFFu, rc, off);
+        ru += __shfl_down_sync(0xFFFFFFFFu, ru, off);
+    }
+    if (lane == 0) {
+        s_red[0][warp] = ra;
+        s_red[1][warp] = rc;
+        s_red[2][warp] = ru;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long sa = 0, sc = 0, su = 0;
+        for (int w = 0; w < kMcThreads / 32; ++w) {
+            sa += s_red[0][w];
+            sc += s_red[1][w];
+            su += s_red[2][w];
+        }
+        if (sa) atomicAdd(&ctrl->attempts, sa);
+        if (sc) {
+            atomicAdd(&ctrl->accepted, sc);
+            atomicAdd(&ctrl->sweep_accepted, sc);
+        }
+        if (su) atomicAdd(&ctrl->uphill, su);
         if (blockIdx.x == 0 && ok) ctrl->sweeps = t0 + (uint32_t)sweeps;
     }
 }
@@ -701,6 +894,7 @@ struct vca_mc {
     int profile_kernels = 0;
     std::vector<cudaEvent_t> prof_events;
     int slab_zoff = -1;                  // z slab of a taller grid (vca_mc_set_slab), -1: none
+    uint8_t* sp8 = nullptr;              // orientation - 1 per cell, for the whole-space sweeps (cap_n bytes)
 };
 
 namespace {
@@ -770,6 +964,7 @@ void mc_free(vca_mc* h) {
     cudaFree(h->gsize);
     cudaFree(h->ghigh);
     cudaFree(h->gacc);
+    cudaFree(h->sp8);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
@@ -779,32 +974,103 @@ void mc_free(vca_mc* h) {
 
 using SweepsKernel = void (*)(McArgs, McColors, int);
 
-template <bool kBatched>
 SweepsKernel sweeps_kernel_of(const vca_mc* h) {
     const bool random_nb = h->nb_host.variants > 1;
-    if (h->mobility_on) return random_nb ? mc_sweeps_kernel<true, true, kBatched> : mc_sweeps_kernel<true, false, kBatched>;
-    return random_nb ? mc_sweeps_kernel<false, true, kBatched> : mc_sweeps_kernel<false, false, kBatched>;
+    if (h->mobility_on) return random_nb ? mc_sweeps_kernel<true, true> : mc_sweeps_kernel<true, false>;
+    return random_nb ? mc_sweeps_kernel<false, true> : mc_sweeps_kernel<false, false>;
 }
 
-// The sweep kernel and its cooperative grid (all blocks resident at once, no more than the largest
-// colour needs).  When every cell of the largest colour gets a thread of its own in the batched
-// form, a colour pass is one trial's latency: batched neighbour loads.  Otherwise each thread has
-// several cells and the loop form, with more resident warps per SM, hides the latency better.
-vca_status sweeps_launch_shape(vca_mc* h, SweepsKernel* kernel, int* grid) {
+constexpr size_t kMcEntryCacheMax = 160 * 1024;  // shared memory a block may spend on its entries
+
+// The sweep kernel's cooperative grid (all blocks resident at once, no more blocks than the widest
+// colour needs), its rounds per colour, and whether the blocks' entries fit in shared memory at
+// that occupancy (then the dynamic shared memory size in *smem).
+vca_status sweeps_launch_shape(vca_mc* h, SweepsKernel kernel, McColors* col, int* grid, size_t* smem) {
     uint64_t widest = 0;
     for (int c = 0; c < h->colors; ++c) widest = std::max<uint64_t>(widest, h->color_off[c + 1] - h->color_off[c]);
     const uint64_t need = std::max<uint64_t>(1, (widest + kMcThreads - 1) / kMcThreads);
-    int per_sm = 0;
-    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweeps_kernel_of<true>(h), kMcThreads, 0));
-    if (need <= (uint64_t)h->sms * std::max(1, per_sm)) {
-        *kernel = sweeps_kernel_of<true>(h);
-        *grid = (int)need;
+    const size_t per_entry = h->mobility_on ? 8 : 4;
+    VCA_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMcEntryCacheMax));
+    int per_sm_max = 0;
+    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_max, kernel, kMcThreads, 0));
+    per_sm_max = std::max(1, per_sm_max);
+    auto rounds_for = [&](uint64_t threads) {
+        int total = 0;
+        for (int c = 0; c < h->colors; ++c) {
+            const uint64_t n = h->color_off[c + 1] - h->color_off[c];
+            col->rounds[c] = (int)((n + threads - 1) / threads);
+            col->round0[c] = total;
+            total += col->rounds[c];
+        }
+        col->total_rounds = total;
+    };
+    for (int per_sm = per_sm_max; per_sm >= 1; --per_sm) {
+        const int g = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * per_sm));
+        rounds_for((uint64_t)g * kMcThreads);
+        const size_t bytes = (size_t)col->total_rounds * kMcThreads * per_entry;
+        if (bytes > kMcEntryCacheMax) continue;
+        int fit = 0;
+        VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kernel, kMcThreads, bytes));
+        if ((uint64_t)fit * h->sms < (uint64_t)g) continue;
+        col->cached = 1;
+        *grid = g;
+        *smem = bytes;
         return VCA_OK;
     }
-    VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweeps_kernel_of<false>(h), kMcThreads, 0));
-    *kernel = sweeps_kernel_of<false>(h);
-    *grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * std::max(1, per_sm)));
+    // entries from global memory at full occupancy
+    const int g = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * per_sm_max));
+    rounds_for((uint64_t)g * kMcThreads);
+    col->cached = 0;
+    *grid = g;
+    *smem = 0;
     return VCA_OK;
+}
+
+using DenseKernel = void (*)(McArgs, McDense, int);
+
+template <bool kParity>
+DenseKernel dense_kernel_of(const vca_mc* h) {
+    const bool random_nb = h->nb_host.variants > 1;
+    if (h->mobility_on)
+        return random_nb ? mc_dense_sweeps_kernel<true, true, kParity> : mc_dense_sweeps_kernel<true, false, kParity>;
+    return random_nb ? mc_dense_sweeps_kernel<false, true, kParity> : mc_dense_sweeps_kernel<false, false, kParity>;
+}
+
+// The whole-space sweeps apply when every cell is in the domain and an orientation fits a byte.
+bool dense_applies(const vca_mc* h) {
+    return !h->profile_kernels && h->slab_zoff < 0 && h->desc.Q <= 256 && !h->color_off.empty() &&
+           h->color_off.back() == h->n && h->n > 0;
+}
+
+McDense dense_args(const vca_mc* h) {
+    McDense d;
+    std::memset(&d, 0, sizeof(d));
+    d.sp = h->sp8;
+    d.mob = h->mobility_on ? h->mobility : nullptr;
+    const int dims[3] = {h->desc.nx, h->desc.ny, h->desc.nz};
+    for (int a = 0; a < 3; ++a) {
+        const int n = dims[a];
+        int* c = d.cnt[a];
+        c[0] = c[1] = c[2] = 1;
+        if (h->parity_colors) {
+            c[0] = a == 0 ? (n + 1) / 2 : n;
+        } else if (h->classes[a] == 1) {
+            c[0] = n;
+        } else if (h->classes[a] == 2) {
+            c[0] = (n + 1) / 2;
+            c[1] = n / 2;
+        } else {
+            c[0] = c[1] = (n - 1) / 2;
+            c[2] = 1;
+        }
+    }
+    for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < 3; ++c) d.div[a][c] = make_fastdiv32((uint32_t)std::max(1, d.cnt[a][c]));
+    const NbTable& nb = h->nb_host;
+    for (int v = 0; v < nb.variants && v < 6; ++v)
+        for (int k = 0; k < nb.count[v]; ++k)
+            d.delta[v][k] = nb.off[v][k][0] + dims[0] * (nb.off[v][k][1] + dims[1] * nb.off[v][k][2]);
+    return d;
 }
 
 }  // namespace
@@ -1139,14 +1405,35 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
         col.colors = h->colors;
         for (int c = 0; c <= h->colors; ++c) col.off[c] = h->color_off[c];
         int grid = 1;
-        SweepsKernel kernel = nullptr;
-        if (vca_status s = sweeps_launch_shape(h, &kernel, &grid)) return s;
+        size_t smem = 0;
+        SweepsKernel kernel = sweeps_kernel_of(h);
+        if (vca_status s = sweeps_launch_shape(h, kernel, &col, &grid, &smem)) return s;
+        const bool dense = dense_applies(h);
+        if (dense && !h->sp8) VCA_CUDA(cudaMalloc(&h->sp8, h->cap_n));
         VCA_CUDA(cudaEventRecord(h->ev_a, h->stream));
-        if (count > 0 && h->color_off.back() > 0) {
+        if (count > 0 && dense) {
+            // whole space: sweeps on the byte copy of the orientations, copied back after
+            const McDense d = dense_args(h);
+            DenseKernel dk = h->parity_colors ? dense_kernel_of<true>(h) : dense_kernel_of<false>(h);
+            int per_sm = 0;
+            VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dk, kMcThreads, 0));
+            const int dgrid = h->sms * std::max(1, per_sm);
+            const int blocks = grid_for(h->n, h->sms);
+            mc_pack8_kernel<<<blocks, 256, 0, h->stream>>>(h->spin, h->sp8, h->n);
+            VCA_CUDA(cudaGetLastError());
+            int n = count;
+            McDense dd = d;
+            void* args[] = {&a, &dd, &n};
+            VCA_CUDA(cudaMemsetAsync(&h->ctrl->bar_arrived, 0, sizeof(unsigned long long), h->stream));
+            VCA_CUDA(cudaLaunchCooperativeKernel((const void*)dk, dgrid, kMcThreads, args, 0, h->stream));
+            mc_unpack8_kernel<<<blocks, 256, 0, h->stream>>>(h->sp8, h->spin, h->n);
+            VCA_CUDA(cudaGetLastError());
+            h->launches += 3;
+        } else if (count > 0 && h->color_off.back() > 0) {
             int n = count;
             void* args[] = {&a, &col, &n};
             VCA_CUDA(cudaMemsetAsync(&h->ctrl->bar_arrived, 0, sizeof(unsigned long long), h->stream));
-            VCA_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, grid, kMcThreads, args, 0, h->stream));
+            VCA_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, grid, kMcThreads, args, smem, h->stream));
             h->launches += 1;
         } else if (count > 0) {
             // empty domain: the sweeps still count (sweepsDone)
