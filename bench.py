@@ -67,9 +67,10 @@ def parse():
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[20.0, 60.0, 120.0, 240.0],
                     help="arrival rates [jobs/s] of the served sweep")
     ap.add_argument("--sweep-seconds", type=float, default=4.0, help="length of each trace of the served sweep")
-    ap.add_argument("--profile-job", choices=["active", "dense", "mc"], default=None,
+    ap.add_argument("--profile-job", choices=["active", "dense", "mc", "mcfull"], default=None,
                     help="run exactly one CA job with this schedule (no warm-up, no MC), or with mc one ACTIVE "
-                         "CA job and its MC stage, and exit: the case ncu captures")
+                         "CA job and its MC stage, or with mcfull the whole-space MC case (--max-steps sweeps), "
+                         "and exit: the case ncu captures")
     ap.add_argument("--max-steps", type=int, default=None, help="with --profile-job: stop the CA after this many steps")
     ap.add_argument("--slabs", action="store_true",
                     help="with --gpus N > 1: one grid of the workload split into N z slabs (strong scaling, halo "
@@ -680,6 +681,19 @@ def reference(args):
 def profile_job(args):
     """One CA job of the workload, nothing else: a bounded case for ncu."""
     from volcano_ca_mc_b200 import capi, workloads
+    if args.profile_job == "mcfull":
+        nx, ny, nz = 512, 512, 256
+        sweeps = args.max_steps or 4
+        mc = capi.PottsMC(capi.McParams(nx, ny, nz, neighborhood="moore", boundary="periodic", domain_full=True,
+                                        seed=9, Q=64, J=1.0, kT=0.5, device=0))
+        mc.set_domain(None)
+        mc.initialize()
+        mc.sweep(sweeps)
+        mi = mc.info()
+        print(json.dumps({"profile_job": "mcfull", "space": [nx, ny, nz], "sweeps": mi.sweeps,
+                          "ms": mc.timing()[0]}))
+        mc.close()
+        return
     w = workloads.get(args.workload)
     if args.max_steps is not None:
         w.max_steps = args.max_steps

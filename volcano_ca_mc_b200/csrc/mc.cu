@@ -89,43 +89,8 @@ __device__ __forceinline__ int32_t spin_at(const McArgs& a, int x, int y, int z)
     return a.spin[(uint64_t)x + (uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z)];
 }
 
-// mc_wrap for a neighbour one cell away, as selects (no branch), so that the loads of all
-// neighbours of a cell can be issued together.  v is only meaningful when the result is true.
-__device__ __forceinline__ bool mc_wrap1_sel(int& v, int n, int periodic) {
-    const bool in = (unsigned)v < (unsigned)n;
-    const int w = v < 0 ? v + n : v - n;
-    v = in ? v : w;
-    return in | ((periodic != 0) & (n > 1));
-}
-
 // unlikeBeforeAfter's neighbour counts (PottsMC.cpp:394-430, PottsMC.hpp:191-204) for the cell
-// (x, y, z) = globalIndex g and variant var: neighbours in the domain (spin != 0) and those equal to
-// cur / prop.  The offsets come from the block's copy of the table and the loads go out together;
-// a neighbour outside the frame reads the cell itself and counts as spin 0.
-__device__ __forceinline__ void nb_counts(const McArgs& a, const NbTable& nb, int var, int x, int y, int z, uint32_t g,
-                                          int32_t cur, int32_t prop, int& in_dom, int& same_a, int& same_b) {
-    const int cnt = nb.count[var];
-    int32_t sv[26];
-#pragma unroll
-    for (int k = 0; k < 26; ++k) {
-        int sx = x + nb.off[var][k][0], sy = y + nb.off[var][k][1], sz = z + nb.off[var][k][2];
-        const bool ok = (k < cnt) & mc_wrap1_sel(sx, a.nx, a.per[0]) & mc_wrap1_sel(sy, a.ny, a.per[1]) &
-                        mc_wrap1_sel(sz, a.nz, a.per[2]);
-        // globalIndex fits 32 bits (at most 2e9 cells)
-        const uint32_t idx = ok ? (uint32_t)sx + (uint32_t)a.nx * ((uint32_t)sy + (uint32_t)a.ny * (uint32_t)sz) : g;
-        const int32_t v = a.spin[idx];
-        sv[k] = ok ? v : 0;
-    }
-    in_dom = same_a = same_b = 0;
-#pragma unroll
-    for (int k = 0; k < 26; ++k) {
-        in_dom += sv[k] != 0;
-        same_a += sv[k] == cur;
-        same_b += sv[k] == prop;
-    }
-}
-// The same counts one neighbour after another: fewer registers, for grids where each thread has
-// several cells and the SM hides the latency with more resident warps.
+// (x, y, z) and variant var, one neighbour after another through the frame (the per-colour launches).
 __device__ __forceinline__ void nb_counts_loop(const McArgs& a, const NbTable& nb, int var, int x, int y, int z,
                                                int32_t cur, int32_t prop, int& in_dom, int& same_a, int& same_b) {
     in_dom = same_a = same_b = 0;
@@ -292,6 +257,60 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
     }
 }
 
+// Offsets (index 0: coordinate - 1, 1: the cell, 2: coordinate + 1, times `stride`) and presence of
+// the two neighbours of coordinate c on an axis of n cells: wrapped on a periodic axis (a 2-cell axis
+// sees its other cell on both sides), absent at the frame otherwise (PottsMC::fillFrame,
+// PottsMC.cpp:226-277).
+__device__ __forceinline__ void mc_axis_nb(int c, int n, int per, int64_t stride, int64_t o[3], bool k[3]) {
+    const bool wrap = per && n > 1;
+    o[0] = c > 0 ? -stride : (int64_t)(n - 1) * stride;
+    o[1] = 0;
+    o[2] = c < n - 1 ? stride : -(int64_t)(n - 1) * stride;
+    k[0] = c > 0 || wrap;
+    k[1] = true;
+    k[2] = c < n - 1 || wrap;
+}
+
+// unlikeBeforeAfter's counts (PottsMC.cpp:394-430) of the cell g = (x, y, z) over the neighbours
+// whose bit (dx + 1) + 3 (dy + 1) + 9 (dz + 1) is set in `mask` (the variant's neighbourhood), on one
+// path for every cell: nine row addresses and three x offsets, wrapped on periodic axes, a missing
+// neighbour (frame) read as `none`.  All loads of the cell go out together.  A neighbour counts as in
+// the domain when its value is not `none` (orientations: 0 outside the domain; the byte copy of a
+// whole-space domain: every existing cell).
+template <typename T>
+__device__ __forceinline__ void mc_count_block(const McArgs& a, const T* base, uint32_t g, int x, int y, int z, uint32_t mask,
+                                               uint32_t none, uint32_t cur, uint32_t prop, int& in_dom, int& same_a,
+                                               int& same_b) {
+    int64_t ox[3], oy[3], oz[3];
+    bool kx[3], ky[3], kz[3];
+    mc_axis_nb(x, a.nx, a.per[0], 1, ox, kx);
+    mc_axis_nb(y, a.ny, a.per[1], a.nx, oy, ky);
+    mc_axis_nb(z, a.nz, a.per[2], (int64_t)a.nx * a.ny, oz, kz);
+    const T* p = base + g;
+    uint32_t sv[27];
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) {
+            const T* r = p + oz[dz] + oy[dy];
+            const bool rk = kz[dz] && ky[dy];
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int bit = dx + 3 * dy + 9 * dz;
+                const bool k = rk && kx[dx] && ((mask >> bit) & 1u);
+                sv[bit] = k ? (uint32_t)r[ox[dx]] : none;
+            }
+        }
+    in_dom = same_a = same_b = 0;
+#pragma unroll
+    for (int bit = 0; bit < 27; ++bit) {
+        if (bit == 13) continue;  // the cell itself
+        in_dom += sv[bit] != none;
+        same_a += sv[bit] == cur;
+        same_b += sv[bit] == prop;
+    }
+}
+
 // Colour classes of the domain list: colour c is list[off[c] .. off[c + 1]).  Thread i of the sweep
 // launch (T threads) takes the entries off[c] + i + k T, k < rounds[c], of colour c; with `cached`
 // set, each block keeps its threads' entries (and their mobilities) in shared memory for the whole
@@ -299,24 +318,29 @@ __global__ __launch_bounds__(kMcThreads) void mc_color_kernel(McArgs a, const ui
 struct McColors {
     int colors;
     int cached;
+    int pre;           // cached and at most kPreRounds rounds per colour: draws computed a pass ahead
     int total_rounds;
     int rounds[28];
     int round0[28];
     uint64_t off[28];
+    uint32_t mask[6];  // per variant: bit (dx + 1) + 3 (dy + 1) + 9 (dz + 1) of each neighbour
 };
 
-// Grid barrier of the cooperative sweep launch.  Thread 0 of each block adds one arrival with
-// release semantics (the block's writes, ordered before it by __syncthreads, become visible with
-// it) and polls the count with acquire loads until every block has arrived `epoch` times; the count
-// only grows during a launch and is zeroed before it.  The wait is bounded; a block that gives up,
-// or sees that another gave up, returns false (ctrl->error is then set).
-__device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks, unsigned long long epoch) {
+// Grid barrier of the cooperative sweep launches, in two halves so that a block can do work of its
+// own between them.  Arrive: after __syncthreads (the block's writes of the pass are ordered before
+// it), thread 0 adds one arrival with release semantics.  Wait: thread 0 polls the count with
+// acquire loads until every block has arrived `epoch` times, then __syncthreads.  The count only
+// grows during a launch and is zeroed before it.  The wait is bounded; a block that gives up, or
+// sees that another gave up, returns false (ctrl->error is then set).
+__device__ __forceinline__ void mc_barrier_arrive(McCtrl* ctrl) {
     __syncthreads();
+    if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.u64 [%0], 1;\n" ::"l"(&ctrl->bar_arrived) : "memory");
+}
+__device__ bool mc_barrier_wait(McCtrl* ctrl, unsigned nblocks, unsigned long long epoch) {
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
-        unsigned long long* cnt = &ctrl->bar_arrived;
+        const unsigned long long* cnt = &ctrl->bar_arrived;
         volatile int* err = &ctrl->error;
-        asm volatile("red.release.gpu.global.add.u64 [%0], 1;\n" ::"l"(cnt) : "memory");
         const unsigned long long target = epoch * nblocks;
         int ok = 1;
         long long spins = 0;
@@ -337,23 +361,53 @@ __device__ bool mc_grid_barrier(McCtrl* ctrl, unsigned nblocks, unsigned long lo
     return s_ok != 0;
 }
 
+// The random draws of one trial (hashRand of its sweep and cell: mobility test, neighbourhood
+// variant, proposed orientation, acceptance number), which do not depend on any orientation.
+struct McDraws {
+    bool attempt;     // passed the mobility test
+    int var;          // neighbourhood variant
+    int32_t prop_raw; // 1 + r % (Q - 1), before the skip over the current orientation
+    uint64_t acc;     // hashRand(..., McAccept)
+};
+template <bool kMobility, bool kRandomNb>
+__device__ __forceinline__ McDraws mc_draws(const McArgs& a, uint64_t prefix, uint32_t g, float mob) {
+    McDraws d;
+    const uint64_t h = hash_index(prefix, g + a.gidx_base);
+    d.attempt = true;
+    if (kMobility) {
+        const uint64_t r = hash_salt(h, kSaltMcMobility);
+        d.attempt = __dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) < (double)mob;
+    }
+    d.var = kRandomNb ? (int)fast_mod(hash_salt(h, kSaltNeighborhood), a.var_mod) : 0;
+    d.prop_raw = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
+    d.acc = hash_salt(h, kSaltMcAccept);
+    return d;
+}
+
 // `sweeps` checkerboard MCS in one cooperative launch: the colour classes in ascending order
 // (sweepColors, PottsMC.cpp:495-514), a grid barrier after each, the same trial as mc_color_kernel
 // (colorTrials, PottsMC.cpp:394-493).  Replaces `sweeps` x `colors` launches.  A colour pass costs
-// the latency of its rounds: per trial the entry and mobility come from shared memory (staged once
-// per launch), the cell's spin and all its neighbours' spins are loaded together (one round trip to
-// L2), then the decision and the store.
+// the latency of its rounds: the entry and mobility come from shared memory (staged once per
+// launch); the draws of the trial were computed while the block waited at the previous barrier
+// (col.pre: kept in shared memory, one slot per thread and round); the cell's spin and all its
+// neighbours' spins are loaded together (one round trip to L2), then the decision and the store.
+constexpr int kPreRounds = 4;  // rounds per colour whose draws are computed ahead
 template <bool kMobility, bool kRandomNb>
-__global__ __launch_bounds__(kMcThreads, 2) void mc_sweeps_kernel(McArgs a, McColors col, int sweeps) {
-    extern __shared__ __align__(16) uint32_t s_ent[];  // [total_rounds][kMcThreads] entries, then mobilities
+__global__ __launch_bounds__(kMcThreads, 2) void mc_sweeps_kernel(const __grid_constant__ McArgs a,
+                                                                  const __grid_constant__ McColors col, int sweeps) {
+    // [total_rounds][kMcThreads] entries, then mobilities; then with col.pre the draws of the next
+    // pass: [kPreRounds][kMcThreads] acceptance numbers, proposals, flags (bit 7 attempt, variant)
+    extern __shared__ __align__(16) uint32_t s_ent[];
     __shared__ unsigned long long s_table[kTableSide * kTableSide];
     __shared__ unsigned long long s_red[3][kMcThreads / 32];
-    __shared__ NbTable s_nb;
     for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
-    stage_nb(a, s_nb);
     const uint64_t T = (uint64_t)gridDim.x * kMcThreads;
     const uint64_t me = (uint64_t)blockIdx.x * kMcThreads + threadIdx.x;
+    const size_t cache_words = (size_t)col.total_rounds * kMcThreads * (kMobility ? 2 : 1);
     float* s_mob = reinterpret_cast<float*>(s_ent + (size_t)col.total_rounds * kMcThreads);
+    uint64_t* s_pacc = reinterpret_cast<uint64_t*>(s_ent + cache_words);
+    int32_t* s_pprop = reinterpret_cast<int32_t*>(s_pacc + kPreRounds * kMcThreads);
+    uint8_t* s_pflag = reinterpret_cast<uint8_t*>(s_pprop + kPreRounds * kMcThreads);
     if (col.cached) {
         for (int c = 0; c < col.colors; ++c)
             for (int k = 0; k < col.rounds[c]; ++k) {
@@ -367,10 +421,24 @@ __global__ __launch_bounds__(kMcThreads, 2) void mc_sweeps_kernel(McArgs a, McCo
     __syncthreads();
     McCtrl* ctrl = a.ctrl;
     const uint32_t t0 = ctrl->sweeps;
-    const NbTable& nb = s_nb;
+    // this thread's draws of pass (sweep s, colour c) into its slots (col.pre only)
+    auto precompute = [&](int s, int c) {
+        const uint64_t prefix = hash_prefix(a.seed, t0 + (uint32_t)s);
+        for (int k = 0; k < col.rounds[c]; ++k) {
+            const int slot = (col.round0[c] + k) * kMcThreads + threadIdx.x;
+            const uint32_t g = s_ent[slot];
+            if (g == 0xFFFFFFFFu) continue;
+            const McDraws d = mc_draws<kMobility, kRandomNb>(a, prefix, g, kMobility ? s_mob[slot] : 0.f);
+            const int ps = k * kMcThreads + threadIdx.x;
+            s_pacc[ps] = d.acc;
+            s_pprop[ps] = d.prop_raw;
+            s_pflag[ps] = (uint8_t)((d.attempt ? 0x80 : 0) | d.var);
+        }
+    };
     unsigned long long my_att = 0, my_acc = 0, my_up = 0;
     bool ok = true;
     unsigned long long epoch = 0;  // grid barriers passed in this launch
+    if (col.pre && sweeps > 0) precompute(0, 0);
     for (int s = 0; s < sweeps && ok; ++s) {
         const uint64_t prefix = hash_prefix(a.seed, t0 + (uint32_t)s);
         for (int c = 0; c < col.colors && ok; ++c) {
@@ -380,34 +448,41 @@ __global__ __launch_bounds__(kMcThreads, 2) void mc_sweeps_kernel(McArgs a, McCo
                 if (col.cached) {
                     const int slot = (col.round0[c] + k) * kMcThreads + threadIdx.x;
                     g = s_ent[slot];
-                    if (kMobility) mob = s_mob[slot];
+                    if (kMobility && !col.pre) mob = s_mob[slot];
                 } else {
                     const uint64_t j = col.off[c] + me + (uint64_t)k * T;
                     g = j < col.off[c + 1] ? a.list[j] : 0xFFFFFFFFu;
                     if (kMobility && g != 0xFFFFFFFFu) mob = a.list_mob[j];
                 }
                 if (g == 0xFFFFFFFFu) continue;
-                const uint64_t h = hash_index(prefix, g + a.gidx_base);
-                if (kMobility) {
-                    const uint64_t r = hash_salt(h, kSaltMcMobility);
-                    if (__dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0) >= (double)mob) continue;
+                McDraws d;
+                if (col.pre) {
+                    const int ps = k * kMcThreads + threadIdx.x;
+                    const unsigned f = s_pflag[ps];
+                    d.attempt = (f & 0x80u) != 0;
+                    d.var = (int)(f & 0x7Fu);
+                    d.prop_raw = s_pprop[ps];
+                    d.acc = s_pacc[ps];
+                } else {
+                    d = mc_draws<kMobility, kRandomNb>(a, prefix, g, mob);
                 }
+                if (!d.attempt) continue;
                 ++my_att;
-                int var = 0;
-                if (kRandomNb) var = (int)fast_mod(hash_salt(h, kSaltNeighborhood), a.var_mod);
+                const int var = d.var;
                 int x, y, z;
                 decode(a, g, x, y, z);
                 const int32_t cur = a.spin[g];
-                int32_t prop = 1 + (int32_t)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
+                int32_t prop = d.prop_raw;
                 if (prop >= cur) ++prop;
                 int in_dom, same_a, same_b;
-                nb_counts(a, nb, var, x, y, z, g, cur, prop, in_dom, same_a, same_b);
+                mc_count_block(a, a.spin, g, x, y, z, col.mask[var], 0u, (uint32_t)cur, (uint32_t)prop, in_dom,
+                                     same_a, same_b);
                 const unsigned long long th = s_table[(in_dom - same_a) * kTableSide + (in_dom - same_b)];
                 bool accept;
                 if (th >> 63) {
                     accept = true;
                 } else {
-                    accept = th != 0 && (hash_salt(h, kSaltMcAccept) >> 11) < th;
+                    accept = th != 0 && (d.acc >> 11) < th;
                     my_up += accept ? 1u : 0u;
                 }
                 if (accept) {
@@ -415,7 +490,13 @@ __global__ __launch_bounds__(kMcThreads, 2) void mc_sweeps_kernel(McArgs a, McCo
                     ++my_acc;
                 }
             }
-            ok = mc_grid_barrier(ctrl, gridDim.x, ++epoch);
+            mc_barrier_arrive(ctrl);
+            if (col.pre) {  // the next pass's draws while the other blocks finish this one
+                const bool last_c = c + 1 == col.colors;
+                if (!last_c) precompute(s, c + 1);
+                else if (s + 1 < sweeps) precompute(s + 1, 0);
+            }
+            ok = mc_barrier_wait(ctrl, gridDim.x, ++epoch);
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -461,7 +542,7 @@ struct McDense {
     const float* mob;        // mobility of every cell (kMobility)
     int cnt[3][3];           // per axis and class: coordinates of the class
     FastDiv32 div[2][3];     // / cnt[0][c] and / cnt[1][c]
-    int delta[6][26];        // linear offsets of each variant's neighbours
+    uint32_t mask[6];        // per variant: bit (dx + 1) + 3 (dy + 1) + 9 (dz + 1) of each neighbour
 };
 
 // Coordinate i of class c on an axis of n cells split into `classes` classes (axisClass,
@@ -480,19 +561,17 @@ __global__ void mc_unpack8_kernel(const uint8_t* sp, int32_t* spin, uint64_t n) 
         spin[g] = (int32_t)sp[g] + 1;
 }
 
-template <bool kMobility, bool kRandomNb, bool kParity>
-__global__ __launch_bounds__(kMcThreads, 2) void mc_dense_sweeps_kernel(McArgs a, McDense d, int sweeps) {
+// kMoore3: the 26-cell Moore neighbourhood of a 3D space, whose interior cells read their 26
+// neighbours from nine row addresses and immediate offsets.
+template <bool kMobility, bool kRandomNb, bool kParity, bool kMoore3>
+__global__ __launch_bounds__(kMcThreads, 3) void mc_dense_sweeps_kernel(const __grid_constant__ McArgs a,
+                                                                        const __grid_constant__ McDense d, int sweeps) {
     __shared__ unsigned long long s_table[kTableSide * kTableSide];
     __shared__ unsigned long long s_red[3][kMcThreads / 32];
-    __shared__ NbTable s_nb;
-    __shared__ int s_delta[6][26];
     for (int i = threadIdx.x; i < kTableSide * kTableSide; i += kMcThreads) s_table[i] = a.table[i];
-    for (int i = threadIdx.x; i < 6 * 26; i += kMcThreads) s_delta[i / 26][i % 26] = d.delta[i / 26][i % 26];
-    stage_nb(a, s_nb);
     __syncthreads();
     McCtrl* ctrl = a.ctrl;
     const uint32_t t0 = ctrl->sweeps;
-    const NbTable& nb = s_nb;
     const uint8_t* sp = d.sp;
     const uint64_t T = (uint64_t)gridDim.x * kMcThreads;
     const uint64_t me = (uint64_t)blockIdx.x * kMcThreads + threadIdx.x;
@@ -540,32 +619,9 @@ __global__ __launch_bounds__(kMcThreads, 2) void mc_dense_sweeps_kernel(McArgs a
                 int prop = 1 + (int)fast_mod(hash_salt(h, kSaltMcOrient), a.qm1_mod);
                 if (prop >= cur) ++prop;
                 const uint32_t cb = (uint32_t)(cur - 1), pb = (uint32_t)(prop - 1);
-                const int cnt = nb.count[var];
-                const bool inner = (a.nx == 1 || (x >= 1 && x <= a.nx - 2)) && (a.ny == 1 || (y >= 1 && y <= a.ny - 2)) &&
-                                   (a.nz == 1 || (z >= 1 && z <= a.nz - 2));
-                int in_dom = 0, same_a = 0, same_b = 0;
-                if (inner) {
-                    in_dom = cnt;
-#pragma unroll
-                    for (int k = 0; k < 26; ++k) {
-                        if (k < cnt) {
-                            const uint32_t v = sp[(int64_t)g + s_delta[var][k]];
-                            same_a += v == cb;
-                            same_b += v == pb;
-                        }
-                    }
-                } else {
-                    for (int k = 0; k < cnt; ++k) {
-                        int sx = x + nb.off[var][k][0], sy = y + nb.off[var][k][1], sz = z + nb.off[var][k][2];
-                        if (!mc_wrap1_sel(sx, a.nx, a.per[0]) || !mc_wrap1_sel(sy, a.ny, a.per[1]) ||
-                            !mc_wrap1_sel(sz, a.nz, a.per[2]))
-                            continue;
-                        const uint32_t v = sp[(uint32_t)sx + (uint32_t)a.nx * ((uint32_t)sy + (uint32_t)a.ny * (uint32_t)sz)];
-                        ++in_dom;
-                        same_a += v == cb;
-                        same_b += v == pb;
-                    }
-                }
+                int in_dom, same_a, same_b;
+                mc_count_block(a, sp, g, x, y, z, kMoore3 ? 0x7FFFFFFu & ~(1u << 13) : d.mask[var], 0x100u, cb, pb,
+                                      in_dom, same_a, same_b);
                 const unsigned long long th = s_table[(in_dom - same_a) * kTableSide + (in_dom - same_b)];
                 bool accept;
                 if (th >> 63) {
@@ -579,7 +635,8 @@ __global__ __launch_bounds__(kMcThreads, 2) void mc_dense_sweeps_kernel(McArgs a
                     ++my_acc;
                 }
             }
-            ok = mc_grid_barrier(ctrl, gridDim.x, ++epoch);
+            mc_barrier_arrive(ctrl);
+            ok = mc_barrier_wait(ctrl, gridDim.x, ++epoch);
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -972,6 +1029,15 @@ void mc_free(vca_mc* h) {
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
+// A variant's neighbours as bits (dx + 1) + 3 (dy + 1) + 9 (dz + 1) of the 3 x 3 x 3 block.
+uint32_t nb_mask(const NbTable& nb, int v) {
+    uint32_t m = 0;
+    if (v < nb.variants)
+        for (int k = 0; k < nb.count[v]; ++k)
+            m |= 1u << ((nb.off[v][k][0] + 1) + 3 * (nb.off[v][k][1] + 1) + 9 * (nb.off[v][k][2] + 1));
+    return m;
+}
+
 using SweepsKernel = void (*)(McArgs, McColors, int);
 
 SweepsKernel sweeps_kernel_of(const vca_mc* h) {
@@ -1007,12 +1073,17 @@ vca_status sweeps_launch_shape(vca_mc* h, SweepsKernel kernel, McColors* col, in
     for (int per_sm = per_sm_max; per_sm >= 1; --per_sm) {
         const int g = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * per_sm));
         rounds_for((uint64_t)g * kMcThreads);
-        const size_t bytes = (size_t)col->total_rounds * kMcThreads * per_entry;
+        int most = 0;
+        for (int c = 0; c < h->colors; ++c) most = std::max(most, col->rounds[c]);
+        const bool pre = most <= kPreRounds;
+        const size_t bytes = (size_t)col->total_rounds * kMcThreads * per_entry +
+                             (pre ? (size_t)kPreRounds * kMcThreads * (8 + 4 + 1) : 0);
         if (bytes > kMcEntryCacheMax) continue;
         int fit = 0;
         VCA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kernel, kMcThreads, bytes));
         if ((uint64_t)fit * h->sms < (uint64_t)g) continue;
         col->cached = 1;
+        col->pre = pre;
         *grid = g;
         *smem = bytes;
         return VCA_OK;
@@ -1021,6 +1092,7 @@ vca_status sweeps_launch_shape(vca_mc* h, SweepsKernel kernel, McColors* col, in
     const int g = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)h->sms * per_sm_max));
     rounds_for((uint64_t)g * kMcThreads);
     col->cached = 0;
+    col->pre = 0;
     *grid = g;
     *smem = 0;
     return VCA_OK;
@@ -1031,9 +1103,11 @@ using DenseKernel = void (*)(McArgs, McDense, int);
 template <bool kParity>
 DenseKernel dense_kernel_of(const vca_mc* h) {
     const bool random_nb = h->nb_host.variants > 1;
+    const bool moore3 = !kParity && !random_nb && h->nb_host.count[0] == 26;
+    if (moore3) return h->mobility_on ? mc_dense_sweeps_kernel<true, false, false, true> : mc_dense_sweeps_kernel<false, false, false, true>;
     if (h->mobility_on)
-        return random_nb ? mc_dense_sweeps_kernel<true, true, kParity> : mc_dense_sweeps_kernel<true, false, kParity>;
-    return random_nb ? mc_dense_sweeps_kernel<false, true, kParity> : mc_dense_sweeps_kernel<false, false, kParity>;
+        return random_nb ? mc_dense_sweeps_kernel<true, true, kParity, false> : mc_dense_sweeps_kernel<true, false, kParity, false>;
+    return random_nb ? mc_dense_sweeps_kernel<false, true, kParity, false> : mc_dense_sweeps_kernel<false, false, kParity, false>;
 }
 
 // The whole-space sweeps apply when every cell is in the domain and an orientation fits a byte.
@@ -1066,10 +1140,7 @@ McDense dense_args(const vca_mc* h) {
     }
     for (int a = 0; a < 2; ++a)
         for (int c = 0; c < 3; ++c) d.div[a][c] = make_fastdiv32((uint32_t)std::max(1, d.cnt[a][c]));
-    const NbTable& nb = h->nb_host;
-    for (int v = 0; v < nb.variants && v < 6; ++v)
-        for (int k = 0; k < nb.count[v]; ++k)
-            d.delta[v][k] = nb.off[v][k][0] + dims[0] * (nb.off[v][k][1] + dims[1] * nb.off[v][k][2]);
+    for (int v = 0; v < 6; ++v) d.mask[v] = nb_mask(h->nb_host, v);
     return d;
 }
 
@@ -1398,12 +1469,18 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
     VCA_CUDA(cudaSetDevice(h->device));
     McArgs a = mc_args(h);
     VCA_CUDA(cudaMemsetAsync(&h->ctrl->sweep_accepted, 0, 8, h->stream));
+    // a cooperative sweep launch: its barrier count starts at zero
+    auto barrier_reset = [&](int) -> vca_status {
+        VCA_CUDA(cudaMemsetAsync(&h->ctrl->bar_arrived, 0, sizeof(unsigned long long), h->stream));
+        return VCA_OK;
+    };
     if (!h->profile_kernels) {
         // all sweeps in one cooperative launch (colour passes separated by grid barriers)
         McColors col;
         std::memset(&col, 0, sizeof(col));
         col.colors = h->colors;
         for (int c = 0; c <= h->colors; ++c) col.off[c] = h->color_off[c];
+        for (int v = 0; v < 6; ++v) col.mask[v] = nb_mask(h->nb_host, v);
         int grid = 1;
         size_t smem = 0;
         SweepsKernel kernel = sweeps_kernel_of(h);
@@ -1424,7 +1501,7 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
             int n = count;
             McDense dd = d;
             void* args[] = {&a, &dd, &n};
-            VCA_CUDA(cudaMemsetAsync(&h->ctrl->bar_arrived, 0, sizeof(unsigned long long), h->stream));
+            if (vca_status s = barrier_reset(dgrid)) return s;
             VCA_CUDA(cudaLaunchCooperativeKernel((const void*)dk, dgrid, kMcThreads, args, 0, h->stream));
             mc_unpack8_kernel<<<blocks, 256, 0, h->stream>>>(h->sp8, h->spin, h->n);
             VCA_CUDA(cudaGetLastError());
@@ -1432,7 +1509,7 @@ vca_status vca_mc_sweep(vca_mc* h, int count, uint64_t* accepted) {
         } else if (count > 0 && h->color_off.back() > 0) {
             int n = count;
             void* args[] = {&a, &col, &n};
-            VCA_CUDA(cudaMemsetAsync(&h->ctrl->bar_arrived, 0, sizeof(unsigned long long), h->stream));
+            if (vca_status s = barrier_reset(grid)) return s;
             VCA_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, grid, kMcThreads, args, smem, h->stream));
             h->launches += 1;
         } else if (count > 0) {
