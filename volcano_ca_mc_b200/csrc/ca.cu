@@ -297,6 +297,7 @@ __device__ __forceinline__ void drop_body(const CaKernelArgs& k, int force_full,
     if (!force_full && bid == 0 && threadIdx.x == 0) {
         ctrl->chg_count[nxt] = 0;   // filled by this step's rules
         ctrl->list_count[nxt] = 0;  // tiles of the next step, scheduled by this step's rules
+        ctrl->tile_next = 0;        // tiles handed out at run time by this step's rules (DENSE)
     }
     if (k.classic) return;
     const CaGeom& g = k.g;
@@ -818,41 +819,53 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         bulk_commit();
     };
 
-    // control pipeline: tile ids of the next two iterations, the mark of the next
+    // control pipeline: the indices of this and the next three iterations (i0 .. i3), the tile ids
+    // of the next two, the mark of the next.  Iteration m of a block takes index bid + m nblk; under
+    // DENSE, where a tile costs a plain copy or the whole rules pass, indices from the fifth on are
+    // handed out at run time from a per-step counter instead, so that blocks that drew cheap tiles
+    // take more of them.  Each block's indices increase, so it stops at the first one past the end;
+    // every index below it is taken by exactly one block.
     const uint64_t G = nblk;
-    uint64_t i = bid;
+    const uint64_t first_dynamic = 4 * G;
+    __shared__ uint64_t s_next[2];  // the index of iteration m, at [m & 1]
+    auto index_of = [&](uint64_t m) -> uint64_t {
+        if (!k.dense) return bid + m * G;
+        return first_dynamic < count ? first_dynamic + atomicAdd(&ctrl->tile_next, 1u) : count;
+    };
+    uint64_t i0 = bid, i1 = bid + G, i2 = bid + 2 * G, i3 = bid + 3 * G;
+    if (tid == 0) s_next[0] = index_of(4);
     uint32_t tile_a = 0, mark_a = 0, vent_a = 0;  // iteration it
     uint32_t tile_b = 0, mark_b = 0, vent_b = 0;  // it + 1
     uint32_t tile_c = 0;                          // it + 2
-    if (i < count) {
-        tile_a = tile_at(i);
+    if (i0 < count) {
+        tile_a = tile_at(i0);
         mark_a = k.tile_mark[cur][tile_a];
         vent_a = k.tile_flags[tile_a];
-        if (i + G < count) tile_b = tile_at(i + G);
-        if (i + 2 * G < count) tile_c = tile_at(i + 2 * G);
+        if (i1 < count) tile_b = tile_at(i1);
+        if (i2 < count) tile_c = tile_at(i2);
         stage(0, tile_a, takes_rules(tile_a, mark_a));
     }
     cp_async_commit();
-    if (i + G < count) {
+    if (i1 < count) {
         mark_b = k.tile_mark[cur][tile_b];
         vent_b = k.tile_flags[tile_b];
     }
 
-    for (int it = 0; i < count; i += G, ++it) {
+    for (int it = 0; i0 < count; ++it) {
         const int si = it & 1;
         RulesSlot& sl = slots[si];
         const uint32_t tile = tile_a;
         const bool rules = takes_rules(tile_a, mark_a);
         const bool tile_vent = (vent_a & 2u) != 0;
         // next tile into the other slot, then the control loads of the tiles after it
-        if (i + G < count) stage(si ^ 1, tile_b, takes_rules(tile_b, mark_b));
+        if (i1 < count) stage(si ^ 1, tile_b, takes_rules(tile_b, mark_b));
         cp_async_commit();
         uint32_t mark_c = 0, vent_c = 0, tile_d = 0;
-        if (i + 2 * G < count) {
+        if (i2 < count) {
             mark_c = k.tile_mark[cur][tile_c];
             vent_c = k.tile_flags[tile_c];
         }
-        if (i + 3 * G < count) tile_d = tile_at(i + 3 * G);
+        if (i3 < count) tile_d = tile_at(i3);
 
         int x0, y0, z0;
         tile_origin(g, tile, x0, y0, z0);
@@ -864,11 +877,15 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
             if (tid == 0) {
                 atomicOr(&ctrl->error, 1);
                 // the copies of the next slot, if any were issued, before the block gives up
-                if (i + G < count) mbar_wait(&s_bar[si ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
+                if (i1 < count) mbar_wait(&s_bar[si ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
             }
             failed = true;
             break;
         }
+        // the index of iteration it + 4 (set during iteration it - 1, or before the loop), and that
+        // of iteration it + 5 into the other word, read after the next barrier
+        const uint64_t i4 = s_next[it & 1];
+        if (tid == 0) s_next[(it + 1) & 1] = index_of((uint64_t)it + 5);
         if (!rules) {
             // No LAVA within one tile: nothing can change, the boxes go to the next buffer as they are.
             if (tid == 0) {
@@ -1131,6 +1148,10 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         mark_b = mark_c;
         vent_b = vent_c;
         tile_c = tile_d;
+        i0 = i1;
+        i1 = i2;
+        i2 = i3;
+        i3 = i4;
     }
     cp_async_wait_all();
     if (tid == 0) {

@@ -45,6 +45,7 @@ struct CaCtrl {
     int32_t random_nb;
     int32_t classic;
     int32_t error;            // bit 0: a bounded device wait ran out (the run stops, VCA_ERR_TIMEOUT)
+    uint32_t tile_next;       // rules pass (DENSE): tiles handed out at run time in the running step
 };
 
 // Geometry of the pitched device planes.  Each (y, z) row holds P >= nx cells, P a multiple of 64,
