@@ -684,7 +684,7 @@ __device__ __forceinline__ uint32_t win_right(const uint8_t* p) {
     return __funnelshift_r(*reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 4), 8);
 }
 
-template <class S>
+template <class S, bool kDyn>
 __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKernelArgs& k, uint32_t bid, uint32_t nblk) {
     using RulesSlot = vca::RulesSlot<S>;
     // Declared with the 16-byte alignment that dynamic shared memory is guaranteed to have, so that
@@ -819,21 +819,27 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         bulk_commit();
     };
 
-    // control pipeline: the indices of this and the next three iterations (i0 .. i3), the tile ids
-    // of the next two, the mark of the next.  Iteration m of a block takes index bid + m nblk; under
-    // DENSE, where a tile costs a plain copy or the whole rules pass, indices from the fifth on are
-    // handed out at run time from a per-step counter instead, so that blocks that drew cheap tiles
-    // take more of them.  Each block's indices increase, so it stops at the first one past the end;
-    // every index below it is taken by exactly one block.
+    // control pipeline: the indices of this iteration and the next three, the tile ids of the next
+    // two, the mark of the next.  Iteration m of a block takes index bid + m nblk.  With kDyn (DENSE
+    // over many tiles per block, where a tile costs a plain copy or the whole rules pass) the indices
+    // from the fifth on are handed out at run time from a per-step counter instead, so that blocks
+    // that drew cheap tiles take more of them; each block's indices still increase, so it stops at
+    // the first one past the end, and every index below that is taken by exactly one block.
     const uint64_t G = nblk;
-    const uint64_t first_dynamic = 4 * G;
-    __shared__ uint64_t s_next[2];  // the index of iteration m, at [m & 1]
-    auto index_of = [&](uint64_t m) -> uint64_t {
-        if (!k.dense) return bid + m * G;
-        return first_dynamic < count ? first_dynamic + atomicAdd(&ctrl->tile_next, 1u) : count;
+    uint64_t i0 = bid, r1 = 0, r2 = 0, r3 = 0;  // kDyn: the indices of iterations it + 1 .. it + 3
+    __shared__ uint64_t s_next[2];               // kDyn: the index of iteration m, at [m & 1]
+    auto hand_out = [&]() -> uint64_t {
+        return 4 * G < count ? 4 * G + atomicAdd(&ctrl->tile_next, 1u) : count;
     };
-    uint64_t i0 = bid, i1 = bid + G, i2 = bid + 2 * G, i3 = bid + 3 * G;
-    if (tid == 0) s_next[0] = index_of(4);
+    if constexpr (kDyn) {
+        r1 = bid + G;
+        r2 = bid + 2 * G;
+        r3 = bid + 3 * G;
+        if (tid == 0) s_next[0] = hand_out();  // iteration 4
+    }
+    auto at1 = [&]() -> uint64_t { if constexpr (kDyn) return r1; else return i0 + G; };
+    auto at2 = [&]() -> uint64_t { if constexpr (kDyn) return r2; else return i0 + 2 * G; };
+    auto at3 = [&]() -> uint64_t { if constexpr (kDyn) return r3; else return i0 + 3 * G; };
     uint32_t tile_a = 0, mark_a = 0, vent_a = 0;  // iteration it
     uint32_t tile_b = 0, mark_b = 0, vent_b = 0;  // it + 1
     uint32_t tile_c = 0;                          // it + 2
@@ -841,12 +847,12 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         tile_a = tile_at(i0);
         mark_a = k.tile_mark[cur][tile_a];
         vent_a = k.tile_flags[tile_a];
-        if (i1 < count) tile_b = tile_at(i1);
-        if (i2 < count) tile_c = tile_at(i2);
+        if (at1() < count) tile_b = tile_at(at1());
+        if (at2() < count) tile_c = tile_at(at2());
         stage(0, tile_a, takes_rules(tile_a, mark_a));
     }
     cp_async_commit();
-    if (i1 < count) {
+    if (at1() < count) {
         mark_b = k.tile_mark[cur][tile_b];
         vent_b = k.tile_flags[tile_b];
     }
@@ -858,14 +864,14 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         const bool rules = takes_rules(tile_a, mark_a);
         const bool tile_vent = (vent_a & 2u) != 0;
         // next tile into the other slot, then the control loads of the tiles after it
-        if (i1 < count) stage(si ^ 1, tile_b, takes_rules(tile_b, mark_b));
+        if (at1() < count) stage(si ^ 1, tile_b, takes_rules(tile_b, mark_b));
         cp_async_commit();
         uint32_t mark_c = 0, vent_c = 0, tile_d = 0;
-        if (i2 < count) {
+        if (at2() < count) {
             mark_c = k.tile_mark[cur][tile_c];
             vent_c = k.tile_flags[tile_c];
         }
-        if (i3 < count) tile_d = tile_at(i3);
+        if (at3() < count) tile_d = tile_at(at3());
 
         int x0, y0, z0;
         tile_origin(g, tile, x0, y0, z0);
@@ -877,15 +883,18 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
             if (tid == 0) {
                 atomicOr(&ctrl->error, 1);
                 // the copies of the next slot, if any were issued, before the block gives up
-                if (i1 < count) mbar_wait(&s_bar[si ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
+                if (at1() < count) mbar_wait(&s_bar[si ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
             }
             failed = true;
             break;
         }
-        // the index of iteration it + 4 (set during iteration it - 1, or before the loop), and that
-        // of iteration it + 5 into the other word, read after the next barrier
-        const uint64_t i4 = s_next[it & 1];
-        if (tid == 0) s_next[(it + 1) & 1] = index_of((uint64_t)it + 5);
+        // kDyn: the index of iteration it + 4 (handed out during iteration it - 1, or before the
+        // loop), and the hand-out of iteration it + 5 into the other word, read after the next barrier
+        uint64_t i4 = 0;
+        if constexpr (kDyn) {
+            i4 = s_next[it & 1];
+            if (tid == 0) s_next[(it + 1) & 1] = hand_out();
+        }
         if (!rules) {
             // No LAVA within one tile: nothing can change, the boxes go to the next buffer as they are.
             if (tid == 0) {
@@ -1148,10 +1157,14 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         mark_b = mark_c;
         vent_b = vent_c;
         tile_c = tile_d;
-        i0 = i1;
-        i1 = i2;
-        i2 = i3;
-        i3 = i4;
+        if constexpr (kDyn) {
+            i0 = r1;
+            r1 = r2;
+            r2 = r3;
+            r3 = i4;
+        } else {
+            i0 += G;
+        }
     }
     cp_async_wait_all();
     if (tid == 0) {
@@ -1184,7 +1197,13 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
 template <class S>
 __global__ __launch_bounds__(kThreads, 4) void ca_rules_kernel(const __grid_constant__ CaTensorMaps tm,
                                                                const __grid_constant__ CaKernelArgs k) {
-    rules_body<S>(tm, k, blockIdx.x, gridDim.x);
+    rules_body<S, false>(tm, k, blockIdx.x, gridDim.x);
+}
+// DENSE over many tiles per block: tiles handed out at run time (rules_body, kDyn)
+template <class S>
+__global__ __launch_bounds__(kThreads, 4) void ca_rules_dyn_kernel(const __grid_constant__ CaTensorMaps tm,
+                                                                   const __grid_constant__ CaKernelArgs k) {
+    rules_body<S, true>(tm, k, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1452,7 +1471,7 @@ struct CaBatchView {
     const int2* cand_map;      // per block of the candidate launch
     const int* rules_n;        // per slot: its blocks in the drop / rules launches (0: free slot)
     const int* cand_n;         // per slot: its blocks in the candidate launch
-    int4* status;              // per slot after a graph: (stop, error, steps, member) or (-1, 0, 0, 0)
+    int4* status;              // per slot after a graph: (stop, error, steps, next tiles) or (-1, 0, 0, 0)
     int slots;
 };
 
@@ -1485,7 +1504,7 @@ __global__ __launch_bounds__(kThreads, 4) void ca_rules_batch_kernel(const __gri
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(base + off) : "memory");
     }
     load_args(s_k, b.args[m.x]);
-    rules_body<ShapeA>(tm, s_k, (uint32_t)m.y, (uint32_t)b.rules_n[m.x]);
+    rules_body<ShapeA, false>(tm, s_k, (uint32_t)m.y, (uint32_t)b.rules_n[m.x]);
 }
 
 __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_batch_kernel(const __grid_constant__ CaBatchView b) {
@@ -1496,13 +1515,14 @@ __global__ __launch_bounds__(kCandThreads, 4) void ca_cand_batch_kernel(const __
     cand_body(s_k, (uint32_t)m.y, (uint32_t)b.cand_n[m.x]);
 }
 
-// Stop state of every member after a graph of steps, gathered for one copy to the host.
+// Stop state of every member after a graph of steps, and the tiles its next step will visit,
+// gathered for one copy to the host.
 __global__ void ca_batch_status_kernel(const __grid_constant__ CaBatchView b) {
     for (int i = threadIdx.x; i < b.slots; i += blockDim.x) {
         int4 st = make_int4(-1, 0, 0, 0);
         if (b.rules_n[i] > 0) {
             const CaCtrl* c = b.args[i].ctrl;
-            st = make_int4(c->stop, c->error, (int)c->steps, i);
+            st = make_int4(c->stop, c->error, (int)c->steps, (int)c->list_count[c->steps & 1u]);
         }
         b.status[i] = st;
     }
@@ -1680,19 +1700,38 @@ vca_status init_state(vca_ca* h, int steps_done) {
 }
 
 // The rules pass of the handle's tile-shape family.
+// Tiles handed out at run time pay where a block has many tiles of uneven cost: DENSE with at
+// least 64 tiles per block (measured: c3 DENSE -20 %; with 14 tiles per block, c2, +12 %).
+constexpr uint64_t kDynTilesPerBlock = 64;
+
+template <class S>
+void launch_rules_shape(const vca_ca* h, const CaKernelArgs& k) {
+    const bool dyn = k.dense && h->ntiles >= kDynTilesPerBlock * (uint64_t)h->grid_blocks;
+    if (dyn)
+        ca_rules_dyn_kernel<S><<<h->grid_blocks, kThreads, rules_dyn_smem<S>(), h->stream>>>(h->tmaps, k);
+    else
+        ca_rules_kernel<S><<<h->grid_blocks, kThreads, rules_dyn_smem<S>(), h->stream>>>(h->tmaps, k);
+}
 void launch_rules(const vca_ca* h, const CaKernelArgs& k) {
     switch (h->geom.shape) {
-        case 0: ca_rules_kernel<ShapeA><<<h->grid_blocks, kThreads, rules_dyn_smem<ShapeA>(), h->stream>>>(h->tmaps, k); break;
-        case 1: ca_rules_kernel<ShapeB><<<h->grid_blocks, kThreads, rules_dyn_smem<ShapeB>(), h->stream>>>(h->tmaps, k); break;
-        default: ca_rules_kernel<ShapeC><<<h->grid_blocks, kThreads, rules_dyn_smem<ShapeC>(), h->stream>>>(h->tmaps, k); break;
+        case 0: launch_rules_shape<ShapeA>(h, k); break;
+        case 1: launch_rules_shape<ShapeB>(h, k); break;
+        default: launch_rules_shape<ShapeC>(h, k); break;
     }
 }
 
+// Resident rules blocks per SM of a shape family: the smaller of the two forms' (they differ by
+// 16 bytes of static shared memory).
 template <class S>
 cudaError_t rules_occupancy(int* per_sm) {
+    int a = 0, b = 0;
     cudaError_t e = cudaFuncSetAttribute(ca_rules_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rules_dyn_smem<S>());
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, ca_rules_kernel<S>, kThreads, rules_dyn_smem<S>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ca_rules_dyn_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rules_dyn_smem<S>());
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, ca_rules_kernel<S>, kThreads, rules_dyn_smem<S>());
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, ca_rules_dyn_kernel<S>, kThreads, rules_dyn_smem<S>());
+    *per_sm = std::min(a, b);
+    return e;
 }
 
 constexpr int kGraphSteps = 16;  // steps captured in one CUDA graph
@@ -2695,7 +2734,8 @@ struct vca_ca_batch {
     int* d_rules_n = nullptr;
     int* d_cand_n = nullptr;
     int4* d_status = nullptr;
-    int4* h_status = nullptr;     // pinned, two ring slots of cap entries
+    int4* h_status = nullptr;     // pinned, two ring slots of cap entries: (stop, error, steps, next tiles)
+    std::vector<uint64_t> weight; // per slot: tiles of the member's next step (its share of the blocks)
     cudaEvent_t status_ev[2] = {nullptr, nullptr};
     cudaEvent_t sync_ev = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -2770,7 +2810,7 @@ vca_status batch_upload(vca_ca_batch* b) {
         tm[(size_t)i] = h->tmaps;
         args[(size_t)i] = make_args(h, true);
         members.push_back(i);
-        w.push_back(std::max<uint64_t>(1, h->ntiles));
+        w.push_back(std::max<uint64_t>(1, b->weight[(size_t)i]));
     }
     std::vector<int> nr, nc;
     split_blocks(w, b->rules_grid, nr);
@@ -2823,6 +2863,14 @@ vca_status batch_collect(vca_ca_batch* b, int r) {
         if (st[i].x != VCA_STOP_RUNNING || st[i].y != 0) {
             if (vca_status s = batch_detach(b, h, &st[i])) return s;
             b->done.push_back(h);
+            continue;
+        }
+        // the blocks follow the work: re-split when a member's visited tiles moved by more than 1/8
+        const uint64_t now = std::max<uint64_t>(1, (uint64_t)std::max(0, st[i].w));
+        uint64_t& was = b->weight[(size_t)i];
+        if (now > was + was / 8 || now + now / 8 < was) {
+            was = now;
+            b->dirty = true;
         }
     }
     return VCA_OK;
@@ -2904,6 +2952,7 @@ vca_status vca_ca_batch_create(int device, int max_members, vca_ca_batch** out) 
     b->cand_grid = prop.multiProcessorCount * std::max(1, cand_per_sm);
     b->cap = std::min(max_members, std::min(b->rules_grid, b->cand_grid));
     b->slots.assign((size_t)b->cap, nullptr);
+    b->weight.assign((size_t)b->cap, 1);
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaStreamCreate"));
 #define BALLOC(ptr, bytes)                                                    \
@@ -2969,6 +3018,7 @@ vca_status vca_ca_batch_add(vca_ca_batch* b, vca_ca* h) {
     VCA_CUDA(cudaEventRecord(b->sync_ev, h->stream));
     VCA_CUDA(cudaStreamWaitEvent(b->stream, b->sync_ev, 0));
     b->slots[(size_t)slot] = h;
+    b->weight[(size_t)slot] = std::max<uint64_t>(1, h->ntiles);  // until its first status
     h->batch = b;
     h->batch_slot = slot;
     b->dirty = true;
