@@ -342,12 +342,16 @@ def roofline(p, w, schedule, peak, peak_kind):
     cells = p["tiles"] * p["cells_per_tile"] / max(1, p["rules_n"])
     bytes_per_launch = BYTES_PER_CELL_UPDATE * cells
     ach = bytes_per_launch / (p["rules_ms"] * 1e-3) / 1e9 if p["rules_ms"] > 0 else 0.0
+    # DENSE over at least 64 tiles per rules block (4 per SM) runs the run-time hand-out form
+    import torch
+    blocks = 4 * torch.cuda.get_device_properties(0).multi_processor_count
+    kernel = "ca_rules_dyn_kernel" if schedule == "dense" and p["tiles_total"] >= 64 * blocks else "ca_rules_kernel"
     traffic, src = None, None
-    t = ncu_traffic_per_cell("ca_rules_kernel", "c3q" if w.name == "c3" else w.name, schedule)
+    t = ncu_traffic_per_cell(kernel, "c3q" if w.name == "c3" else w.name, schedule)
     if t is not None:
         traffic, src = int(round(t[0] * cells)), t[1]
     return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
-            "traffic": traffic, "kernel": "ca_rules_kernel", "schedule": schedule,
+            "traffic": traffic, "kernel": kernel, "schedule": schedule,
             "launch_ms": round(p["rules_ms"], 5), "bytes_per_launch": int(bytes_per_launch), "launches": p["rules_n"],
             "peak_kind": peak_kind,
             "traffic_ratio": round(traffic / bytes_per_launch, 3) if traffic else None,
@@ -421,13 +425,19 @@ def job_mixes(args, device):
     keys = ("slots", "jobs", "makespan_s", "jobs_per_s", "cell_updates_per_s", "p50_s", "p99_s", "mean_concurrency")
     pick = lambda r: {k: (round(r[k], 4) if isinstance(r[k], float) else r[k]) for k in keys}
     out = {}
+    # a whole mix takes one to three seconds and varies by up to a third from run to run (host
+    # threads of the server against the GPU): each mode runs twice, the faster run is reported
+    def best(**kw):
+        runs = [serve.run(device=device, **kw) for _ in range(2)]
+        return max(runs, key=lambda r: r["jobs_per_s"])
+
     if not args.no_batched:
         jobs = serve.make_mix(96, 2026)
-        many = serve.run(jobs, slots=args.slots, batched=True, device=device)
-        one = serve.run(jobs, slots=1, batched=False, device=device)
-        streams = serve.run(jobs, slots=args.slots, batched=False, device=device)
+        many = best(jobs=jobs, slots=args.slots, batched=True)
+        one = best(jobs=jobs, slots=1, batched=False)
+        streams = best(jobs=jobs, slots=args.slots, batched=False)
         out["batched"] = {"mix": "96 jobs, master seed 2026: 2D sides 128-2048, 3D sides 64-256 (z = side/2), "
-                                 "200-600 CA steps, 20-100 MCS, sent at once",
+                                 "200-600 CA steps, 20-100 MCS, sent at once; each mode the faster of two runs",
                           "cells": sum(j.cells for j in jobs), **pick(many), "server": many["server"],
                           "one_at_a_time": pick(one), "independent_streams": pick(streams),
                           "mismatches": serve.compare(many, one) + serve.compare(streams, one)}
