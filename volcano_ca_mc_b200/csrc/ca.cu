@@ -1009,17 +1009,20 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                     const uint32_t dc = win_mid(reinterpret_cast<const uint8_t*>(sl.drop) +
                                                 ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq);
                     const uint32_t lands = __vcmpges4(dc, 0u), flat = __vcmpeq4(dc, 0u);
+                    // the same-level sources count only where the cell lands, the ones above only where
+                    // it is flat: a thread whose cells do neither (AIR over LAVA) skips those windows
                     uint32_t level = 0, above = 0, fall = 0;
                     for (int dy = -hy_on; dy <= hy_on; ++dy) {
                         const uint8_t* rp = sl.type + (hr + dy) * kSmemRowBytes + kRowOff + 4 * xq;
-                        level |= __vcmpeq4(win_left(rp), 0x02020202u) | __vcmpeq4(win_mid(rp), 0x02020202u) |
-                                 __vcmpeq4(win_right(rp), 0x02020202u);
+                        if (lands)
+                            level |= __vcmpeq4(win_left(rp), 0x02020202u) | __vcmpeq4(win_mid(rp), 0x02020202u) |
+                                     __vcmpeq4(win_right(rp), 0x02020202u);
                         if (hz_on) {
                             const uint8_t* ap = rp + HY * kSmemRowBytes;
-                            const uint32_t mid = __vcmpeq4(win_mid(ap), 0x02020202u);
-                            above |= __vcmpeq4(win_left(ap), 0x02020202u) | __vcmpeq4(win_right(ap), 0x02020202u) |
-                                     (dy != 0 ? mid : 0u);
-                            if (dy == 0) fall = mid;
+                            if (dy == 0) fall = __vcmpeq4(win_mid(ap), 0x02020202u);
+                            if (flat)
+                                above |= __vcmpeq4(win_left(ap), 0x02020202u) | __vcmpeq4(win_right(ap), 0x02020202u) |
+                                         (dy != 0 ? __vcmpeq4(win_mid(ap), 0x02020202u) : 0u);
                         }
                     }
                     near = (level & lands) | (above & flat) | fall;
@@ -1062,8 +1065,9 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                 uint32_t acc = 0;
                 const uint8_t* dropc =
                     reinterpret_cast<const uint8_t*>(sl.drop) + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
+                // without support no side cell matters: D(n) is -1 for every unsupported LAVA cell
 #pragma unroll
-                for (int sy = -1; sy <= 1; ++sy) {
+                for (int sy = -1; sy <= 1 && sup; ++sy) {
                     const unsigned bits = (k.side_mask >> (3 * (sy + 1))) & 7u;
                     if (!bits) continue;
                     const uint8_t* tp = rowp + sy * kSmemRowBytes;
