@@ -986,9 +986,6 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
             uint32_t w = valid ? win_mid(rowp) : 0xFFFFFFFFu;
             if (x + 4 > g.nx) w |= 0xFFFFFFFFu << (8 * max(0, g.nx - x));  // padding cells stay VOID
             const int cell = row * kTileX + 4 * xq;
-            int4 f4 = *reinterpret_cast<const int4*>(&sl.flow[cell]);
-            float4 t4 = *reinterpret_cast<const float4*>(&sl.temp[cell]);
-            uint2 s2 = *reinterpret_cast<const uint2*>(&sl.solid[cell]);
 
             bool any_lava = false, any_changed = false;
             unsigned nbas = 0, ncand = 0;
@@ -1083,6 +1080,10 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                     my_active += own * (__popc(lava_m) >> 3);
                     any_lava = true;
                 } else {
+                    // the state of the thread's four cells, read only where one of them is LAVA
+                    const int4 f4 = *reinterpret_cast<const int4*>(&sl.flow[cell]);
+                    const float4 t4 = *reinterpret_cast<const float4*>(&sl.temp[cell]);
+                    const uint2 s2 = *reinterpret_cast<const uint2*>(&sl.solid[cell]);
                     float te[4] = {t4.x, t4.y, t4.z, t4.w};
                     const int32_t fl[4] = {f4.x, f4.y, f4.z, f4.w};
                     uint32_t so[2] = {s2.x, s2.y};
@@ -1123,10 +1124,12 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
 
             // candidates: block-wide positions in the shared buffer
             unsigned incl = ncand;
+            if (__any_sync(0xFFFFFFFFu, ncand != 0)) {  // most warps of a tile list no candidate
 #pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const unsigned u = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-                if (lane >= off) incl += u;
+                for (int off = 1; off < 32; off <<= 1) {
+                    const unsigned u = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                    if (lane >= off) incl += u;
+                }
             }
             if (lane == 31) s_wtot[warp] = incl;
             unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
