@@ -1063,8 +1063,10 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                 const uint8_t* dropc =
                     reinterpret_cast<const uint8_t*>(sl.drop) + ((ly + hy_on) + HY * lz) * kSmemRowBytes + kRowOff + 4 * xq;
                 // without support no side cell matters: D(n) is -1 for every unsupported LAVA cell
+                // (and D(n) of the thread's other cells is never read)
+                const bool scan = (sup & lava_m) != 0;
 #pragma unroll
-                for (int sy = -1; sy <= 1 && sup; ++sy) {
+                for (int sy = -1; sy <= 1 && scan; ++sy) {
                     const unsigned bits = (k.side_mask >> (3 * (sy + 1))) & 7u;
                     if (!bits) continue;
                     const uint8_t* tp = rowp + sy * kSmemRowBytes;
