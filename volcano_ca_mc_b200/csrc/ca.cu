@@ -744,9 +744,14 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
 
     auto flush_schedule = [&]() {
         __syncthreads();
+        // lane (dx, dy, dz) of a tile with LAVA schedules that neighbour when the LAVA touches the
+        // faces towards it; a tile that changed schedules itself
+        const int ddx = lane % 3 - 1, ddy = (lane / 3) % 3 - 1, ddz = lane / 9 - 1;
         for (int e = warp; e < nsched; e += kThreads / 32) {
             const unsigned f = s_sched_flag[e];
-            schedule_around(k, s_sched_tile[e], t, nxt, lane, (f & 1u) || ((f & 2u) && lane == 13), (f & 1u) != 0);
+            const bool touch = (ddx == 0 || ((f >> (ddx < 0 ? 2 : 3)) & 1u)) && (ddy == 0 || ((f >> (ddy < 0 ? 4 : 5)) & 1u)) &&
+                               (ddz == 0 || ((f >> (ddz < 0 ? 6 : 7)) & 1u));
+            schedule_around(k, s_sched_tile[e], t, nxt, lane, ((f & 1u) && touch) || ((f & 2u) && lane == 13), (f & 1u) != 0);
         }
         __syncthreads();
         nsched = 0;
@@ -988,6 +993,7 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
             const int cell = row * kTileX + 4 * xq;
 
             bool any_lava = false, any_changed = false;
+            uint32_t surv = 0;  // bytes of the thread's cells that are LAVA after the step
             unsigned nbas = 0, ncand = 0;
             uint32_t bas[4], cand[4];
             const uint32_t g0 = (uint32_t)(x + g.nx * (y + g.ny * z));
@@ -1081,6 +1087,7 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                 if (k.classic) {
                     my_active += own * (__popc(lava_m) >> 3);
                     any_lava = true;
+                    surv = lava_m;
                 } else {
                     // the state of the thread's four cells, read only where one of them is LAVA
                     const int4 f4 = *reinterpret_cast<const int4*>(&sl.flow[cell]);
@@ -1110,6 +1117,7 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                         } else {
                             my_active += own;
                             any_lava = true;
+                            surv |= 0xFFu << (8 * j);
                             if (nt != before) {
                                 my_changed += own;
                                 any_changed = true;
@@ -1134,7 +1142,20 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                 }
             }
             if (lane == 31) s_wtot[warp] = incl;
-            unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u);
+            // the faces of the tile that LAVA after the step touches (bits 2-7: -x, +x, -y, +y, -z,
+            // +z): a neighbouring tile can change in the next step only if LAVA lies within one cell
+            // of it, so the schedule visits only the neighbours across touched faces
+            unsigned faces = 0;
+            if (surv && valid) {
+                const int xlast = min(kTileX, g.nx - x0) - 1, jl = xlast - 4 * xq;
+                if (xq == 0 && (surv & 0xFFu)) faces |= 1u << 2;
+                if (jl >= 0 && jl < 4 && ((surv >> (8 * jl)) & 0xFFu)) faces |= 1u << 3;
+                if (ly == 0) faces |= 1u << 4;
+                if (ly == min(g.TY, g.ny - y0) - 1) faces |= 1u << 5;
+                if (lz == 0) faces |= 1u << 6;
+                if (lz == min(g.TZ, g.nz - z0) - 1) faces |= 1u << 7;
+            }
+            unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u) | faces;
             bits = __reduce_or_sync(0xFFFFFFFFu, bits);
             if (lane == 0 && bits) atomicOr(&s_flags[rit & 1], bits);
             fence_proxy_async();  // the slot's results are read by the TMA stores below
