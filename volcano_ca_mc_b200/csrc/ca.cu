@@ -482,6 +482,27 @@ __device__ __forceinline__ bool air_gains_lava(const CaKernelArgs& k, const uint
     return gained;
 }
 
+// Whether a tile whose LAVA touches the faces `f` (bits 2-7: -x, +x, -y, +y, -z, +z) can reach its
+// neighbour (dx, dy, dz) = lane's offset in the next step: LAVA lies within one cell of it only when it
+// touches the faces towards it.
+__device__ __forceinline__ bool faces_reach(unsigned f, int lane) {
+    const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+    return (dx == 0 || ((f >> (dx < 0 ? 2 : 3)) & 1u)) && (dy == 0 || ((f >> (dy < 0 ? 4 : 5)) & 1u)) &&
+           (dz == 0 || ((f >> (dz < 0 ? 6 : 7)) & 1u));
+}
+
+// The face bits of a cell (x, y, z) of the tile with origin (x0, y0, z0): the faces it lies on.
+__device__ __forceinline__ unsigned cell_faces(const CaGeom& g, int x, int y, int z, int x0, int y0, int z0) {
+    unsigned f = 0;
+    if (x == x0) f |= 1u << 2;
+    if (x == min(x0 + kTileX, g.nx) - 1) f |= 1u << 3;
+    if (y == y0) f |= 1u << 4;
+    if (y == min(y0 + g.TY, g.ny) - 1) f |= 1u << 5;
+    if (z == z0) f |= 1u << 6;
+    if (z == min(z0 + g.TZ, g.nz) - 1) f |= 1u << 7;
+    return f;
+}
+
 // Schedule the tiles within one tile of `tile` for step t + 1; lanes 0..26 of a warp each try one
 // target, `want` says which lanes take part.  The mark of a tile scheduled for step s is
 // 2 (s + 1) plus a lava bit: the bit says that LAVA lies within one tile, so the tile's cells may
@@ -746,12 +767,10 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         __syncthreads();
         // lane (dx, dy, dz) of a tile with LAVA schedules that neighbour when the LAVA touches the
         // faces towards it; a tile that changed schedules itself
-        const int ddx = lane % 3 - 1, ddy = (lane / 3) % 3 - 1, ddz = lane / 9 - 1;
         for (int e = warp; e < nsched; e += kThreads / 32) {
             const unsigned f = s_sched_flag[e];
-            const bool touch = (ddx == 0 || ((f >> (ddx < 0 ? 2 : 3)) & 1u)) && (ddy == 0 || ((f >> (ddy < 0 ? 4 : 5)) & 1u)) &&
-                               (ddz == 0 || ((f >> (ddz < 0 ? 6 : 7)) & 1u));
-            schedule_around(k, s_sched_tile[e], t, nxt, lane, ((f & 1u) && touch) || ((f & 2u) && lane == 13), (f & 1u) != 0);
+            schedule_around(k, s_sched_tile[e], t, nxt, lane, ((f & 1u) && faces_reach(f, lane)) || ((f & 2u) && lane == 13),
+                            (f & 1u) != 0);
         }
         __syncthreads();
         nsched = 0;
@@ -1269,6 +1288,7 @@ __device__ __forceinline__ void cand_body(const CaKernelArgs& k, uint32_t bid, u
         const uint64_t j = base + threadIdx.x;
         bool gained = false;
         uint32_t gi = 0, tile = 0;
+        unsigned faces = 0;  // of the gained cell in its tile
         if (j < n) {
             gi = k.cand_list[j];
             const uint32_t r = gi / (uint32_t)g.nx;
@@ -1286,19 +1306,23 @@ __device__ __forceinline__ void cand_body(const CaKernelArgs& k, uint32_t bid, u
                 k.arrival[nxt][p] = (uint16_t)stamp;
                 gained = true;
                 born += (z >= k.own_z0 && z < k.own_z1) ? 1u : 0u;
-                tile = (uint32_t)(x / kTileX) +
-                       (uint32_t)g.tiles_x * ((uint32_t)(y / g.TY) + (uint32_t)g.tiles_y * (uint32_t)(z / g.TZ));
+                const int tx = x / kTileX, ty = y / g.TY, tz = z / g.TZ;
+                tile = (uint32_t)tx + (uint32_t)g.tiles_x * ((uint32_t)ty + (uint32_t)g.tiles_y * (uint32_t)tz);
+                faces = cell_faces(g, x, y, z, tx * kTileX, ty * g.TY, tz * g.TZ);
             }
         }
         if (!k.classic && __any_sync(0xFFFFFFFFu, gained))
             warp_append(k.chg_list[nxt], &ctrl->chg_count[nxt], k.chg_cap, lane, gained ? 1u : 0u, &gi);
-        // the tiles that gained lava have their neighbourhoods scheduled by the whole warp, once each
+        // the tiles that gained lava have their neighbourhoods scheduled by the whole warp, once each:
+        // the tile itself and the neighbours across the faces its new LAVA cells lie on
         unsigned todo = __ballot_sync(0xFFFFFFFFu, gained);
         while (todo) {
             const int src = __ffs(todo) - 1;
             const uint32_t tl = __shfl_sync(0xFFFFFFFFu, tile, src);
-            todo &= ~__ballot_sync(0xFFFFFFFFu, gained && tile == tl);
-            schedule_around(k, tl, t, nxt, lane, true, true);
+            const bool mine = gained && tile == tl;
+            todo &= ~__ballot_sync(0xFFFFFFFFu, mine);
+            const unsigned f = __reduce_or_sync(0xFFFFFFFFu, mine ? faces : 0u);
+            schedule_around(k, tl, t, nxt, lane, faces_reach(f, lane), true);
         }
     }
     const unsigned b = __reduce_add_sync(0xFFFFFFFFu, born);
