@@ -484,23 +484,33 @@ __device__ __forceinline__ bool air_gains_lava(const CaKernelArgs& k, const uint
 
 // Whether a tile whose LAVA touches the faces `f` (bits 2-7: -x, +x, -y, +y, -z, +z) can reach its
 // neighbour (dx, dy, dz) = lane's offset in the next step: LAVA lies within one cell of it only when it
-// touches the faces towards it.
-__device__ __forceinline__ bool faces_reach(unsigned f, int lane) {
+// touches the faces towards it.  In lava mode an AIR cell takes LAVA only from its own level, from
+// the level above, or by ponding from the cell straight below (gatherLavaCandidates,
+// LavaCA.hpp:462-519), so a tile above is reached only straight up and only by ponding (bit 7 is
+// then set only for LAVA that can pond upwards).
+__device__ __forceinline__ bool faces_reach(unsigned f, int lane, bool lava_mode) {
     const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+    if (lava_mode && dz > 0 && (dx != 0 || dy != 0)) return false;
     return (dx == 0 || ((f >> (dx < 0 ? 2 : 3)) & 1u)) && (dy == 0 || ((f >> (dy < 0 ? 4 : 5)) & 1u)) &&
            (dz == 0 || ((f >> (dz < 0 ? 6 : 7)) & 1u));
 }
 
-// The face bits of a cell (x, y, z) of the tile with origin (x0, y0, z0): the faces it lies on.
-__device__ __forceinline__ unsigned cell_faces(const CaGeom& g, int x, int y, int z, int x0, int y0, int z0) {
+// The face bits of a LAVA cell (x, y, z) of the tile with origin (x0, y0, z0): the faces it lies on;
+// the top face only when `up` (the cell can feed the one above it).
+__device__ __forceinline__ unsigned cell_faces(const CaGeom& g, int x, int y, int z, int x0, int y0, int z0, bool up) {
     unsigned f = 0;
     if (x == x0) f |= 1u << 2;
     if (x == min(x0 + kTileX, g.nx) - 1) f |= 1u << 3;
     if (y == y0) f |= 1u << 4;
     if (y == min(y0 + g.TY, g.ny) - 1) f |= 1u << 5;
     if (z == z0) f |= 1u << 6;
-    if (z == min(z0 + g.TZ, g.nz) - 1) f |= 1u << 7;
+    if (up && z == min(z0 + g.TZ, g.nz) - 1) f |= 1u << 7;
     return f;
+}
+// A LAVA cell at (x, y, z) can feed the AIR cell above it: in classic mode always, in lava mode by
+// ponding when that cell lies at or below its column's spill level (LavaCA.hpp:443-461).
+__device__ __forceinline__ bool feeds_up(const CaKernelArgs& k, int spill_level, int z) {
+    return k.classic || (k.ponding && k.spill != nullptr && z + 1 <= spill_level);
 }
 
 // Schedule the tiles within one tile of `tile` for step t + 1; lanes 0..26 of a warp each try one
@@ -769,8 +779,8 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
         // faces towards it; a tile that changed schedules itself
         for (int e = warp; e < nsched; e += kThreads / 32) {
             const unsigned f = s_sched_flag[e];
-            schedule_around(k, s_sched_tile[e], t, nxt, lane, ((f & 1u) && faces_reach(f, lane)) || ((f & 2u) && lane == 13),
-                            (f & 1u) != 0);
+            schedule_around(k, s_sched_tile[e], t, nxt, lane,
+                            ((f & 1u) && faces_reach(f, lane, !k.classic)) || ((f & 2u) && lane == 13), (f & 1u) != 0);
         }
         __syncthreads();
         nsched = 0;
@@ -1172,7 +1182,14 @@ __device__ __forceinline__ void rules_body(const CaTensorMaps& tm, const CaKerne
                 if (ly == 0) faces |= 1u << 4;
                 if (ly == min(g.TY, g.ny - y0) - 1) faces |= 1u << 5;
                 if (lz == 0) faces |= 1u << 6;
-                if (lz == min(g.TZ, g.nz - z0) - 1) faces |= 1u << 7;
+                if (lz == min(g.TZ, g.nz - z0) - 1) {
+                    bool up = k.classic;
+                    if (!up && stage_spill && k.ponding)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            up = up || (((surv >> (8 * j)) & 0xFFu) && z + 1 <= sl.spill[ly * kTileX + 4 * xq + j]);
+                    if (up) faces |= 1u << 7;
+                }
             }
             unsigned bits = (any_lava ? 1u : 0u) | (any_changed ? 2u : 0u) | faces;
             bits = __reduce_or_sync(0xFFFFFFFFu, bits);
@@ -1308,7 +1325,8 @@ __device__ __forceinline__ void cand_body(const CaKernelArgs& k, uint32_t bid, u
                 born += (z >= k.own_z0 && z < k.own_z1) ? 1u : 0u;
                 const int tx = x / kTileX, ty = y / g.TY, tz = z / g.TZ;
                 tile = (uint32_t)tx + (uint32_t)g.tiles_x * ((uint32_t)ty + (uint32_t)g.tiles_y * (uint32_t)tz);
-                faces = cell_faces(g, x, y, z, tx * kTileX, ty * g.TY, tz * g.TZ);
+                const int sp = (!k.classic && k.spill != nullptr) ? __ldg(k.spill + x + (int64_t)g.nx * y) : 0;
+                faces = cell_faces(g, x, y, z, tx * kTileX, ty * g.TY, tz * g.TZ, feeds_up(k, sp, z));
             }
         }
         if (!k.classic && __any_sync(0xFFFFFFFFu, gained))
@@ -1322,7 +1340,7 @@ __device__ __forceinline__ void cand_body(const CaKernelArgs& k, uint32_t bid, u
             const bool mine = gained && tile == tl;
             todo &= ~__ballot_sync(0xFFFFFFFFu, mine);
             const unsigned f = __reduce_or_sync(0xFFFFFFFFu, mine ? faces : 0u);
-            schedule_around(k, tl, t, nxt, lane, faces_reach(f, lane), true);
+            schedule_around(k, tl, t, nxt, lane, faces_reach(f, lane, !k.classic), true);
         }
     }
     const unsigned b = __reduce_add_sync(0xFFFFFFFFu, born);
