@@ -19,7 +19,8 @@ and MC run, outside their device events (c3's 7 GB of state is far larger than L
                  bytes per cell of the same kernel on the c3q case (profiles/), times the cells of a launch.
   kernels_ms     device time per step of the drop-depth, rules and candidate kernels.
   e2e            the same metric through the C ABI with host buffers: reset, terrain and vents from host
-                 memory, run, all five planes back into pinned host memory, host wall clock.
+                 memory, run, all five planes back into pinned host memory, host wall clock over a run of
+                 jobs with two in flight (one computing, the other's planes copying); one_at_a_time beside it.
   cpu_baseline   the reference engine (oracle/_ref/engine, --threads = host cores) on one full job.
   c2             the 256 x 256 x 128 workload: ACTIVE / DENSE figures and its parity.
   batched/served many small independent jobs through the job server (volcano_ca_mc_b200.serve).
@@ -49,6 +50,8 @@ BYTES_PER_TRIAL = 12         # spin read + spin write + mobility read
 # The reference arm's bounded sample: the first REF_SAMPLE_STEPS CA steps of the workload's job (its
 # front sweep runs from step 0 only: the reference engine has no resume), MC off.
 REF_SAMPLE_STEPS = {"c1": 300, "c2": 400, "c3": 300, "c3q": 300}
+# jobs in flight in the e2e measurement: one computing while the other's planes travel
+E2E_INFLIGHT = 2
 
 
 def parse():
@@ -303,37 +306,76 @@ class Resident:
 
 
 class E2E:
-    """The call sequence of a job through the C ABI on one resident handle: reset, terrain and vents
-    from host memory, run to the stop rule, all five planes back into pinned host memory.  The handle
-    and the pinned buffers are set up once, outside the timed steps."""
+    """The call sequence of a job through the C ABI: reset, terrain and vents from host memory, run to
+    the stop rule, all five planes back into pinned host memory.  Jobs go through `inflight` resident
+    handles, each driven by a host thread of its own; a lock admits one vca_ca_run at a time, so every
+    job computes with the whole GPU to itself while the previous job's planes travel back to the host
+    and the next job's terrain goes up (the job server's form).  With inflight = 1 this is the plain
+    one-at-a-time sequence.  Handles and pinned buffers are set up once, outside the timed jobs."""
 
-    def __init__(self, w, device):
+    def __init__(self, w, device, inflight=1):
         import torch
         from volcano_ca_mc_b200 import capi
         self.w = w
-        self.ca = capi.LavaCA(ca_params(w, capi.SWEEP_ACTIVE, device))
         n = w.cells
         pin = lambda dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()
-        self.out = (pin(torch.uint8), pin(torch.int32), pin(torch.float32), pin(torch.int16).view("uint16"),
-                    pin(torch.int16).view("uint16"))
+        self.slots = []
+        for _ in range(inflight):
+            ca = capi.LavaCA(ca_params(w, capi.SWEEP_ACTIVE, device))
+            out = (pin(torch.uint8), pin(torch.int32), pin(torch.float32), pin(torch.int16).view("uint16"),
+                   pin(torch.int16).view("uint16"))
+            self.slots.append((ca, out))
         self.heights = torch.from_numpy(w.heights.copy()).pin_memory().numpy()
+        self.vents = w.vent_cells()
 
-    def step(self):
-        """One job; returns (ms, steps)."""
+    def jobs(self, count):
+        """`count` jobs; returns (wall ms of all of them, CA steps summed, per-phase medians in ms)."""
+        run_lock, take_lock = threading.Lock(), threading.Lock()
+        todo = [count]
+        phases, steps, errors = [], [], []
+
+        def worker(ca, out):
+            try:
+                while True:
+                    with take_lock:
+                        if todo[0] == 0:
+                            return
+                        todo[0] -= 1
+                    t0 = time.perf_counter()
+                    ca.reset()
+                    ca.apply_terrain(self.heights)
+                    ca.place_seeds(self.vents)
+                    t1 = time.perf_counter()
+                    with run_lock:
+                        t2 = time.perf_counter()
+                        ca.run()
+                        t3 = time.perf_counter()
+                    ca.download(out)
+                    t4 = time.perf_counter()
+                    steps.append(ca.info().steps)
+                    phases.append((t1 - t0, t3 - t2, t4 - t3))
+            except Exception as e:  # noqa: BLE001
+                errors.append(e)
+
+        threads = [threading.Thread(target=worker, args=s) for s in self.slots]
         t0 = time.perf_counter()
-        self.ca.reset()
-        self.ca.apply_terrain(self.heights)
-        self.ca.place_seeds(self.w.vent_cells())
-        self.ca.run()
-        self.ca.download(self.out)
-        steps = self.ca.info().steps
-        return (time.perf_counter() - t0) * 1e3, steps
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        wall = (time.perf_counter() - t0) * 1e3
+        if errors:
+            raise errors[0]
+        med = {k: round(statistics.median(p[i] for p in phases) * 1e3, 2)
+               for i, k in enumerate(("prep_ms", "run_ms", "download_ms"))}
+        return wall, sum(steps), med
 
     def bytes(self):
-        return self.heights.nbytes + 16 * len(self.w.vents), sum(int(a.nbytes) for a in self.out)
+        return self.heights.nbytes + 16 * len(self.w.vents), sum(int(a.nbytes) for a in self.slots[0][1])
 
     def close(self):
-        self.ca.close()
+        for ca, _ in self.slots:
+            ca.close()
 
 
 def roofline(p, w, schedule, peak, peak_kind):
@@ -570,17 +612,22 @@ def ours(args):
     roof_dense = roofline(profs["dense"], w, "dense", peak, peak_kind)
     roof_active = roofline(profs["active"], w, "active", peak, peak_kind)
 
-    # e2e through the C ABI with host buffers, on a resident handle
-    e2e = E2E(w, local)
-    e2e.step()  # warm-up
-    e2e_runs = [e2e.step() for _ in range(max(1, min(3, args.steps)))]
-    e2e_ms = sum(r[0] for r in e2e_runs)
-    e2e_cu = sum(r[1] * w.cells for r in e2e_runs)
+    # e2e through the C ABI with host buffers on resident handles: two jobs in flight (one computing,
+    # one copying), and one at a time
+    e2e = E2E(w, local, inflight=E2E_INFLIGHT)
+    e2e.jobs(E2E_INFLIGHT)  # warm-up: one job per handle
+    e2e_jobs = max(2 * E2E_INFLIGHT, min(4 * E2E_INFLIGHT, args.steps))
+    e2e_ms, e2e_steps, e2e_phases = e2e.jobs(e2e_jobs)
     e2e_h2d, e2e_d2h = e2e.bytes()
     e2e.close()
+    e1 = E2E(w, local, inflight=1)
+    e1.jobs(1)
+    e1_jobs = max(1, min(3, args.steps))
+    e1_ms, e1_steps, e1_phases = e1.jobs(e1_jobs)
+    e1.close()
 
-    ca_ms, mc_ms, dense_ms, e2e_ms, wall_ms = max_over_ranks([ca_ms, mc_ms, dj["ca_ms"], e2e_ms, wall * 1e3],
-                                                             f"cuda:{local}", world)
+    ca_ms, mc_ms, dense_ms, e2e_ms, e1_ms, wall_ms = max_over_ranks(
+        [ca_ms, mc_ms, dj["ca_ms"], e2e_ms, e1_ms, wall * 1e3], f"cuda:{local}", world)
     extra = {}
     cpu = None
     if rank == 0 and world == 1:
@@ -630,10 +677,15 @@ def ours(args):
         "kernels_ms": {"active": profs["active"]["kernels"], "dense": profs["dense"]["kernels"]},
         "active_tiles_frac": round(profs["active"]["tiles"] / max(1, profs["active"]["tiles_total"] *
                                                                    profs["active"]["steps"]), 4),
-        "e2e": {"value": world * e2e_cu / (e2e_ms * 1e-3), "unit": "cell-updates/s",
-                "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h, "ms_per_step": e2e_ms / len(e2e_runs),
-                "path": "vca_ca_reset + apply_terrain (host priority flood + upload) + place_seeds + run + download of "
-                        "the five planes into pinned memory, one resident handle, host wall clock"},
+        "e2e": {"value": world * w.cells * e2e_steps / (e2e_ms * 1e-3), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h, "ms_per_step": e2e_ms / e2e_jobs,
+                "jobs": e2e_jobs, "jobs_in_flight": E2E_INFLIGHT, "phases_median": e2e_phases,
+                "path": "per job: vca_ca_reset + apply_terrain (host priority flood + upload) + place_seeds + run + "
+                        "download of the five planes into pinned memory; resident handles each driven by a host "
+                        "thread, one run at a time (a job's download and the next job's upload overlap the running "
+                        "job); host wall clock over all jobs, first job's upload and last job's download included",
+                "one_at_a_time": {"value": world * w.cells * e1_steps / (e1_ms * 1e-3), "ms_per_step": e1_ms / e1_jobs,
+                                  "jobs": e1_jobs, "phases_median": e1_phases}},
         "gpu_launches": launches,
         "clocks": clocks,
         "wall_s_timed_loop": round(wall_ms / 1e3, 3),

@@ -1506,6 +1506,16 @@ __global__ void ca_init_schedule_kernel(const __grid_constant__ CaKernelArgs k, 
 }
 
 // Fill the padding cells x in [nx, P) of every row with VOID (both buffers).
+// The control block copied by one warp into host-mapped pinned memory.  A kernel, not a
+// device-to-host copy: such a copy queues on the copy engines behind any large download of another
+// handle on the same device, and the next step graph would wait behind it.
+__global__ void ca_ctrl_snapshot_kernel(const CaCtrl* src, CaCtrl* dst) {
+    static_assert(sizeof(CaCtrl) % sizeof(uint32_t) == 0, "CaCtrl is copied as words");
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    volatile uint32_t* d = reinterpret_cast<volatile uint32_t*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(CaCtrl) / sizeof(uint32_t)); i += 32) d[i] = s[i];
+}
+
 __global__ void ca_pad_kernel(uint8_t* t0, uint8_t* t1, int nx, int P, int64_t rows) {
     const int pad = P - nx;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows * pad; i += (int64_t)gridDim.x * blockDim.x) {
@@ -1708,7 +1718,8 @@ void drop_graph(vca_ca* h) {
 
 // Pull the control block to the host mirror.
 vca_status sync_ctrl(vca_ca* h) {
-    VCA_CUDA(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(CaCtrl), cudaMemcpyDeviceToHost, h->stream));
+    ca_ctrl_snapshot_kernel<<<1, 32, 0, h->stream>>>(h->ctrl, h->ctrl_host_dev);
+    VCA_CUDA(cudaGetLastError());
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     h->steps = (int)h->ctrl_host->steps;
     h->stop = h->ctrl_host->stop;
@@ -1852,9 +1863,10 @@ vca_status run_graphs(vca_ca* h, const CaKernelArgs& k) {
     for (int launched = 0; launched < needed; ++launched) {
         const int slot = launched & 1;
         VCA_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
-        VCA_CUDA(cudaMemcpyAsync(&h->ctrl_ring[slot], h->ctrl, sizeof(CaCtrl), cudaMemcpyDeviceToHost, h->stream));
+        ca_ctrl_snapshot_kernel<<<1, 32, 0, h->stream>>>(h->ctrl, h->ctrl_ring_dev + slot);
+        VCA_CUDA(cudaGetLastError());
         VCA_CUDA(cudaEventRecord(h->ring_ev[slot], h->stream));
-        h->launches += 3 * kGraphSteps;
+        h->launches += 3 * kGraphSteps + 1;
         if (pending >= 0) {
             VCA_CUDA(cudaEventSynchronize(h->ring_ev[pending]));
             if (h->ctrl_ring[pending].stop != VCA_STOP_RUNNING || h->ctrl_ring[pending].error) break;
@@ -2308,8 +2320,9 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
     ALLOC(h->heights_dev, sizeof(int32_t) * need.cols);
 #undef ALLOC
     h->cap = need;
-    e = cudaMallocHost(&h->ctrl_host, sizeof(CaCtrl));
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaHostAlloc(&h->ctrl_host, sizeof(CaCtrl), cudaHostAllocMapped)) != cudaSuccess ||
+        (e = cudaHostGetDevicePointer(&h->ctrl_host_dev, h->ctrl_host, 0)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaHostAlloc (mapped)"));
     if ((e = rules_occupancy<ShapeA>(&h->rules_per_sm[0])) != cudaSuccess ||
         (e = rules_occupancy<ShapeB>(&h->rules_per_sm[1])) != cudaSuccess ||
         (e = rules_occupancy<ShapeC>(&h->rules_per_sm[2])) != cudaSuccess)
@@ -2320,7 +2333,9 @@ vca_status vca_ca_create(const vca_ca_desc* d, vca_ca** out) {
         (e = cudaEventCreateWithFlags(&h->ring_ev[0], cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&h->ring_ev[1], cudaEventDisableTiming)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaEventCreate"));
-    if ((e = cudaMallocHost(&h->ctrl_ring, 2 * sizeof(CaCtrl))) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaHostAlloc(&h->ctrl_ring, 2 * sizeof(CaCtrl), cudaHostAllocMapped)) != cudaSuccess ||
+        (e = cudaHostGetDevicePointer(&h->ctrl_ring_dev, h->ctrl_ring, 0)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaHostAlloc (mapped)"));
     const char* prof = std::getenv("VCA_PROFILE_KERNELS");
     h->profile_kernels = prof != nullptr && prof[0] == '1';
     if (vca_status s = configure(h, d)) return fail(s);

@@ -929,7 +929,8 @@ struct vca_mc {
     std::vector<uint64_t> color_off;
     unsigned long long* table = nullptr;
     McCtrl* ctrl = nullptr;
-    McCtrl* ctrl_host = nullptr;
+    McCtrl* ctrl_host = nullptr;      // pinned, host-mapped mirror
+    McCtrl* ctrl_host_dev = nullptr;  // its device address
     bool domain_set = false;
     bool initialized = false;
     int sms = 148;
@@ -993,8 +994,18 @@ McArgs mc_args(const vca_mc* h) {
     return a;
 }
 
+// The control block copied by one warp into host-mapped pinned memory (not a device-to-host copy,
+// which would queue behind another handle's large download on the copy engines).
+__global__ void mc_ctrl_snapshot_kernel(const McCtrl* src, McCtrl* dst) {
+    static_assert(sizeof(McCtrl) % sizeof(uint32_t) == 0, "McCtrl is copied as words");
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    volatile uint32_t* d = reinterpret_cast<volatile uint32_t*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(McCtrl) / sizeof(uint32_t)); i += 32) d[i] = s[i];
+}
+
 vca_status mc_sync(vca_mc* h) {
-    VCA_CUDA(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(McCtrl), cudaMemcpyDeviceToHost, h->stream));
+    mc_ctrl_snapshot_kernel<<<1, 32, 0, h->stream>>>(h->ctrl, h->ctrl_host_dev);
+    VCA_CUDA(cudaGetLastError());
     VCA_CUDA(cudaStreamSynchronize(h->stream));
     return VCA_OK;
 }
@@ -1255,7 +1266,9 @@ vca_status vca_mc_create(const vca_mc_desc* d, vca_mc** out) {
         (e = cudaMalloc(&h->table, 8 * kTableSide * kTableSide)) != cudaSuccess ||
         (e = cudaMalloc(&h->ctrl, sizeof(McCtrl))) != cudaSuccess)
         return fail(cuda_fail(e, "cudaMalloc"));
-    if ((e = cudaMallocHost(&h->ctrl_host, sizeof(McCtrl))) != cudaSuccess) return fail(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaHostAlloc(&h->ctrl_host, sizeof(McCtrl), cudaHostAllocMapped)) != cudaSuccess ||
+        (e = cudaHostGetDevicePointer(&h->ctrl_host_dev, h->ctrl_host, 0)) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaHostAlloc (mapped)"));
     if ((e = cudaEventCreate(&h->ev_a)) != cudaSuccess || (e = cudaEventCreate(&h->ev_b)) != cudaSuccess)
         return fail(cuda_fail(e, "cudaEventCreate"));
     const char* prof = std::getenv("VCA_PROFILE_KERNELS");

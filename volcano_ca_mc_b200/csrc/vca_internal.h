@@ -177,7 +177,8 @@ struct vca_ca {
     size_t flow_sums_cap = 0;
     int vent_slots = 0;
     vca::CaCtrl* ctrl = nullptr;
-    vca::CaCtrl* ctrl_host = nullptr;   // pinned mirror
+    vca::CaCtrl* ctrl_host = nullptr;   // pinned, host-mapped mirror
+    vca::CaCtrl* ctrl_host_dev = nullptr;  // its device address
     uint32_t* tile_flags = nullptr;
     uint32_t* tile_mark[2] = {nullptr, nullptr};
     int8_t* desc_plane = nullptr;
@@ -203,7 +204,8 @@ struct vca_ca {
     vca::CaKernelArgs graph_args;            // the arguments, maps and grids graph_exec was captured with
     vca::CaTensorMaps graph_tm;
     int graph_grid = 0, graph_cand = 0;
-    vca::CaCtrl* ctrl_ring = nullptr;       // pinned: two in-flight copies of the control block
+    vca::CaCtrl* ctrl_ring = nullptr;       // pinned, host-mapped: two in-flight copies of the control block
+    vca::CaCtrl* ctrl_ring_dev = nullptr;   // its device address
     cudaEvent_t ring_ev[2] = {nullptr, nullptr};
     vca_ca_batch* batch = nullptr;          // the batch stepping this handle, if any (vca_ca_batch_add)
     int batch_slot = -1;
