@@ -464,7 +464,8 @@ def job_mixes(args, device):
     agree between the two modes."""
     from volcano_ca_mc_b200 import serve
 
-    keys = ("slots", "jobs", "makespan_s", "jobs_per_s", "cell_updates_per_s", "p50_s", "p99_s", "mean_concurrency")
+    keys = ("slots", "jobs", "makespan_s", "jobs_per_s", "cell_updates_per_s", "p50_s", "p99_s", "mean_concurrency",
+            "phases_ms")
     pick = lambda r: {k: (round(r[k], 4) if isinstance(r[k], float) else r[k]) for k in keys}
     out = {}
     # a whole mix takes one to three seconds and varies by up to a third from run to run (host

@@ -45,17 +45,20 @@ public:
     void update(const void* data, size_t n) {
         const unsigned char* p = static_cast<const unsigned char*>(data);
         total_ += n;
-        while (n > 0) {
+        if (fill_ > 0) {  // complete the staged block first
             const size_t take = std::min(n, sizeof(buf_) - fill_);
             std::memcpy(buf_ + fill_, p, take);
             fill_ += take;
             p += take;
             n -= take;
-            if (fill_ == sizeof(buf_)) {
-                block(buf_);
-                fill_ = 0;
-            }
+            if (fill_ < sizeof(buf_)) return;
+            block(buf_);
+            fill_ = 0;
         }
+        // whole blocks straight from the input; the tail is staged
+        for (; n >= sizeof(buf_); p += sizeof(buf_), n -= sizeof(buf_)) block(p);
+        std::memcpy(buf_, p, n);
+        fill_ = n;
     }
     std::string hex() const {
         uint64_t h = (lane_[0] * 3) ^ (lane_[1] * 5) ^ (lane_[2] * 7) ^ (lane_[3] * 11);
@@ -432,6 +435,7 @@ private:
                 double ca_done = 0.0;
                 if (!r->out.empty()) fs::create_directories(r->out);
                 Timing timing;
+                timing.detail = true;
                 Progress progress;
                 RunHandles res;
                 res.ca = slot->ca;
@@ -452,6 +456,7 @@ private:
                 resp["steps"] = job.ca.steps;
                 resp["stop"] = stop_text(job.ca.stop);
                 resp["cell_updates"] = (unsigned long long)r->cfg.space.cells() * (unsigned long long)job.ca.steps;
+                const auto td = Clock::now();
                 Json dg = Json::object();
                 if (job.ca.ca_ran) dg["ca_result.bin"] = ca_digest(job.ca.result);
                 if (job.mc_ran) {
@@ -460,6 +465,14 @@ private:
                     resp["energyEnd"] = job.mc.history.back().energy;
                 }
                 resp["digest"] = dg;
+                // where the job's time went: the sections of its times.json, the MC set-up details and
+                // the digests (caDevice / mcDevice are running totals of the resident handles: left out)
+                Json tm = Json::object();
+                for (const auto& sec : timing.sections) tm[sec.first] = round_to(sec.second, 3);
+                for (const auto& det : timing.details)
+                    if (det.first != "caDevice" && det.first != "mcDevice") tm[det.first] = round_to(det.second, 3);
+                tm["digest"] = round_to(ms_since(td), 3);
+                resp["times_ms"] = tm;
                 if (!r->out.empty()) resp["out"] = r->out;
                 {
                     std::lock_guard<std::mutex> lk(om_);
