@@ -77,3 +77,13 @@ def test_server_answers_refused_requests_without_a_gpu():
     assert "hexagonal" in srv.answers["b"]["error"]
     assert "Nie można otworzyć pliku konfiguracyjnego" in srv.answers["c"]["error"]
     assert srv.summary["failed"] == 3 and srv.summary["jobs"] == 0
+
+
+def test_phase_sums_add_the_answers_sections():
+    """The per-mode phase sums of the bench: every answer's times_ms sections added up; answers
+    without times (refused requests) add nothing."""
+    recs = [{"times_ms": {"caSim": 2.5, "save": 1.0, "digest": 0.25}},
+            {"times_ms": {"caSim": 1.5, "mcSim": 3.0, "digest": 0.75}},
+            {"status": "error"}]
+    assert serve.phase_sums(recs) == {"caSim": 4.0, "save": 1.0, "digest": 1.0, "mcSim": 3.0}
+    assert serve.phase_sums([]) == {}

@@ -235,16 +235,23 @@ def run(jobs: list[JobSpec], slots: int = 16, batched: bool = True, budget_gb: f
     makespan = (last - first) / 1e3
     lat = np.array([r["latency_ms"] / 1e3 for r in recs.values()])
     busy = sum(r["done_ms"] - r["admitted_ms"] for r in recs.values()) / 1e3
-    phases: dict[str, float] = {}
-    for r in recs.values():
-        for k, v in r.get("times_ms", {}).items():
-            phases[k] = phases.get(k, 0.0) + v
+    phases = phase_sums(recs.values())
     return {"records": recs, "slots": slots, "batched": batched, "jobs": len(recs), "makespan_s": makespan,
             "jobs_per_s": len(recs) / makespan if makespan > 0 else 0.0,
             "cell_updates_per_s": sum(r["cell_updates"] for r in recs.values()) / makespan if makespan > 0 else 0.0,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_concurrency": busy / makespan if makespan > 0 else 0.0, "server": srv.summary,
-            "phases_ms": {k: round(v, 3) for k, v in phases.items()}}
+            "phases_ms": phases}
+
+
+def phase_sums(records) -> dict[str, float]:
+    """The per-section times of the answers (`times_ms`: times.json sections, MC set-up details,
+    digest) summed over the jobs, in ms."""
+    sums: dict[str, float] = {}
+    for r in records:
+        for k, v in r.get("times_ms", {}).items():
+            sums[k] = sums.get(k, 0.0) + float(v)
+    return {k: round(v, 3) for k, v in sums.items()}
 
 
 def compare(a: dict, b: dict) -> int:
