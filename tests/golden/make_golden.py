@@ -7,6 +7,8 @@ Run where the reference sources are at hand (the reference engine is built by
     python tests/golden/make_golden.py --large         # hashes of the full-size 1024 x 1024 x 256 workload (c3)
     python tests/golden/make_golden.py --large c1 c2   # the same for the 512 x 1 x 256 and 256 x 256 x 128 workloads
     python tests/golden/make_golden.py --config-errors # the reference's validation messages for bad configs
+    VCA_REFERENCE_DIR=<checkout> python tests/golden/make_golden.py --ref-configs
+                                                       # the reference's own configs/*.json (ref_<name>/)
 
 For every case in CASES it writes ``cases/<name>.json`` (the config, in the reference's schema),
 runs ``engine --config cases/<name>.json --out <tmp>`` and stores under ``<name>/``:
@@ -205,8 +207,8 @@ def expectation(out: str, rc: int) -> dict:
     return exp
 
 
-def run_ref(args: list[str]) -> int:
-    r = subprocess.run([O.REF_ENGINE, *args], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+def run_ref(args: list[str], cwd: str | None = None) -> int:
+    r = subprocess.run([O.REF_ENGINE, *args], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, cwd=cwd)
     if r.returncode != 0:
         sys.stderr.write(r.stderr)
     return r.returncode
@@ -285,9 +287,72 @@ def config_errors() -> None:
     print("config_errors ok")
 
 
+# The reference's own config files (configs/*.json of its checkout), run as they are (each takes
+# under a second of reference CPU time); mc_basalt is the reference's MC-only config, run with
+# --mc-from on the result of REF_MC_FROM's CA run.  Only the reference engine's outputs are kept:
+# config_used.json (its merged config), the step-0 state and the hashes.
+REF_CONFIGS = ["test_2d", "test_3d", "lava_mc_2d", "lava_mc_3d", "heightmap_kaldera", "heightmap_kanion",
+               "heightmap_podwojny", "etna_3d", "etna_real", "etna_real_boczna", "wezuwiusz_real", "classic_ref",
+               "mc_full_2d", "mc_full_3d"]
+REF_MC_FROM = {"mc_basalt": "lava_mc_3d"}
+
+
+def ref_configs() -> None:
+    """tests/golden/ref_<name>/: the reference engine run on its own configs/<name>.json: expect.json
+    (hashes, stats, mc_stats.csv), config_used.json (the engine's merged config) and, for a CA run,
+    initial.npz (its step-0 snapshot).  The checkout is the working directory of each run: heightmap
+    paths in the configs are relative to it."""
+    ref = os.environ.get("VCA_REFERENCE_DIR", "")
+    if not ref:
+        sys.exit("set VCA_REFERENCE_DIR to the reference checkout")
+    tmp = tempfile.mkdtemp(prefix="vca_golden_ref_")
+    # bin results (the configs ask for txt too) and the GPU update (a config asking for the random
+    # sequential update would be refused by bin/engine)
+    over = ["--set", "output.format=bin", "--set", "mc.update=checkerboard"]
+
+    def keep(name: str, out: str, source: str) -> None:
+        dst = os.path.join(HERE, f"ref_{name}")
+        os.makedirs(dst, exist_ok=True)
+        exp = expectation(out, 0)
+        exp["source"] = source
+        with open(os.path.join(dst, "expect.json"), "w") as f:
+            json.dump(exp, f, indent=1, ensure_ascii=False)
+            f.write("\n")
+        shutil.copyfile(os.path.join(out, "config_used.json"), os.path.join(dst, "config_used.json"))
+
+    try:
+        outs = {}
+        for name in REF_CONFIGS:
+            src = os.path.join(ref, "configs", f"{name}.json")
+            out = os.path.join(tmp, name)
+            assert run_ref(["--config", src, "--out", out, *over], cwd=ref) == 0, name
+            outs[name] = out
+            keep(name, out, f"configs/{name}.json of the reference")
+            with open(os.path.join(out, "config_used.json")) as f:
+                used = json.load(f)
+            if not (used["mc"]["enabled"] and used["mc"]["domain"] == "full"):
+                init = os.path.join(tmp, name + "_init")
+                assert run_ref(["--config", src, "--out", init, *over, "--set", "output.snapshotsEvery=65535",
+                                "--set", "mc.enabled=false"], cwd=ref) == 0, name
+                save_initial(os.path.join(HERE, f"ref_{name}", "initial.npz"),
+                             O.read_ca_bin(os.path.join(init, "snapshots", "step_000000.bin")))
+            print(name, "ok")
+        for name, src_name in REF_MC_FROM.items():
+            src = os.path.join(ref, "configs", f"{name}.json")
+            out = os.path.join(tmp, name)
+            assert run_ref(["--mc-from", outs[src_name], "--config", src, "--out", out, *over], cwd=ref) == 0, name
+            keep(name, out, f"configs/{name}.json of the reference, --mc-from the result of ref_{src_name}")
+            print(name, "ok")
+    finally:
+        shutil.rmtree(tmp)
+
+
 def main() -> None:
     if "--config-errors" in sys.argv:
         config_errors()
+        return
+    if "--ref-configs" in sys.argv:
+        ref_configs()
         return
     if "--large" in sys.argv:
         names = [a for a in sys.argv[sys.argv.index("--large") + 1:] if not a.startswith("-")] or ["c3"]
