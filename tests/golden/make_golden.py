@@ -315,10 +315,13 @@ def ref_configs() -> None:
         os.makedirs(dst, exist_ok=True)
         exp = expectation(out, 0)
         exp["source"] = source
+        # the generator's scratch folder (named by --mc-from runs) is not part of the fixture
         with open(os.path.join(dst, "expect.json"), "w") as f:
-            json.dump(exp, f, indent=1, ensure_ascii=False)
-            f.write("\n")
-        shutil.copyfile(os.path.join(out, "config_used.json"), os.path.join(dst, "config_used.json"))
+            f.write(json.dumps(exp, indent=1, ensure_ascii=False).replace(tmp, "<scratch>") + "\n")
+        with open(os.path.join(out, "config_used.json")) as f:
+            used = f.read()
+        with open(os.path.join(dst, "config_used.json"), "w") as f:
+            f.write(used.replace(tmp, "<scratch>"))
 
     try:
         outs = {}
