@@ -267,6 +267,21 @@ CONFIG_ERRORS: list[list[str]] = [
     ["ca.mode=classic", "mc.enabled=true"], ["ca.mode=classic", "vents.count=100000000", "space.nx=20", "space.nz=20"],
     ["vents.positions=[[1,0]]"], ["ca.mode=classic", "vents.placement=positions"],
     ["mc.enabled=true", "mc.domain=full", "mc.update=checkerboard"], ["output.format=png"], ["mc.statsEvery=0"],
+    ["mc.domain=foo"], ["mc.mobilityMin=-1"], ["mc.mobilityMin=1.5"], ["vents.placement=xyz"], ["terrain.type=xyz"],
+    ["terrain.peakHeight=-5"], ["terrain.baseRadius=0"], ["terrain.craterRadius=-1"], ["terrain.noise=-0.5"],
+    ["output.snapshotsEvery=-1"], ["ca.coolingAmbient=-1"], ["ca.coolingLateral=-2"], ["ca.coolingFall=-0.1"],
+    ["ca.solidusTemp=-5"], ["ca.solidusTemp=2000"], ["rngSeed=-1"], ["rngSeed=1.5"], ["space.nz=0"],
+    ["neighborhood=foo"], ["mc.update=foo"], ["mc.mcs=-1"], ["ca.sweep=foo"], ["grid=matrix"],
+    ["parallel.threads=-2"], ["parallel.schedule=foo"], ["parallel.chunk=-1"], ["parallel.affinity=foo"],
+    ["parallel.priority=foo"], ["mc.Q=100000"], ["mc.snapshotsEvery=-1"], ["vents.eruptionSteps=-1"],
+    ["vents.count=-1"], ["ca.mode=foo"], ["mc.enabled=1"], ["output.format=bin", "output.snapshotsEvery=5"],
+    ["terrain.type=flat"], ["space.nx=3", "space.nz=3"], ["vents.placement=random"], ["ca.maxSteps=70000"],
+    ["ca.maxSteps=1.5"], ["boundary=periodic", "space.nx=1"], ["mc.J=-1"],
+    ["mc.domain=full", "mc.enabled=true", "mc.update=checkerboard", "ca.mode=classic"], ["terrain.file=x.csv"],
+    ["vents.positions=[[1,2,3]]"], ["space.ny=2", "neighborhood=hexagonal", "space.nz=1"],
+    # number literals beyond the double range: an overflow is the JSON library's range error, an
+    # underflow the nearest value
+    ["mc.kT=1e400"], ["mc.kT=-1e400"], ["space.nx=1e400"], ["mc.kT=1e-400"],
 ]
 
 

@@ -108,3 +108,16 @@ def test_validation_messages_equal_reference():
         r = run(*args)
         out = json.loads(r.stdout)
         assert (r.returncode, out["errors"], out["warnings"]) == (case["exit"], case["errors"], case["warnings"]), case
+
+
+def test_number_overflow_in_a_config_file(tmp_path):
+    """A literal beyond the double range in a config file is the reference's JSON range error, word
+    for word and not wrapped as a syntax error: listed by --validate, and in a run the generic error
+    (exit 3, prefix "Błąd: "), as the reference engine gives it for the same file."""
+    cfg = tmp_path / "overflow.json"
+    cfg.write_text('{"mc": {"kT": 1e400}}')
+    text = "[json.exception.out_of_range.406] number overflow parsing '1e400'"
+    r = run("--validate", "--config", str(cfg))
+    assert r.returncode == 1 and json.loads(r.stdout)["errors"] == [text]
+    r = run("--config", str(cfg), "--out", str(tmp_path / "out"))
+    assert r.returncode == 3 and r.stderr.strip() == "Błąd: " + text

@@ -4,6 +4,7 @@
 #include <charconv>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace eng {
@@ -112,6 +113,16 @@ struct Parser {
         }
         double d = 0.0;
         auto r = std::from_chars(b, e, d);
+        if (r.ec == std::errc::result_out_of_range && r.ptr == e) {
+            // beyond the double range: an underflow is the nearest value (0 or a subnormal), as
+            // strtod gives it; an overflow is an error that names the literal, in the text of the
+            // reference's JSON library (its out_of_range error 406)
+            const std::string lit(b, e);
+            d = std::strtod(lit.c_str(), nullptr);
+            if (!std::isfinite(d))
+                throw JsonRangeError("[json.exception.out_of_range.406] number overflow parsing '" + lit + "'");
+            return Json(d);
+        }
         if (r.ec != std::errc() || r.ptr != e) fail("invalid number");
         return Json(d);
     }

@@ -137,6 +137,14 @@ struct JsonError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
+// A number literal whose value is beyond the range of a double.  Not a JsonError: the reference's
+// JSON library reports it as a range error, which its config loader does not turn into a syntax
+// message or a plain-string override, so it leaves the loader as it is (engine/src/io/Config.cpp
+// catches parse errors only).
+struct JsonRangeError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 // Shortest round-trip text of a double in the writer's format.
 std::string format_double(double d);
 
