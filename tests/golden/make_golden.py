@@ -7,6 +7,7 @@ Run where the reference sources are at hand (the reference engine is built by
     python tests/golden/make_golden.py --large         # hashes of the full-size 1024 x 1024 x 256 workload (c3)
     python tests/golden/make_golden.py --large c1 c2   # the same for the 512 x 1 x 256 and 256 x 256 x 128 workloads
     python tests/golden/make_golden.py --config-errors # the reference's validation messages for bad configs
+    python tests/golden/make_golden.py --cli-errors    # its messages for refused command lines
     VCA_REFERENCE_DIR=<checkout> python tests/golden/make_golden.py --ref-configs
                                                        # the reference's own configs/*.json (ref_<name>/)
 
@@ -365,9 +366,51 @@ def ref_configs() -> None:
         shutil.rmtree(tmp)
 
 
+# Command lines that the reference engine refuses before any simulation work (engine/src/app/Cli.cpp,
+# Batch.cpp, ConfigCheck.cpp): "{d}" is a scratch folder holding one config, c.json.
+CLI_ERRORS: list[list[str]] = [
+    ["--out"], ["--config"], ["--frobnicate"], ["--threads", "abc", "--out", "{d}/o"],
+    ["--threads", "-3", "--out", "{d}/o"], ["--batch", "{d}", "--config", "{d}/c.json"], ["--batch", "{d}", "--mc-from", "{d}"],
+    ["--set"], ["--set", "novalue", "--validate"], ["--print-defaults", "--out", "{d}/o"],
+    ["--mc-from", "{d}/nope", "--out", "{d}/o"], ["--config", "{d}/missing.json", "--out", "{d}/o"], ["--batch", "{d}/nope"],
+    ["--threads"], ["--progress", "--validate"], ["--timing-detail", "--validate"], ["--set", "=5", "--validate"],
+    ["positional"], ["--config", "{d}/c.json", "--batch", "{d}"], ["--validate", "--batch", "{d}"],
+    ["--print-defaults", "--validate"], ["--validate", "--mc-from", "{d}/nope"], ["--validate", "--mc-from", "{d}"],
+    ["--validate", "--mc-from", "{d}", "--set", "mc.domain=full"], ["--validate", "--config", "{d}/c.json", "--set", "terrain.type=file",
+                                                                    "--set", "terrain.file={d}/nope.csv"],
+    ["--batch", "{d}/empty", "--out", "{d}/o"],
+]
+
+
+def cli_errors() -> None:
+    """tests/golden/cli_errors.json: the reference engine's exit code and first line of stderr (the
+    message; its usage text follows argument errors) for each command line of CLI_ERRORS."""
+    tmp = tempfile.mkdtemp(prefix="vca_golden_cli_")
+    try:
+        with open(os.path.join(tmp, "c.json"), "w") as f:
+            f.write('{"space": {"nx": 40, "ny": 1, "nz": 30}}')
+        os.makedirs(os.path.join(tmp, "empty"))
+        out = []
+        for args in CLI_ERRORS:
+            real = [a.replace("{d}", tmp) for a in args]
+            r = subprocess.run([O.REF_ENGINE, *real], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, cwd=tmp)
+            first = (r.stderr.strip().splitlines() or [""])[0].replace(tmp, "{d}")
+            stdout = r.stdout.replace(tmp, "{d}") if r.stdout.strip() else None  # --validate's report
+            out.append({"args": args, "exit": r.returncode, "stderr_first_line": first, "stdout": stdout})
+        with open(os.path.join(HERE, "cli_errors.json"), "w") as f:
+            json.dump(out, f, indent=1, ensure_ascii=False)
+            f.write("\n")
+        print("cli_errors ok")
+    finally:
+        shutil.rmtree(tmp)
+
+
 def main() -> None:
     if "--config-errors" in sys.argv:
         config_errors()
+        return
+    if "--cli-errors" in sys.argv:
+        cli_errors()
         return
     if "--ref-configs" in sys.argv:
         ref_configs()

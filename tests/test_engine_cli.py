@@ -121,3 +121,21 @@ def test_number_overflow_in_a_config_file(tmp_path):
     assert r.returncode == 1 and json.loads(r.stdout)["errors"] == [text]
     r = run("--config", str(cfg), "--out", str(tmp_path / "out"))
     assert r.returncode == 3 and r.stderr.strip() == "Błąd: " + text
+
+
+def test_refused_command_lines_equal_reference(tmp_path):
+    """Command lines refused before any simulation work: the exit code and the message line are the
+    reference engine's, word for word, and --validate's report too (tests/golden/cli_errors.json, made
+    by make_golden.py --cli-errors; engine/src/app/Cli.cpp, Batch.cpp, ConfigCheck.cpp).  After an
+    argument error both engines print their usage text, which differs: this engine lists --serve."""
+    (tmp_path / "c.json").write_text('{"space": {"nx": 40, "ny": 1, "nz": 30}}')
+    (tmp_path / "empty").mkdir()
+    with open(os.path.join(GOLDEN, "cli_errors.json")) as f:
+        cases = json.load(f)
+    d = str(tmp_path)
+    for case in cases:
+        r = run(*[a.replace("{d}", d) for a in case["args"]], cwd=d)
+        first = (r.stderr.strip().splitlines() or [""])[0].replace(d, "{d}")
+        assert (r.returncode, first) == (case["exit"], case["stderr_first_line"]), case["args"]
+        if case["stdout"] is not None:
+            assert json.loads(r.stdout.replace(d, "{d}")) == json.loads(case["stdout"]), case["args"]

@@ -77,7 +77,7 @@ struct CliOptions {
 CliOptions parse_cli(int argc, char** argv) {
     CliOptions o;
     auto need = [&](int& i, const std::string& opt) -> std::string {
-        if (i + 1 >= argc) throw CliError("option " + opt + " needs a value");
+        if (i + 1 >= argc) throw CliError("opcja " + opt + " wymaga wartości");
         return argv[++i];
     };
     for (int i = 1; i < argc; ++i) {
@@ -90,13 +90,13 @@ CliOptions parse_cli(int argc, char** argv) {
         else if (a == "--set") {
             const std::string kv = need(i, a);
             if (kv.find('=') == std::string::npos || kv.front() == '=')
-                throw CliError("--set needs key=value (e.g. space.nx=100), given: " + kv);
+                throw CliError("--set wymaga postaci klucz=wartość (np. space.nx=100), podano: " + kv);
             o.overrides.push_back(kv);
         } else if (a == "--grid") o.overrides.push_back("grid=" + need(i, a));
         else if (a == "--threads") {
             const std::string n = need(i, a);
             if (n.empty() || n.find_first_not_of("0123456789") != std::string::npos)
-                throw CliError("option --threads needs an integer >= 0, given: " + n);
+                throw CliError("opcja --threads wymaga liczby całkowitej >= 0 (0 = wszystkie wątki OpenMP), podano: " + n);
             o.overrides.push_back("parallel.threads=" + n);
         } else if (a == "--thread-stats") o.thread_stats = true;
         else if (a == "--high-priority") o.overrides.push_back("parallel.priority=high");
@@ -110,35 +110,35 @@ CliOptions parse_cli(int argc, char** argv) {
         else if (a == "--slots") {
             const std::string n = need(i, a);
             if (n.empty() || n.find_first_not_of("0123456789") != std::string::npos || std::atoi(n.c_str()) < 1)
-                throw CliError("option --slots needs an integer >= 1, given: " + n);
+                throw CliError("opcja --slots wymaga liczby całkowitej >= 1, podano: " + n);
             o.slots = std::atoi(n.c_str());
         } else if (a == "--budget-gb") {
             const std::string n = need(i, a);
             char* end = nullptr;
             o.budget_gb = std::strtod(n.c_str(), &end);
             if (n.empty() || *end != '\0' || !(o.budget_gb > 0.0))
-                throw CliError("option --budget-gb needs a number > 0, given: " + n);
-        } else throw CliError("unknown argument: " + a + " (see --help)");
+                throw CliError("opcja --budget-gb wymaga liczby > 0, podano: " + n);
+        } else throw CliError("nieznany argument: " + a + " (zobacz --help)");
     }
     if (o.serve && (o.print_defaults || o.validate || o.benchmark || !o.config.empty() || !o.out.empty() ||
                     !o.mc_from.empty() || !o.batch.empty() || !o.overrides.empty()))
-        throw CliError("--serve reads its jobs from standard input and takes only --slots, --budget-gb and --no-batch");
+        throw CliError("--serve czyta zadania ze standardowego wejścia i przyjmuje tylko --slots, --budget-gb i --no-batch");
     if (!o.serve && (o.slots != 16 || o.budget_gb != 120.0 || !o.serve_batch))
-        throw CliError("--slots, --budget-gb and --no-batch belong to --serve");
+        throw CliError("--slots, --budget-gb i --no-batch dotyczą tylko --serve");
     if (o.print_defaults && (o.validate || o.benchmark || o.progress || o.timing_detail || o.thread_stats ||
                              !o.config.empty() || !o.out.empty() || !o.mc_from.empty() || !o.batch.empty() ||
                              !o.overrides.empty()))
-        throw CliError("--print-defaults takes no other options");
+        throw CliError("--print-defaults nie przyjmuje innych opcji");
     if (!o.batch.empty() && (!o.config.empty() || !o.mc_from.empty() || o.benchmark || o.validate))
-        throw CliError("--batch runs every config of a folder and does not combine with --config, --mc-from, "
-                       "--benchmark or --validate (allowed: --out, --set, --grid, --threads, --timing-detail, "
+        throw CliError("--batch uruchamia wszystkie configi z folderu i nie łączy się z --config, --mc-from, "
+                       "--benchmark ani --validate (dozwolone: --out, --set, --grid, --threads, --timing-detail, "
                        "--thread-stats, --progress)");
     if (o.validate && (o.benchmark || o.progress || o.timing_detail || o.thread_stats))
-        throw CliError("--validate only checks the config (--config, --set, --mc-from) and does not combine with "
-                       "--benchmark, --progress, --timing-detail or --thread-stats");
+        throw CliError("--validate tylko sprawdza config (--config, --set, --mc-from) i nie łączy się z "
+                       "--benchmark, --progress, --timing-detail ani --thread-stats");
     if (o.benchmark)
-        throw CliError("--benchmark compares the reference's CPU grid layouts (vector vs matrix); this engine has one "
-                       "GPU layout and no such benchmark");
+        throw CliError("--benchmark porównuje układy siatki CPU (vector i matrix); ten silnik ma jeden układ na GPU "
+                       "i nie wykonuje tego porównania");
     return o;
 }
 
@@ -583,10 +583,11 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
             s.mobility_used = cfg.mc.mobility_from_cooling;
         }
         if (cooling == Cooling::None && cfg.mc.mobility_from_cooling)
-            s.warnings.push_back("the CA result has no solidStep/arrivalStep (txt file): cooling mobility is off, MC as "
-                                 "with mobilityFromCooling = false");
+            s.warnings.push_back("wynik CA bez solidStep/arrivalStep (plik txt): mobilność ze stygnięcia "
+                                 "wyłączona, MC jak dla mobilityFromCooling = false");
         if (cooling == Cooling::SolidOnly)
-            s.warnings.push_back("ca_result.bin version 1 has no arrivalStep, liquid time counted from step 0 (= solidStep)");
+            s.warnings.push_back("ca_result.bin w wersji 1 nie zawiera arrivalStep, czas w stanie płynnym "
+                                 "liczony od kroku 0 (= solidStep)");
     }
     timing.add_detail("mcDomainMobility", ms_since(td));
     td = Clock::now();
@@ -596,7 +597,7 @@ McSummary run_mc(const Config& cfg, vca_ca* ca, const Microstructure* file, Cool
     vcheck(vca_mc_get_info(mc.h, &info), "vca_mc_get_info");
     s.domain_cells = info.domain_cells;
     if (s.domain_cells == 0)
-        s.warnings.push_back(full ? "the MC domain is empty" : "the MC domain is empty: the CA result holds no basalt");
+        s.warnings.push_back(full ? "domena MC jest pusta" : "domena MC jest pusta: wynik CA nie zawiera bazaltu");
     timing.add("mcInit", ms_since(t));
 
     const bool moore = cfg.neighborhood != Nb::VonNeumann;
@@ -750,7 +751,7 @@ void save_mc(const Config& cfg, const McSummary& s, const std::string& out_dir, 
     const auto tf = Clock::now();
     const std::string csv = (out / "mc_stats.csv").string();
     std::ofstream f(csv);
-    if (!f) throw std::runtime_error("Cannot create the file: " + csv);
+    if (!f) throw std::runtime_error("Nie można utworzyć pliku: " + csv);
     f << "mcs,grains,meanGrainSize,energy,acceptRate\n";
     char line[160];
     for (const McStats& st : s.history) {
@@ -758,7 +759,7 @@ void save_mc(const Config& cfg, const McSummary& s, const std::string& out_dir, 
                       st.energy, st.accept_rate);
         f << line;
     }
-    if (!f) throw std::runtime_error("Error writing the file: " + csv);
+    if (!f) throw std::runtime_error("Błąd zapisu pliku: " + csv);
     f.close();
     timing.add_file(csv, ms_since(tf));
     timing.add("mcSave", ms_since(t));
@@ -924,10 +925,11 @@ int run_from_cli(const CliOptions& opt, Clock::time_point start) {
     if (!opt.mc_from.empty()) {
         // Simulation::runMcFrom (Simulation.cpp:334-402)
         if (cfg.mc.full)
-            throw ConfigError("--mc-from crystallises a CA result from a file, so it needs mc.domain = \"basalt\"");
+            throw ConfigError("--mc-from krystalizuje wynik CA z pliku, więc wymaga mc.domain = \"basalt\" (podano \"" +
+                              std::string(cfg.mc.full ? "full" : "basalt") + "\")");
         std::vector<std::string> warnings;
         if (!cfg.mc.enabled) {
-            warnings.push_back("mc.enabled = false, but --mc-from always runs Monte Carlo");
+            warnings.push_back("mc.enabled = false, a w trybie --mc-from Monte Carlo jest uruchamiane zawsze");
             cfg.mc.enabled = true;
         }
         t = Clock::now();
@@ -935,11 +937,13 @@ int run_from_cli(const CliOptions& opt, Clock::time_point start) {
         const Microstructure ca = read_ca_folder(opt.mc_from, &src);
         timing.add("readInput", ms_since(t));
         if (ca.dims != cfg.space && cfg.space_from_user)
-            warnings.push_back("the file's dimensions " + std::to_string(ca.dims.nx) + " x " + std::to_string(ca.dims.ny) +
-                               " x " + std::to_string(ca.dims.nz) + " differ from the config's space; the file's apply");
+            warnings.push_back("wymiary z pliku " + std::to_string(ca.dims.nx) + " x " + std::to_string(ca.dims.ny) +
+                               " x " + std::to_string(ca.dims.nz) + " różnią się od space z configu (" +
+                               std::to_string(cfg.space.nx) + " x " + std::to_string(cfg.space.ny) + " x " +
+                               std::to_string(cfg.space.nz) + "); obowiązują wymiary z pliku");
         cfg.space = ca.dims;
         if (cfg.neighborhood == Nb::Hexagonal && !cfg.space.is2d())
-            throw ConfigError("The \"hexagonal\" neighbourhood is defined in 2D only, and the CA result in the file is 3D");
+            throw ConfigError("Sąsiedztwo „hexagonal” jest zdefiniowane tylko w 2D, a wynik CA z pliku jest 3D");
         Json space = Json::object();
         space["nx"] = ca.dims.nx;
         space["ny"] = ca.dims.ny;
@@ -1025,12 +1029,14 @@ int validate(const CliOptions& opt) {
         for (const auto& w : cfg.warnings) warnings.push_back(w);
         if (!opt.mc_from.empty()) {
             if (cfg.mc.full)
-                errors.push_back("--mc-from crystallises a CA result from a file, so it needs mc.domain = \"basalt\"");
-            if (!cfg.mc.enabled) warnings.push_back("mc.enabled = false, but --mc-from always runs Monte Carlo");
+                errors.push_back(std::string("--mc-from krystalizuje wynik CA z pliku, więc wymaga mc.domain = \"basalt\" ") +
+                                 "(podano \"full\")");
+            if (!cfg.mc.enabled)
+                warnings.push_back("mc.enabled = false, a w trybie --mc-from Monte Carlo jest uruchamiane zawsze");
             const fs::path dir(opt.mc_from);
-            if (!fs::is_directory(dir)) errors.push_back("The CA result folder (--mc-from) does not exist: " + opt.mc_from);
+            if (!fs::is_directory(dir)) errors.push_back("Folder wyniku CA (--mc-from) nie istnieje: " + opt.mc_from);
             else if (!fs::exists(dir / "ca_result.bin") && !fs::exists(dir / "ca_result.txt"))
-                errors.push_back("The folder " + opt.mc_from + " holds neither ca_result.bin nor ca_result.txt");
+                errors.push_back("W folderze " + opt.mc_from + " nie ma ca_result.bin ani ca_result.txt");
         } else if (!cfg.mc.full_only() && cfg.ca.mode == Mode::Lava && cfg.terrain.type == TerrainType::File) {
             (void)build_terrain(cfg);
         }
@@ -1108,7 +1114,7 @@ std::string self_exe() {
 
 int run_batch(const CliOptions& opt) {
     fs::path folder(opt.batch);
-    if (!fs::is_directory(folder)) throw CliError("--batch: the config folder does not exist: " + opt.batch);
+    if (!fs::is_directory(folder)) throw CliError("--batch: folder z configami nie istnieje: " + opt.batch);
     if (folder.filename().empty()) folder = folder.parent_path();
     const fs::path out = opt.out.empty() ? fs::path("results") / folder.filename() : fs::path(opt.out);
     struct Item {
@@ -1127,7 +1133,8 @@ int run_batch(const CliOptions& opt) {
     }
     std::sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.name < b.name; });
     if (items.empty())
-        throw ConfigError("The folder " + opt.batch + " holds no *.json config (series.json and _*.json are skipped)");
+        throw ConfigError("W folderze " + opt.batch + " nie ma plików konfiguracyjnych *.json "
+                          "(series.json i pliki _*.json są pomijane)");
     fs::create_directories(out);
     std::vector<std::string> extra;
     for (const std::string& o : opt.overrides) {
@@ -1211,6 +1218,7 @@ int run_batch(const CliOptions& opt) {
         rows.push_back(row);
         {
             std::ofstream f(out / "batch_summary.csv", std::ios::trunc);
+            if (!f) throw std::runtime_error("Nie można zapisać podsumowania serii: " + (out / "batch_summary.csv").string());
             for (size_t c = 0; c < cols.size(); ++c) f << (c ? "," : "") << cols[c];
             f << '\n';
             for (const auto& r : rows) {

@@ -16,7 +16,7 @@ namespace {
 
 std::ofstream open_out(const std::string& path, bool binary) {
     std::ofstream out(path, binary ? std::ios::binary : std::ios::out);
-    if (!out) throw std::runtime_error("Cannot create the file: " + path);
+    if (!out) throw std::runtime_error("Nie można utworzyć pliku: " + path);
     return out;
 }
 
@@ -28,7 +28,7 @@ void write_array(std::ofstream& out, const std::vector<T>& v) {
 template <class T>
 void read_array(std::ifstream& in, std::vector<T>& v, const std::string& path) {
     in.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(v.size() * sizeof(T)));
-    if (!in) throw std::runtime_error("File " + path + " is truncated (too little data)");
+    if (!in) throw std::runtime_error("Plik " + path + " jest obcięty (za mało danych)");
 }
 
 // Buffered text writer: rows appended to a ~1 MB buffer, flushed when full.
@@ -52,7 +52,7 @@ public:
     }
     void close(const std::string& path) {
         flush();
-        if (!out_) throw std::runtime_error("Error writing the file: " + path);
+        if (!out_) throw std::runtime_error("Błąd zapisu pliku: " + path);
     }
 
 private:
@@ -94,7 +94,7 @@ void write_ca_bin(const std::string& path, const Microstructure& m) {
     write_array(out, m.temp);
     write_array(out, m.solid);
     write_array(out, m.arrival);
-    if (!out) throw std::runtime_error("Error writing the file: " + path);
+    if (!out) throw std::runtime_error("Błąd zapisu pliku: " + path);
 }
 
 void write_ca_txt(const std::string& path, const Microstructure& m) {
@@ -129,7 +129,7 @@ void write_crystal_bin(const std::string& path, const CrystalMap& m) {
     out.write(magic, 4);
     out.write(reinterpret_cast<const char*>(dims), 12);
     write_array(out, m.crystal);
-    if (!out) throw std::runtime_error("Error writing the file: " + path);
+    if (!out) throw std::runtime_error("Błąd zapisu pliku: " + path);
 }
 
 void write_crystal_txt(const std::string& path, const CrystalMap& m) {
@@ -156,16 +156,16 @@ void write_crystal_txt(const std::string& path, const CrystalMap& m) {
 void write_json(const std::string& path, const Json& j) {
     std::ofstream out = open_out(path, false);
     out << j.dump(2) << '\n';
-    if (!out) throw std::runtime_error("Error writing the file: " + path);
+    if (!out) throw std::runtime_error("Błąd zapisu pliku: " + path);
 }
 
 namespace {
 
 Dims read_txt_header(std::ifstream& in, const std::string& path) {
-    if (!in) throw std::runtime_error("Cannot open the file: " + path);
+    if (!in) throw std::runtime_error("Nie można otworzyć pliku: " + path);
     Dims d;
     if (!(in >> d.nx >> d.ny >> d.nz) || d.nx < 1 || d.ny < 1 || d.nz < 1)
-        throw std::runtime_error("File " + path + ": invalid dimension header");
+        throw std::runtime_error("Plik " + path + ": nieprawidłowy nagłówek wymiarów");
     std::string line;
     std::getline(in, line);
     std::getline(in, line);
@@ -182,10 +182,10 @@ Microstructure read_txt(const std::string& path) {
         int32_t flow = 0;
         float temp = 0.0f;
         if (!(in >> x >> y >> z >> type >> flow >> temp))
-            throw std::runtime_error("File " + path + ": too few data rows (read " + std::to_string(n) + " of " +
+            throw std::runtime_error("Plik " + path + ": za mało wierszy danych (wczytano " + std::to_string(n) + " z " +
                                      std::to_string(d.cells()) + ")");
         if (x < 0 || x >= d.nx || y < 0 || y >= d.ny || z < 0 || z >= d.nz)
-            throw std::runtime_error("File " + path + ": coordinates outside the space in line " + std::to_string(n + 3));
+            throw std::runtime_error("Plik " + path + ": współrzędne poza przestrzenią w wierszu " + std::to_string(n + 3));
         const size_t i = (size_t)x + (size_t)d.nx * ((size_t)y + (size_t)d.ny * z);
         m.type[i] = (uint8_t)type;
         m.flow[i] = flow;
@@ -196,16 +196,16 @@ Microstructure read_txt(const std::string& path) {
 
 Microstructure read_bin(const std::string& path, uint32_t* version_out) {
     std::ifstream in(path, std::ios::binary);
-    if (!in) throw std::runtime_error("Cannot open the file: " + path);
+    if (!in) throw std::runtime_error("Nie można otworzyć pliku: " + path);
     char magic[4] = {};
     uint32_t version = 0;
     int32_t dims[3] = {};
     in.read(magic, 4);
     in.read(reinterpret_cast<char*>(&version), 4);
     in.read(reinterpret_cast<char*>(dims), 12);
-    if (!in || std::memcmp(magic, "VOLC", 4) != 0) throw std::runtime_error("File " + path + " is not a VOLC result file");
-    if (version < 1 || version > 2) throw std::runtime_error("File " + path + ": unsupported format version " + std::to_string(version));
-    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1) throw std::runtime_error("File " + path + ": invalid dimensions");
+    if (!in || std::memcmp(magic, "VOLC", 4) != 0) throw std::runtime_error("Plik " + path + " nie jest plikiem wyników VOLC");
+    if (version < 1 || version > 2) throw std::runtime_error("Plik " + path + ": nieobsługiwana wersja formatu " + std::to_string(version));
+    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1) throw std::runtime_error("Plik " + path + ": nieprawidłowe wymiary");
     Microstructure m;
     m.resize(Dims{dims[0], dims[1], dims[2]});
     read_array(in, m.type, path);

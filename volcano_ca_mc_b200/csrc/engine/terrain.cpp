@@ -95,7 +95,7 @@ Heightmap cone_terrain(const Config& c) {
 // ny data rows of nx non-negative numbers; ROCK count = ceil(value) clamped to nz.
 Heightmap load_heightmap_csv(const std::string& path, const Dims& d) {
     std::ifstream in(path);
-    if (!in) throw ConfigError("Cannot open the heightmap file: " + path);
+    if (!in) throw ConfigError("Nie można otworzyć pliku mapy wysokości: " + path);
     Heightmap hm;
     hm.nx = d.nx;
     hm.ny = d.ny;
@@ -118,22 +118,22 @@ Heightmap load_heightmap_csv(const std::string& path, const Dims& d) {
         }
         if (!cur.empty()) fields.push_back(cur);
         if (fields.empty() || fields[0][0] == '#') continue;
-        if (row >= d.ny) throw ConfigError("Heightmap " + path + " has more data rows than ny = " + std::to_string(d.ny));
+        if (row >= d.ny) throw ConfigError("Mapa wysokości " + path + " ma więcej wierszy danych niż ny = " + std::to_string(d.ny));
         if ((int)fields.size() != d.nx)
-            throw ConfigError("Heightmap " + path + ", line " + std::to_string(line_no) + ": " + std::to_string(fields.size()) +
-                              " values, expected nx = " + std::to_string(d.nx));
+            throw ConfigError("Mapa wysokości " + path + ", wiersz " + std::to_string(line_no) + ": " + std::to_string(fields.size()) +
+                              " wartości, oczekiwano nx = " + std::to_string(d.nx));
         for (size_t col = 0; col < fields.size(); ++col) {
             char* end = nullptr;
             const double h = std::strtod(fields[col].c_str(), &end);
             if (end == fields[col].c_str() || *end != '\0' || !std::isfinite(h) || h < 0.0)
-                throw ConfigError("Heightmap " + path + ", line " + std::to_string(line_no) + ", column " +
-                                  std::to_string(col + 1) + ": expected a non-negative number, found \"" + fields[col] + "\"");
+                throw ConfigError("Mapa wysokości " + path + ", wiersz " + std::to_string(line_no) + ", kolumna " +
+                                  std::to_string(col + 1) + ": oczekiwano nieujemnej liczby, jest \"" + fields[col] + "\"");
             hm.height.push_back(std::min((int)std::ceil(h), d.nz));
         }
         ++row;
     }
     if (row != d.ny)
-        throw ConfigError("Heightmap " + path + " has " + std::to_string(row) + " data rows, expected ny = " + std::to_string(d.ny));
+        throw ConfigError("Mapa wysokości " + path + " ma " + std::to_string(row) + " wierszy danych, oczekiwano ny = " + std::to_string(d.ny));
     return hm;
 }
 
@@ -156,10 +156,10 @@ std::vector<Vent> place_vents(const Config& c, const Heightmap& hm) {
             if (ok) cand.emplace_back(x, y);
         }
     if ((int)cand.size() < c.vents.count)
-        throw ConfigError(std::string("Too few places for vents (placement = ") +
-                          (c.vents.placement == Placement::Crater ? "crater" : "random") + "): " + std::to_string(cand.size()) +
-                          " available, vents.count = " + std::to_string(c.vents.count) +
-                          (c.vents.placement == Placement::Crater ? "; increase terrain.craterRadius" : ""));
+        throw ConfigError(std::string("Za mało miejsc na kratery (placement = ") +
+                          (c.vents.placement == Placement::Crater ? "crater" : "random") + "): dostępnych " +
+                          std::to_string(cand.size()) + ", a vents.count = " + std::to_string(c.vents.count) +
+                          (c.vents.placement == Placement::Crater ? "; zwiększ terrain.craterRadius" : ""));
     std::mt19937_64 gen(splitmix64(c.seed ^ kSaltVents));
     std::vector<Vent> vents;
     for (int i = 0; i < c.vents.count; ++i) {
