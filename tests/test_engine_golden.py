@@ -8,6 +8,7 @@ import csv
 import hashlib
 import json
 import os
+import re
 import shutil
 import subprocess
 
@@ -78,6 +79,9 @@ def test_engine_progress_same_result(tmp_path):
     assert r.returncode == 0, r.stderr
     lines = [l for l in r.stdout.splitlines() if l.startswith("PROGRESS ")]
     assert any(l.startswith("PROGRESS ca ") for l in lines) and any(l.startswith("PROGRESS mc ") for l in lines)
+    # every line in the form the reference's GUI job queue parses (gui/jobs.py:63)
+    gui = re.compile(r"^PROGRESS (\w+) (\d+)/(\d+)(?: (\w+)=(\d+))?\s*$")
+    assert all(gui.match(l) for l in lines), [l for l in lines if not gui.match(l)][:3]
     compare(str(out), load_expect("lava2d_moore"))
 
 
