@@ -50,6 +50,7 @@ def ca_runs() -> dict:
     def run(name):
         cfg, _ = load(name)
         return name, oracle_ca(cfg, initial(name))
+    O.lib()  # loaded once, before the threads share it
     with ThreadPoolExecutor(max_workers=max(1, min(len(CA_CONFIGS), os.cpu_count() or 1))) as ex:
         return dict(ex.map(run, sorted(CA_CONFIGS, key=lambda n: n.startswith("etna"), reverse=True)))
 
